@@ -1,0 +1,124 @@
+"""ctypes mirrors of the C ABI structs in include/adrt_b200.h.
+
+Every Python entry point of the package (and the tests and bench harness)
+passes arrays to the native library through these structs.  Field order and
+types must match the header exactly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+ADRT_OK = 0
+ADRT_ERR_INVALID_ARGUMENT = -1
+ADRT_ERR_UNSUPPORTED = -2
+ADRT_ERR_CUDA = -3
+ADRT_ERR_OUT_OF_MEMORY = -4
+ADRT_ERR_WORKSPACE = -5
+ADRT_ERR_NUMERICAL = -6
+
+ADRT_FLAG_SINGULAR_PIVOT = 1
+ADRT_FLAG_NONFINITE = 2
+ADRT_FLAG_BAD_INPUT = 4
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+MOMENTS_SHARED = 0
+MOMENTS_PER_WAVENUMBER = 1
+MOMENTS_PER_LAYER = 2
+
+_dp = C.POINTER(C.c_double)
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("num_wavenumbers", C.c_int),
+        ("num_layers", C.c_int),
+        ("num_quadrature", C.c_int),
+        ("num_moments", C.c_int),
+        ("moment_layout", C.c_int),
+        ("precision", C.c_int),
+        ("use_thermal_emission", C.c_int),
+        ("use_delta_m", C.c_int),
+        ("use_diffusion_lower_bc", C.c_int),
+        ("index_from_bottom", C.c_int),
+        ("temperature_per_wavenumber", C.c_int),
+        ("surface_albedo", C.c_double),
+        ("surface_emission", C.c_double),
+        ("surface_temperature", C.c_double),
+        ("top_emission", C.c_double),
+        ("top_temperature", C.c_double),
+        ("solar_flux", C.c_double),
+        ("solar_mu", C.c_double),
+        ("wavenumber_low", C.c_double),
+        ("wavenumber_high", C.c_double),
+        ("spectrum_scaling", C.c_double),
+    ]
+
+
+INPUT_FIELDS = (
+    "delta_tau",
+    "single_scat_albedo",
+    "phase_moments",
+    "temperature",
+    "planck_levels",
+    "surface_albedo",
+    "solar_mu",
+    "wavenumber_low",
+    "wavenumber_high",
+    "surface_emission",
+    "top_emission",
+)
+
+OUTPUT_FIELDS = (
+    "flux_up",
+    "flux_down",
+    "flux_direct",
+    "mean_intensity",
+    "flux_divergence",
+    "toa_flux_up",
+    "toa_flux_down",
+    "boa_flux_direct",
+)
+
+INTERFACE_OUTPUTS = OUTPUT_FIELDS[:5]
+
+
+class Inputs(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in INPUT_FIELDS]
+
+
+class Outputs(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
+
+
+class ColumnDesc(C.Structure):
+    _fields_ = [("desc", BatchDesc), ("inp", Inputs), ("out", Outputs)]
+
+
+class EngineOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("max_workspace_bytes", C.c_size_t)]
+
+
+DESC_INT_FIELDS = tuple(n for n, t in BatchDesc._fields_ if t is C.c_int)
+DESC_FLOAT_FIELDS = tuple(n for n, t in BatchDesc._fields_ if t is C.c_double)
+
+
+def make_desc(**kw) -> BatchDesc:
+    """BatchDesc with the reference's defaults (ADConfig / BatchConfig)."""
+    d = BatchDesc()
+    d.num_quadrature = 8
+    d.moment_layout = MOMENTS_SHARED
+    d.surface_temperature = -1.0
+    d.top_temperature = -1.0
+    d.solar_mu = 1.0
+    d.spectrum_scaling = 1.0
+    for k, v in kw.items():
+        if not hasattr(d, k):
+            raise AttributeError(f"adrt_batch_desc has no field {k!r}")
+        setattr(d, k, v)
+    return d
+
+
+def desc_to_dict(d: BatchDesc) -> dict:
+    return {n: getattr(d, n) for n, _ in BatchDesc._fields_}

@@ -1,0 +1,626 @@
+// adrt_engine.cu -- host engine behind the C ABI of include/adrt_b200.h.
+//
+// The engine owns every device buffer a solve needs (quadrature tables, the
+// per-slot work buffer, the work counter and the status word), so a solve
+// launch allocates nothing once adrt_engine_reserve() has sized it, and the
+// only stream operations are one memset and one kernel launch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/adrt_b200.h"
+#include "adrt_kernel.cuh"
+
+using namespace adrt_dev;
+
+namespace {
+
+thread_local std::string g_detail;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_detail = buf;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                             \
+  do {                                                                             \
+    cudaError_t e_ = (expr);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(ADRT_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));  \
+  } while (0)
+
+// Gauss-Legendre nodes and weights on [0,1]: Newton iteration on P_n from the
+// Chebyshev-like start cos(pi (i + 3/4) / (n + 1/2)), stopping at |dz| < 1e-15
+// -- the construction of the reference's src/quadrature.cpp:11-51, which the
+// engine must reproduce to the last bit so that its quadrature matches.
+void gauss_legendre01(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = std::cos(kPi * (i + 0.75) / (n + 0.5));
+    double pp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const double pk = ((2 * k - 1) * z * p1 - (k - 1) * p0) / k;
+        p0 = p1;
+        p1 = pk;
+      }
+      pp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = -p1 / pp;
+      z += dz;
+      if (std::fabs(dz) < 1e-15) break;
+    }
+    const double wi = 2.0 / ((1.0 - z * z) * pp * pp);
+    x[i] = (1.0 - z) / 2.0;
+    x[n - 1 - i] = (1.0 + z) / 2.0;
+    w[i] = wi / 2.0;
+    w[n - 1 - i] = wi / 2.0;
+  }
+}
+
+// Kernel table: one instantiation per padded order and precision.
+using LaunchFn = int (*)(const SolveParams&, const ColumnDev&, int grid, cudaStream_t);
+
+template <int NP, typename Real>
+struct Kern {
+  using Gm = Geo<NP, Real>;
+  static constexpr int kThreads = 128;
+  static constexpr int kGroups = kThreads / Gm::G;
+  static size_t smem() { return (size_t)kGroups * SmemLayout<Gm>::bytes; }
+  static size_t slot_bytes(int lmax) { return SlotLayout<Gm>::bytes(lmax); }
+  static int max_blocks_per_sm() {
+    static int cached = -1;
+    if (cached < 0) {
+      cudaFuncSetAttribute(solve_kernel<NP, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem());
+      int nb = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_kernel<NP, Real>, kThreads, smem());
+      cached = nb > 0 ? nb : 1;
+    }
+    return cached;
+  }
+  static int launch(const SolveParams& p, const ColumnDev& c0, int grid, cudaStream_t s) {
+    solve_kernel<NP, Real><<<grid, kThreads, smem(), s>>>(p, c0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ADRT_ERR_CUDA, "solve kernel launch: %s", cudaGetErrorString(e));
+    return ADRT_OK;
+  }
+};
+
+struct KernInfo {
+  int np, groups;
+  size_t (*slot_bytes)(int);
+  int (*max_blocks)();
+  LaunchFn launch;
+};
+
+template <int NP, typename Real>
+KernInfo kinfo() {
+  return KernInfo{NP, Kern<NP, Real>::kGroups, &Kern<NP, Real>::slot_bytes,
+                  &Kern<NP, Real>::max_blocks_per_sm, &Kern<NP, Real>::launch};
+}
+
+int padded_order(int n) { return n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : 32; }
+
+KernInfo pick(int n, int precision) {
+  const int np = padded_order(n);
+  if (precision == ADRT_PRECISION_MIXED) {
+    switch (np) {
+      case 4: return kinfo<4, float>();
+      case 8: return kinfo<8, float>();
+      case 16: return kinfo<16, float>();
+      default: return kinfo<32, float>();
+    }
+  }
+  switch (np) {
+    case 4: return kinfo<4, double>();
+    case 8: return kinfo<8, double>();
+    case 16: return kinfo<16, double>();
+    default: return kinfo<32, double>();
+  }
+}
+
+}  // namespace
+
+struct adrt_engine {
+  int device = 0;
+  int num_sms = 0;
+  size_t max_ws = 0;
+  cudaStream_t last_stream = nullptr;
+  char* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  unsigned long long* counter = nullptr;
+  unsigned int* status = nullptr;
+  ColumnDev* d_cols = nullptr;
+  size_t d_cols_cap = 0;
+  struct Quad {
+    double* buf = nullptr;
+    int mmax = 0;
+    QuadDev dev{};
+  } quad[kMaxN + 1];
+  // host-entry staging buffers
+  std::vector<void*> host_stage;
+  std::mutex mu;
+};
+
+namespace {
+
+int set_device(adrt_engine* e) {
+  CUDA_TRY(cudaSetDevice(e->device));
+  return ADRT_OK;
+}
+
+// Quadrature table for order n with Legendre rows up to mmax.
+int ensure_quad(adrt_engine* e, int n, int mmax) {
+  auto& q = e->quad[n];
+  if (q.buf && q.mmax >= mmax) return ADRT_OK;
+  mmax = std::max(mmax, 2 * n);
+  std::vector<double> x, w;
+  gauss_legendre01(n, x, w);
+  std::vector<double> host((size_t)2 * n + (size_t)mmax * n);
+  for (int i = 0; i < n; ++i) {
+    host[i] = x[i];
+    host[n + i] = w[i];
+  }
+  double* pl = host.data() + 2 * n;
+  for (int i = 0; i < n; ++i) pl[i] = 1.0;
+  if (mmax > 1)
+    for (int i = 0; i < n; ++i) pl[n + i] = x[i];
+  for (int l = 2; l < mmax; ++l)
+    for (int i = 0; i < n; ++i)
+      pl[l * n + i] = ((2 * l - 1) * x[i] * pl[(l - 1) * n + i] - (l - 1) * pl[(l - 2) * n + i]) / l;
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s += x[i] * w[i];
+  if (q.buf) {
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(q.buf);
+    q.buf = nullptr;
+  }
+  if (cudaMalloc(&q.buf, host.size() * sizeof(double)) != cudaSuccess)
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "quadrature table allocation failed");
+  CUDA_TRY(cudaMemcpy(q.buf, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice));
+  q.mmax = mmax;
+  q.dev.mu = q.buf;
+  q.dev.wt = q.buf + n;
+  q.dev.pl = q.buf + 2 * n;
+  q.dev.mmax = mmax;
+  q.dev.xfac = 0.5 / s;
+  return ADRT_OK;
+}
+
+int check_desc(const adrt_batch_desc* d) {
+  if (!d) return fail(ADRT_ERR_INVALID_ARGUMENT, "null batch description");
+  if (d->num_wavenumbers < 1) return fail(ADRT_ERR_INVALID_ARGUMENT, "num_wavenumbers must be >= 1");
+  if (d->num_layers <= 0) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: num_layers must be > 0");
+  if (d->num_quadrature < 2) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: num_quadrature must be >= 2");
+  if (d->num_quadrature > kMaxN)
+    return fail(ADRT_ERR_UNSUPPORTED, "num_quadrature %d > 32 is not supported", d->num_quadrature);
+  if (d->num_moments < 1 || d->num_moments > kMaxMoments)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "num_moments must be in 1..%d", kMaxMoments);
+  if (d->moment_layout < 0 || d->moment_layout > 2)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "unknown moment_layout %d", d->moment_layout);
+  if (d->precision != ADRT_PRECISION_FP64 && d->precision != ADRT_PRECISION_MIXED)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "unknown precision %d", d->precision);
+  if (d->surface_albedo < 0.0 || d->surface_albedo > 1.0)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: surface_albedo out of [0,1]");
+  if (d->solar_flux > 0.0 && (d->solar_mu <= 0.0 || d->solar_mu > 1.0))
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: solar_mu must be in (0,1] when solar_flux > 0");
+  if (d->use_thermal_emission) {
+    if (d->wavenumber_low < 0.0 || d->wavenumber_high < d->wavenumber_low)
+      return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: invalid wavenumber range");
+  } else if (d->surface_temperature >= 0.0) {
+    return fail(ADRT_ERR_INVALID_ARGUMENT,
+                "ADConfig: surface_temperature requires use_thermal_emission "
+                "(use surface_emission for raw thermal sources)");
+  } else if (d->top_temperature >= 0.0) {
+    return fail(ADRT_ERR_INVALID_ARGUMENT,
+                "ADConfig: top_temperature requires use_thermal_emission "
+                "(use top_emission for raw thermal sources)");
+  }
+  return ADRT_OK;
+}
+
+int check_inputs(const adrt_batch_desc* d, const adrt_inputs* in) {
+  if (!in) return fail(ADRT_ERR_INVALID_ARGUMENT, "null inputs");
+  if (!in->delta_tau) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: delta_tau size mismatch");
+  if (!in->single_scat_albedo)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: single_scat_albedo size mismatch");
+  if (!in->phase_moments)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: phase_function_moments size mismatch");
+  if (d->use_thermal_emission && !in->temperature)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: temperature size must be num_layers+1");
+  if (d->use_diffusion_lower_bc && !d->use_thermal_emission && !in->planck_levels)
+    return fail(ADRT_ERR_INVALID_ARGUMENT,
+                "ADConfig: use_diffusion_lower_bc requires use_thermal_emission or planck_levels");
+  return ADRT_OK;
+}
+
+ColumnDev make_column(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
+                      const adrt_outputs* out) {
+  ColumnDev c{};
+  c.W = d->num_wavenumbers;
+  c.L = d->num_layers;
+  c.N = d->num_quadrature;
+  c.NP = padded_order(d->num_quadrature);
+  c.M = d->num_moments;
+  c.moment_layout = d->moment_layout;
+  c.thermal = d->use_thermal_emission;
+  c.delta_m = d->use_delta_m;
+  c.diffusion = d->use_diffusion_lower_bc;
+  c.from_bottom = d->index_from_bottom;
+  c.temp_per_wav = d->temperature_per_wavenumber;
+  c.precision = d->precision;
+  c.surface_albedo = d->surface_albedo;
+  c.surface_emission = d->surface_emission;
+  c.surface_temperature = d->surface_temperature;
+  c.top_emission = d->top_emission;
+  c.top_temperature = d->top_temperature;
+  c.solar_flux = d->solar_flux;
+  c.solar_mu = d->solar_mu;
+  c.wn_lo = d->wavenumber_low;
+  c.wn_hi = d->wavenumber_high;
+  c.spectrum_scaling = d->spectrum_scaling;
+  c.dtau = in->delta_tau;
+  c.ssa = in->single_scat_albedo;
+  c.moments = in->phase_moments;
+  c.temperature = in->temperature;
+  c.planck = in->planck_levels;
+  c.albedo_w = in->surface_albedo;
+  c.mu0_w = in->solar_mu;
+  c.wlo_w = in->wavenumber_low;
+  c.whi_w = in->wavenumber_high;
+  c.semis_w = in->surface_emission;
+  c.temis_w = in->top_emission;
+  if (out) {
+    c.fu = out->flux_up;
+    c.fd = out->flux_down;
+    c.fdir = out->flux_direct;
+    c.J = out->mean_intensity;
+    c.divF = out->flux_divergence;
+    c.toa_fu = out->toa_flux_up;
+    c.toa_fd = out->toa_flux_down;
+    c.boa_fdir = out->boa_flux_direct;
+  }
+  c.quad = e->quad[d->num_quadrature].dev;
+  c.task_begin = 0;
+  return c;
+}
+
+// Size the work buffer for (kernel, lmax); grows only outside stream capture.
+int ensure_scratch(adrt_engine* e, const KernInfo& k, int lmax, int* grid, size_t* slot_bytes) {
+  const int bps = k.max_blocks();
+  *slot_bytes = (k.slot_bytes(lmax) + 255) & ~size_t(255);
+  int blocks = bps * e->num_sms;
+  size_t need = (size_t)blocks * k.groups * (*slot_bytes);
+  if (e->max_ws && need > e->max_ws) {
+    blocks = (int)(e->max_ws / ((size_t)k.groups * (*slot_bytes)));
+    if (blocks < 1)
+      return fail(ADRT_ERR_WORKSPACE, "workspace limit %zu B below one slot (%zu B)", e->max_ws,
+                  *slot_bytes);
+    need = (size_t)blocks * k.groups * (*slot_bytes);
+  }
+  if (need > e->scratch_bytes) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (e->last_stream) cudaStreamIsCapturing(e->last_stream, &cap);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE,
+                  "work buffer too small during stream capture; call adrt_engine_reserve first");
+    if (e->scratch) {
+      CUDA_TRY(cudaDeviceSynchronize());
+      cudaFree(e->scratch);
+      e->scratch = nullptr;
+      e->scratch_bytes = 0;
+    }
+    if (cudaMalloc(&e->scratch, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "work buffer allocation of %zu B failed", need);
+    }
+    e->scratch_bytes = need;
+  }
+  *grid = (int)(e->scratch_bytes / ((size_t)k.groups * (*slot_bytes)));
+  *grid = std::min(*grid, bps * e->num_sms);
+  return ADRT_OK;
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+const char* adrt_last_status_detail(void) { return g_detail.c_str(); }
+const char* adrt_version(void) { return "adrt-b200 0.1.0 (sm_100a)"; }
+
+int adrt_engine_create(const adrt_engine_opts* opts, adrt_engine** out) {
+  if (!out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine out-pointer");
+  *out = nullptr;
+  int dev = 0;
+  if (opts && opts->device >= 0) {
+    dev = opts->device;
+  } else {
+    CUDA_TRY(cudaGetDevice(&dev));
+  }
+  int ndev = 0;
+  CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (dev >= ndev) return fail(ADRT_ERR_INVALID_ARGUMENT, "device %d not present", dev);
+  auto* e = new adrt_engine();
+  e->device = dev;
+  e->max_ws = opts ? opts->max_workspace_bytes : 0;
+  int rc = set_device(e);
+  if (rc) {
+    delete e;
+    return rc;
+  }
+  cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaMalloc(&e->counter, 64) != cudaSuccess || cudaMalloc(&e->status, 64) != cudaSuccess) {
+    delete e;
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "engine allocation failed");
+  }
+  cudaMemset(e->status, 0, 64);
+  *out = e;
+  return ADRT_OK;
+}
+
+int adrt_engine_destroy(adrt_engine* e) {
+  if (!e) return ADRT_OK;
+  cudaSetDevice(e->device);
+  cudaDeviceSynchronize();
+  cudaFree(e->scratch);
+  cudaFree(e->counter);
+  cudaFree(e->status);
+  cudaFree(e->d_cols);
+  for (auto& q : e->quad) cudaFree(q.buf);
+  for (void* p : e->host_stage) cudaFree(p);
+  delete e;
+  return ADRT_OK;
+}
+
+int adrt_engine_reserve(adrt_engine* e, const adrt_batch_desc* d) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = set_device(e))) return rc;
+  if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
+  KernInfo k = pick(d->num_quadrature, d->precision);
+  int grid;
+  size_t sb;
+  return ensure_scratch(e, k, d->num_layers, &grid, &sb);
+}
+
+int adrt_engine_workspace_bytes(const adrt_engine* e, size_t* bytes) {
+  if (!e || !bytes) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = e->scratch_bytes;
+  return ADRT_OK;
+}
+
+int adrt_engine_read_status(adrt_engine* e, int* flags) {
+  if (!e || !flags) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lk(e->mu);
+  int rc = set_device(e);
+  if (rc) return rc;
+  CUDA_TRY(cudaDeviceSynchronize());
+  unsigned int v = 0;
+  CUDA_TRY(cudaMemcpy(&v, e->status, sizeof v, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemset(e->status, 0, sizeof v));
+  *flags = (int)v;
+  return ADRT_OK;
+}
+
+int adrt_validate_batch(const adrt_batch_desc* d, const adrt_inputs* in) {
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if ((rc = check_inputs(d, in))) return rc;
+  const int W = d->num_wavenumbers, L = d->num_layers;
+  for (int w = 0; w < W; ++w) {
+    for (int l = 0; l < L; ++l) {
+      const double t = in->delta_tau[(size_t)w * L + l];
+      const double o = in->single_scat_albedo[(size_t)w * L + l];
+      if (!(t >= 0.0)) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: delta_tau[%d] < 0 (wavenumber %d)", l, w);
+      if (!(o >= 0.0 && o <= 1.0))
+        return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: single_scat_albedo[%d] out of [0,1] (wavenumber %d)", l, w);
+    }
+    const double a = in->surface_albedo ? in->surface_albedo[w] : d->surface_albedo;
+    if (!(a >= 0.0 && a <= 1.0)) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: surface_albedo out of [0,1]");
+    const double m0 = in->solar_mu ? in->solar_mu[w] : d->solar_mu;
+    if (d->solar_flux > 0.0 && !(m0 > 0.0 && m0 <= 1.0))
+      return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: solar_mu must be in (0,1] when solar_flux > 0");
+    if (d->use_thermal_emission) {
+      const double lo = in->wavenumber_low ? in->wavenumber_low[w] : d->wavenumber_low;
+      const double hi = in->wavenumber_high ? in->wavenumber_high[w] : d->wavenumber_high;
+      if (!(lo >= 0.0 && hi >= lo)) return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: invalid wavenumber range");
+    }
+  }
+  if (d->use_thermal_emission) {
+    const size_t nt = (size_t)(d->temperature_per_wavenumber ? W : 1) * (L + 1);
+    for (size_t i = 0; i < nt; ++i)
+      if (!(in->temperature[i] >= 0.0))
+        return fail(ADRT_ERR_INVALID_ARGUMENT, "ADConfig: temperature[%zu] < 0", i % (L + 1));
+  }
+  return ADRT_OK;
+}
+
+int adrt_solve_batch(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
+                     const adrt_outputs* out, void* stream_ptr) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if ((rc = check_inputs(d, in))) return rc;
+  if (!out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null outputs");
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = set_device(e))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  e->last_stream = s;
+  if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
+  KernInfo k = pick(d->num_quadrature, d->precision);
+  int grid;
+  size_t sb;
+  if ((rc = ensure_scratch(e, k, d->num_layers, &grid, &sb))) return rc;
+  ColumnDev c0 = make_column(e, d, in, out);
+  SolveParams p{};
+  p.cols = nullptr;
+  p.ncols = 1;
+  p.ntasks = d->num_wavenumbers;
+  p.counter = e->counter;
+  p.status = e->status;
+  p.scratch = e->scratch;
+  p.slot_bytes = sb;
+  p.nslots = grid * k.groups;
+  p.max_layers = d->num_layers;
+  const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
+  grid = std::min(grid, need_blocks);
+  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+  return k.launch(p, c0, grid, s);
+}
+
+int adrt_solve_batch_uneven(adrt_engine* e, const adrt_column_desc* cols, int ncols,
+                            void* stream_ptr) {
+  if (!e || !cols || ncols < 1) return fail(ADRT_ERR_INVALID_ARGUMENT, "bad uneven-batch arguments");
+  int rc;
+  int np = -1, prec = -1, lmax = 0, mmax = 0;
+  for (int i = 0; i < ncols; ++i) {
+    if ((rc = check_desc(&cols[i].desc))) return rc;
+    if ((rc = check_inputs(&cols[i].desc, &cols[i].in))) return rc;
+    const int npi = padded_order(cols[i].desc.num_quadrature);
+    if (np >= 0 && (npi != np || cols[i].desc.precision != prec))
+      return fail(ADRT_ERR_UNSUPPORTED,
+                  "uneven batch: columns must share the padded quadrature class and precision");
+    np = npi;
+    prec = cols[i].desc.precision;
+    lmax = std::max(lmax, cols[i].desc.num_layers);
+    mmax = std::max(mmax, cols[i].desc.num_moments);
+  }
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = set_device(e))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  e->last_stream = s;
+  std::vector<ColumnDev> h(ncols);
+  long long total = 0;
+  for (int i = 0; i < ncols; ++i) {
+    if ((rc = ensure_quad(e, cols[i].desc.num_quadrature, cols[i].desc.num_moments))) return rc;
+  }
+  for (int i = 0; i < ncols; ++i) {
+    h[i] = make_column(e, &cols[i].desc, &cols[i].in, &cols[i].out);
+    h[i].task_begin = total;
+    total += cols[i].desc.num_wavenumbers;
+  }
+  KernInfo k = pick(np, prec);
+  int grid;
+  size_t sb;
+  if ((rc = ensure_scratch(e, k, lmax, &grid, &sb))) return rc;
+  if (e->d_cols_cap < (size_t)ncols) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE, "column table too small during capture");
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->d_cols);
+    e->d_cols = nullptr;
+    if (cudaMalloc(&e->d_cols, sizeof(ColumnDev) * ncols) != cudaSuccess)
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "column table allocation failed");
+    e->d_cols_cap = ncols;
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_cols, h.data(), sizeof(ColumnDev) * ncols, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  SolveParams p{};
+  p.cols = e->d_cols;
+  p.ncols = ncols;
+  p.ntasks = total;
+  p.counter = e->counter;
+  p.status = e->status;
+  p.scratch = e->scratch;
+  p.slot_bytes = sb;
+  p.nslots = grid * k.groups;
+  p.max_layers = lmax;
+  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+  return k.launch(p, h[0], grid, s);
+}
+
+int adrt_solve_batch_host(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* hin,
+                          const adrt_outputs* hout) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if ((rc = check_inputs(d, hin))) return rc;
+  if (!hout) return fail(ADRT_ERR_INVALID_ARGUMENT, "null outputs");
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    if ((rc = set_device(e))) return rc;
+  }
+  const size_t W = d->num_wavenumbers, L = d->num_layers, M = d->num_moments;
+  size_t nmom = d->moment_layout == ADRT_MOMENTS_SHARED ? L * M
+                : d->moment_layout == ADRT_MOMENTS_PER_WAVENUMBER ? W * M : W * L * M;
+  struct Arr {
+    const double* h;
+    size_t n;
+  };
+  const Arr ins[11] = {{hin->delta_tau, W * L},
+                       {hin->single_scat_albedo, W * L},
+                       {hin->phase_moments, nmom},
+                       {hin->temperature, (d->temperature_per_wavenumber ? W : 1) * (L + 1)},
+                       {hin->planck_levels, W * (L + 1)},
+                       {hin->surface_albedo, W},
+                       {hin->solar_mu, W},
+                       {hin->wavenumber_low, W},
+                       {hin->wavenumber_high, W},
+                       {hin->surface_emission, W},
+                       {hin->top_emission, W}};
+  double* const* outs_h = &hout->flux_up;
+  const size_t out_n[8] = {W * (L + 1), W * (L + 1), W * (L + 1), W * (L + 1),
+                           W * (L + 1), W, W, W};
+  size_t total = 0;
+  for (const auto& a : ins)
+    if (a.h) total += (a.n * sizeof(double) + 255) & ~size_t(255);
+  for (int i = 0; i < 8; ++i)
+    if (outs_h[i]) total += (out_n[i] * sizeof(double) + 255) & ~size_t(255);
+  char* dbuf = nullptr;
+  if (cudaMalloc(&dbuf, total) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "host-entry staging allocation of %zu B failed", total);
+  }
+  cudaStream_t s = nullptr;
+  adrt_inputs din{};
+  adrt_outputs dout{};
+  const double** din_p = &din.delta_tau;
+  double** dout_p = &dout.flux_up;
+  size_t off = 0;
+  rc = ADRT_OK;
+  for (int i = 0; i < 11 && rc == ADRT_OK; ++i) {
+    if (!ins[i].h) continue;
+    double* dp = reinterpret_cast<double*>(dbuf + off);
+    off += (ins[i].n * sizeof(double) + 255) & ~size_t(255);
+    if (cudaMemcpyAsync(dp, ins[i].h, ins[i].n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      rc = fail(ADRT_ERR_CUDA, "host-to-device copy failed");
+    din_p[i] = dp;
+  }
+  for (int i = 0; i < 8 && rc == ADRT_OK; ++i) {
+    if (!outs_h[i]) continue;
+    dout_p[i] = reinterpret_cast<double*>(dbuf + off);
+    off += (out_n[i] * sizeof(double) + 255) & ~size_t(255);
+  }
+  if (rc == ADRT_OK) rc = adrt_solve_batch(e, d, &din, &dout, s);
+  for (int i = 0; i < 8 && rc == ADRT_OK; ++i) {
+    if (!outs_h[i]) continue;
+    if (cudaMemcpyAsync(outs_h[i], dout_p[i], out_n[i] * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      rc = fail(ADRT_ERR_CUDA, "device-to-host copy failed");
+  }
+  cudaError_t se = cudaStreamSynchronize(s);
+  cudaFree(dbuf);
+  if (rc == ADRT_OK && se != cudaSuccess)
+    rc = fail(ADRT_ERR_CUDA, "solve failed: %s", cudaGetErrorString(se));
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,485 @@
+// adrt_solver.cuh -- the fused per-wavenumber adding-doubling solver.
+//
+// One thread group (a warp for N <= 16, four warps for N = 32) solves one
+// wavenumber column end to end:
+//
+//   prologue   Planck levels, delta-M scaled tau/omega, scaled cumulative tau
+//              (src/solver.cpp:385-514, src/planck.cpp:35-131)
+//   upward     for each layer from the bottom: phase matrices
+//              (src/phase_matrix.hpp:61-181), thin-layer init and doubling
+//              (src/doubling.hpp:29-230), then adding onto the composite of
+//              everything below it (src/adding.hpp:263-490).  The composite
+//              keeps only R_ab and the upward source with the lower boundary
+//              intensity folded in (T_ba I_bot + s_up), which is all the
+//              interface formulas of src/solver.cpp:24-73 read from rbase.
+//   downward   from the top: the downward intensity below layer l solves
+//              (I - R_l R_base) I_dn = T_l I_dn(above) + R_l U_base + s_dn_l, and
+//              I_up = R_base I_dn + U_base -- the same linear system the
+//              reference solves with its rtop composites (computeIdown /
+//              computeIup), without building rtop.
+//   fluxes     F = 2 pi sum w mu I, J (+ beam), divF (src/solver.cpp:605-700).
+//
+// Matrices are NP x NP (NP = N rounded up to 4, 8, 16 or 32; padded with the
+// identity/zero blocks, which the algebra keeps exact).  Each thread of the
+// group owns a TR x TC register tile of every matrix; products C = A B are
+// formed tile by tile from operands staged in shared memory (A column-major,
+// B row-major, so every operand load is one contiguous vector).  The
+// (I - R R)^{-1} right-solves are Gauss-Jordan eliminations on the register
+// tiles with column pivoting on the largest |entry| of the pivot row -- the
+// pivot rule of the reference's LU of the transpose (src/matrix.hpp:120-124)
+// -- selected with one warp-wide max-reduction per step.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "adrt_types.cuh"
+
+namespace adrt_dev {
+
+// ============================================================== geometry
+template <int NP_, typename Real_>
+struct Geo {
+  static constexpr int NP = NP_;
+  using Real = Real_;
+  static constexpr int G = (NP <= 16) ? 32 : 128;  // threads per wavenumber
+  static constexpr int RB = (G == 32) ? 4 : 8;      // thread-grid rows
+  static constexpr int CB = G / RB;                 // thread-grid cols
+  static constexpr int TR = (NP + RB - 1) / RB;     // tile rows per thread
+  static constexpr int TC = (NP + CB - 1) / CB;     // tile cols per thread
+  static constexpr int TE = TR * TC;
+  static constexpr int DIM = (RB * TR > CB * TC) ? RB * TR : CB * TC;
+  static constexpr int PAD = 16 / (int)sizeof(Real);  // rows stay 16-byte aligned
+  static constexpr int LD = DIM + PAD;
+  static constexpr int MAT = DIM * LD;                // Reals per smem matrix
+  static constexpr int NW = G / 32;                   // warps per group
+  // matvec lanes: warp 0 only; LPR lanes per row
+  static constexpr int LPR = (32 / NP < NP) ? (32 / NP) : NP;
+  static constexpr int KCH = NP / LPR;
+};
+
+// Shared-memory layout of one group (byte offsets).
+template <class Gm>
+struct SmemLayout {
+  using Real = typename Gm::Real;
+  static constexpr int NP = Gm::NP;
+  static constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+  // Real matrices
+  static constexpr size_t mats = 0;                                  // 4 x MAT Real
+  static constexpr size_t gj = align16(mats + 4 * sizeof(Real) * Gm::MAT);  // row/colA/colB x2, inv x2
+  static constexpr size_t vecs = align16(gj + sizeof(Real) * (6 * Gm::DIM + 4));
+  static constexpr int NVEC = 24;                                    // Real vectors of NP
+  static constexpr size_t dmats = align16(vecs + sizeof(Real) * NVEC * NP);  // Ppp, Ppm (double)
+  static constexpr size_t dvecs = align16(dmats + 2 * sizeof(double) * NP * NP);
+  static constexpr int NDVEC = 6;                                    // double vectors of NP
+  static constexpr size_t misc = align16(dvecs + sizeof(double) * NDVEC * NP);
+  static constexpr size_t bytes = align16(misc + 64);
+};
+
+// Vector slots (Real) inside SmemLayout::vecs.
+enum VecSlot {
+  V_Y0 = 0, V_Y1, V_Z0, V_Z1, V_SU0, V_SU1, V_SD0, V_SD1,
+  V_RU, V_RD, V_UB, V_SDN, V_SUP, V_ID, V_IU, V_RHS, V_TMP, V_TMP2, V_T, V_X
+};
+// Double vector slots inside SmemLayout::dvecs.
+enum DVecSlot { D_PP = 0, D_PM, D_COL, D_IBOT };
+
+// ============================================================== sync / reductions
+template <int G>
+__device__ __forceinline__ void gsync(int bar) {
+  if constexpr (G == 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(G) : "memory");
+  }
+}
+
+// Max of a 32-bit key over the group.  red: 2*NW unsigned in smem (double
+// buffered by `parity`).
+template <int G>
+__device__ __forceinline__ unsigned gmax_u32(unsigned key, unsigned* red, int parity, int bar) {
+  unsigned m = __reduce_max_sync(0xffffffffu, key);
+  if constexpr (G == 32) {
+    return m;
+  } else {
+    constexpr int NW = G / 32;
+    const int t = threadIdx.x % G;
+    if ((t & 31) == 0) red[parity * NW + (t >> 5)] = m;
+    gsync<G>(bar);
+    unsigned r = red[parity * NW];
+#pragma unroll
+    for (int i = 1; i < NW; ++i) r = max(r, red[parity * NW + i]);
+    return r;
+  }
+}
+
+// ============================================================== small helpers
+template <typename T>
+__device__ __forceinline__ T sel(const T* v, int idx, int n) {
+  T r = v[0];
+#pragma unroll
+  for (int i = 1; i < 8; ++i)
+    if (i < n && idx == i) r = v[i];
+  return r;
+}
+
+template <typename Real, int CNT>
+__device__ __forceinline__ void lds_vec(Real (&dst)[CNT], const Real* src) {
+  if constexpr (sizeof(Real) * CNT % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < CNT; i += 16 / (int)sizeof(Real)) {
+      if constexpr (sizeof(Real) == 8) {
+        double2 v = *reinterpret_cast<const double2*>(src + i);
+        dst[i] = v.x;
+        dst[i + 1] = v.y;
+      } else {
+        float4 v = *reinterpret_cast<const float4*>(src + i);
+        dst[i] = v.x;
+        dst[i + 1] = v.y;
+        dst[i + 2] = v.z;
+        dst[i + 3] = v.w;
+      }
+    }
+  } else if constexpr (sizeof(Real) == 4 && CNT == 2) {
+    float2 v = *reinterpret_cast<const float2*>(src);
+    dst[0] = v.x;
+    dst[1] = v.y;
+  } else {
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) dst[i] = src[i];
+  }
+}
+
+// ============================================================== tile algebra
+template <class Gm>
+struct TileOps {
+  using Real = typename Gm::Real;
+  static constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, G = Gm::G;
+  using Tile = Real[TR][TC];
+
+  int t, rb, cb, bar;
+
+  __device__ __forceinline__ TileOps(int tid, int bar_id)
+      : t(tid), rb(tid / Gm::CB), cb(tid % Gm::CB), bar(bar_id) {}
+
+  __device__ __forceinline__ int row(int a) const { return rb * TR + a; }
+  __device__ __forceinline__ int col(int b) const { return cb * TC + b; }
+  __device__ __forceinline__ bool valid(int a, int b) const { return row(a) < NP && col(b) < NP; }
+
+  __device__ __forceinline__ void sync() const { gsync<G>(bar); }
+
+  __device__ __forceinline__ void zero(Tile& X) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) X[a][b] = Real(0);
+  }
+  __device__ __forceinline__ void identity(Tile& X) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) X[a][b] = (row(a) == col(b)) ? Real(1) : Real(0);
+  }
+  __device__ __forceinline__ void copy(Tile& D, const Tile& S) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) D[a][b] = S[a][b];
+  }
+
+  // Row-major store of the tile into an smem matrix.
+  __device__ __forceinline__ void stage_rm(const Tile& X, Real* s) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+        if (valid(a, b)) s[row(a) * LD + col(b)] = X[a][b];
+  }
+  // Column-major store (s[c*LD + r] = X[r][c]).
+  __device__ __forceinline__ void stage_cm(const Tile& X, Real* s) const {
+#pragma unroll
+    for (int b = 0; b < TC; ++b)
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+        if (valid(a, b)) s[col(b) * LD + row(a)] = X[a][b];
+  }
+
+  // acc (+)= X Y, with X given column-major (sXT[k*LD + r] = X[r][k]) and Y row-major.
+  template <bool ACC>
+  __device__ __forceinline__ void gemm(Tile& acc, const Real* sXT, const Real* sY) const {
+    if constexpr (!ACC) zero(acc);
+    const Real* xp = sXT + rb * TR;
+    const Real* yp = sY + cb * TC;
+#pragma unroll 4
+    for (int k = 0; k < NP; ++k) {
+      Real xa[TR], yb[TC];
+      lds_vec<Real, TR>(xa, xp + k * LD);
+      lds_vec<Real, TC>(yb, yp + k * LD);
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+    }
+  }
+
+  // Tile to / from global memory in tile order (thread t owns TE contiguous Reals).
+  __device__ __forceinline__ void store_g(const Tile& X, Real* g) const {
+    Real* p = g + t * Gm::TE;
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) p[a * TC + b] = X[a][b];
+  }
+  __device__ __forceinline__ void load_g(Tile& X, const Real* g) const {
+    const Real* p = g + t * Gm::TE;
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) X[a][b] = p[a * TC + b];
+  }
+
+  // X = B A^{-1} by Gauss-Jordan column elimination with column pivoting on
+  // the pivot row (the pivot rule of LU with partial pivoting of A^T).
+  // A and B are destroyed.  The result is written column-major to sXT.
+  // Returns nonzero (on every thread) if an exactly-zero pivot was met.
+  __device__ __forceinline__ int gj_right_solve(Tile& A, Tile& B, Real* sXT, Real* gjbuf,
+                                                unsigned* red) const {
+    constexpr int DIM = Gm::DIM;
+    unsigned used = 0;
+    int q[TC];
+#pragma unroll
+    for (int b = 0; b < TC; ++b) q[b] = 0;
+    int singular = 0;
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const int par = k & 1;
+      Real* rowb = gjbuf + par * DIM;
+      Real* colA = gjbuf + 2 * DIM + par * DIM;
+      Real* colB = gjbuf + 4 * DIM + par * DIM;
+      Real* invb = gjbuf + 6 * DIM + par;
+      const int kr = k / TR, ka = k % TR;
+      // 1. pivot search over the unused columns of row k
+      unsigned key = 0;
+      if (rb == kr) {
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          const int c = col(b);
+          if (c < NP && !((used >> c) & 1u)) {
+            float f = fabsf(static_cast<float>(A[ka][b]));
+            unsigned bits = __float_as_uint(f);
+            unsigned kk = (bits & ~63u) | 32u | (unsigned)c;
+            key = max(key, kk);
+          }
+        }
+      }
+      key = gmax_u32<G>(key, red, par, bar);
+      const int p = (int)(key & 31u);
+      singular |= ((key >> 6) == 0u);
+      used |= 1u << p;
+      const int pb = p % TC;
+      // 2. publish row k, column p and 1/pivot
+      if (rb == kr) {
+#pragma unroll
+        for (int b = 0; b < TC; ++b)
+          if (col(b) < NP) rowb[col(b)] = A[ka][b];
+        if (cb == p / TC) {
+          Real piv = A[ka][0];
+#pragma unroll
+          for (int b = 1; b < TC; ++b)
+            if (pb == b) piv = A[ka][b];
+          *invb = Real(1) / piv;
+        }
+      }
+      if (cb == p / TC) {
+#pragma unroll
+        for (int a = 0; a < TR; ++a) {
+          Real va = A[a][0], vb = B[a][0];
+#pragma unroll
+          for (int b = 1; b < TC; ++b)
+            if (pb == b) {
+              va = A[a][b];
+              vb = B[a][b];
+            }
+          colA[row(a)] = va;
+          colB[row(a)] = vb;
+        }
+      }
+      sync();
+      // 3. eliminate
+      const Real inv = *invb;
+      Real cA[TR], cB[TR], rv[TC];
+      lds_vec<Real, TR>(cA, colA + rb * TR);
+      lds_vec<Real, TR>(cB, colB + rb * TR);
+      lds_vec<Real, TC>(rv, rowb + cb * TC);
+#pragma unroll
+      for (int a = 0; a < TR; ++a) {
+        cA[a] *= inv;
+        cB[a] *= inv;
+      }
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          if (col(b) == p) {
+            A[a][b] = cA[a];
+            B[a][b] = cB[a];
+          } else {
+            A[a][b] = fma(-cA[a], rv[b], A[a][b]);
+            B[a][b] = fma(-cB[a], rv[b], B[a][b]);
+          }
+        }
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+        if (col(b) == p) q[b] = k;
+    }
+    // write B A^{-1}: column c of the reduced B is column q[c] of the result
+#pragma unroll
+    for (int b = 0; b < TC; ++b)
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+        if (valid(a, b)) sXT[q[b] * LD + row(a)] = B[a][b];
+    return singular;
+  }
+};
+
+// ============================================================== matvec (warp 0)
+// y = X v for up to three vectors, X column-major in smem (sXT[k*LD+i] = X[i][k]).
+// Executed by warp 0 of the group; returns the sums on lanes with part == 0.
+template <class Gm, int NV>
+__device__ __forceinline__ void matvec_cm(const typename Gm::Real* sXT,
+                                          const typename Gm::Real* const (&v)[NV],
+                                          typename Gm::Real (&y)[NV], int lane) {
+  using Real = typename Gm::Real;
+  constexpr int NP = Gm::NP, LPR = Gm::LPR, KCH = Gm::KCH, LD = Gm::LD;
+  const int i = lane % NP, part = lane / NP;
+#pragma unroll
+  for (int n = 0; n < NV; ++n) y[n] = Real(0);
+  if (part < LPR) {
+#pragma unroll
+    for (int kk = 0; kk < KCH; ++kk) {
+      const int k = part * KCH + kk;
+      const Real x = sXT[k * LD + i];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) y[n] = fma(x, v[n][k], y[n]);
+    }
+  }
+#pragma unroll
+  for (int off = NP; off < NP * LPR; off <<= 1)
+#pragma unroll
+    for (int n = 0; n < NV; ++n) y[n] += __shfl_xor_sync(0xffffffffu, y[n], off);
+}
+
+// Same with X row-major (sX[i*LD+k]).
+template <class Gm, int NV>
+__device__ __forceinline__ void matvec_rm(const typename Gm::Real* sX,
+                                          const typename Gm::Real* const (&v)[NV],
+                                          typename Gm::Real (&y)[NV], int lane) {
+  using Real = typename Gm::Real;
+  constexpr int NP = Gm::NP, LPR = Gm::LPR, KCH = Gm::KCH, LD = Gm::LD;
+  const int i = lane % NP, part = lane / NP;
+#pragma unroll
+  for (int n = 0; n < NV; ++n) y[n] = Real(0);
+  if (part < LPR) {
+#pragma unroll
+    for (int kk = 0; kk < KCH; ++kk) {
+      const int k = part * KCH + kk;
+      const Real x = sX[i * LD + k];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) y[n] = fma(x, v[n][k], y[n]);
+    }
+  }
+#pragma unroll
+  for (int off = NP; off < NP * LPR; off <<= 1)
+#pragma unroll
+    for (int n = 0; n < NV; ++n) y[n] += __shfl_xor_sync(0xffffffffu, y[n], off);
+}
+
+// ============================================================== Planck (device)
+// Band-integrated Planck function, DisORT method: Simpson refinement for
+// narrow bands, small-v polynomial / large-v exponential series otherwise.
+// Same algorithm and constants as the reference (src/planck.cpp:13-131) so
+// that the level sources agree to round-off.
+__device__ __forceinline__ double planck_kernel_v(double v) { return v * v * v / (exp(v) - 1.0); }
+
+__device__ inline double planck_band(double wnumlo, double wnumhi, double temp) {
+  const double C2 = 1.438786, SIGMA = 5.67032E-8, VCUT = 1.5;
+  const double A1 = 1.0 / 3.0, A2 = -1.0 / 8.0, A3 = 1.0 / 60.0, A4 = -1.0 / 5040.0;
+  const double A5 = 1.0 / 272160.0, A6 = -1.0 / 13305600.0;
+  if (temp < 0.0 || wnumhi < wnumlo || wnumlo < 0.0) return -1.0;
+  if (temp < 1.e-4) return 0.0;
+  if (wnumhi == wnumlo) {
+    double arg = exp(-C2 * wnumhi / temp);
+    return 1.1911e-8 * wnumhi * wnumhi * wnumhi * arg / (1.0 - arg);
+  }
+  const double vmax = 709.782712893384;  // log(DBL_MAX)
+  const double sigdpi = SIGMA / kPi;
+  const double conc = 15.0 / pow(kPi, 4.0);
+  const double v0 = C2 * wnumlo / temp, v1 = C2 * wnumhi / temp;
+  if (v0 > 2.220446049250313e-16 && v1 < vmax && (wnumhi - wnumlo) / wnumhi < 1.e-2) {
+    const double hh = v1 - v0;
+    double oldval = 0.0;
+    const double val0 = planck_kernel_v(v0) + planck_kernel_v(v1);
+    for (int n = 1; n <= 10; ++n) {
+      const double del = hh / (2.0 * n);
+      double val = val0;
+      for (int k = 1; k <= 2 * n - 1; ++k) val += 2.0 * (1 + k % 2) * planck_kernel_v(v0 + k * del);
+      val *= del * A1;
+      if (fabs((val - oldval) / val) <= 1.e-6) return sigdpi * pow(temp, 4.0) * conc * val;
+      oldval = val;
+    }
+    return sigdpi * pow(temp, 4.0) * conc * oldval;
+  }
+  const double vcp[7] = {10.25, 5.7, 3.9, 2.9, 2.3, 1.9, 0.0};
+  double v[2] = {v0, v1}, p[2] = {0.0, 0.0}, d[2] = {0.0, 0.0};
+  int smallv = 0;
+  for (int i = 0; i < 2; ++i) {
+    if (v[i] < VCUT) {
+      smallv++;
+      const double vsq = v[i] * v[i];
+      p[i] = conc * vsq * v[i] * (A1 + v[i] * (A2 + v[i] * (A3 + vsq * (A4 + vsq * (A5 + vsq * A6)))));
+    } else {
+      int mmax = 1;
+      while (v[i] < vcp[mmax - 1]) mmax++;
+      const double ex = exp(-v[i]);
+      double exm = 1.0;
+      double s = 0.0;
+      for (int m = 1; m <= mmax; ++m) {
+        const double mv = m * v[i];
+        exm *= ex;
+        s += exm * (6.0 + mv * (6.0 + mv * (3.0 + mv))) / (double)(m * m * m * m);
+      }
+      d[i] = s * conc;
+    }
+  }
+  double ans;
+  if (smallv == 2)
+    ans = p[1] - p[0];
+  else if (smallv == 1)
+    ans = 1.0 - p[0] - d[1];
+  else
+    ans = d[0] - d[1];
+  ans *= sigdpi * pow(temp, 4.0);
+  return (ans == 0.0) ? 0.0 : ans;
+}
+
+// Extra doublings from omega (src/doubling.hpp:20-26).
+__device__ __forceinline__ int ipow0(double omega) {
+  return omega < 0.01 ? 4 : (omega < 0.1 ? 10 : 16);
+}
+
+// nn = max(1, trunc(ln tau / ln 2) + ipow0) (src/doubling.hpp:107-109).  An
+// exact power of two takes its exponent directly, so that the truncation
+// agrees with the host library on the inputs where ln(tau)/ln(2) is integral.
+__device__ __forceinline__ int num_doublings(double tau, double omega) {
+  int e;
+  const double m = frexp(tau, &e);
+  int lg;
+  if (m == 0.5)
+    lg = e - 1;
+  else
+    lg = (int)(log(tau) / log(2.0));
+  const int nn = lg + ipow0(omega);
+  return nn < 1 ? 1 : nn;
+}
+
+}  // namespace adrt_dev

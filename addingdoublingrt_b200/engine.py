@@ -1,0 +1,117 @@
+"""Python handle on the native engine.
+
+`Engine` owns one adrt_engine (device work buffers) and solves batches held
+either in host numpy arrays (`solve_host`, the adrt_solve_batch_host entry)
+or in CUDA tensors (`solve_device`, the stream-ordered adrt_solve_batch
+entry).  PyTorch is used only to hold device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi, _lib
+from .workloads import Batch
+
+
+class Engine:
+    def __init__(self, device: int = -1, max_workspace_bytes: int = 0):
+        self.lib = _lib.load()
+        opts = _abi.EngineOpts(device=device, max_workspace_bytes=max_workspace_bytes)
+        h = C.c_void_p()
+        _lib.check(self.lib.adrt_engine_create(C.byref(opts), C.byref(h)))
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.adrt_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, desc: _abi.BatchDesc) -> None:
+        _lib.check(self.lib.adrt_engine_reserve(self.handle, C.byref(desc)))
+
+    def workspace_bytes(self) -> int:
+        v = C.c_size_t()
+        _lib.check(self.lib.adrt_engine_workspace_bytes(self.handle, C.byref(v)))
+        return int(v.value)
+
+    def read_status(self) -> int:
+        v = C.c_int()
+        _lib.check(self.lib.adrt_engine_read_status(self.handle, C.byref(v)))
+        return int(v.value)
+
+    # ------------------------------------------------------------------ host entry
+    def solve_host(self, batch: Batch, which=_abi.OUTPUT_FIELDS, out: dict | None = None) -> dict:
+        """adrt_solve_batch_host: host arrays in, host arrays out (synchronous)."""
+        out = batch.alloc_outputs(which) if out is None else out
+        ins = batch.inputs_struct()
+        outs = Batch.outputs_struct(out)
+        _lib.check(self.lib.adrt_solve_batch_host(self.handle, C.byref(batch.desc),
+                                                  C.byref(ins), C.byref(outs)))
+        return out
+
+    # ------------------------------------------------------------------ device entry
+    def solve_device(self, desc: _abi.BatchDesc, dev_inputs: dict, dev_outputs: dict,
+                     stream=None) -> None:
+        """adrt_solve_batch on CUDA tensors (float64, contiguous); stream ordered."""
+        ins = _abi.Inputs()
+        for f in _abi.INPUT_FIELDS:
+            t = dev_inputs.get(f)
+            setattr(ins, f, _ptr(t))
+        outs = _abi.Outputs()
+        for f in _abi.OUTPUT_FIELDS:
+            setattr(outs, f, _ptr(dev_outputs.get(f)))
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        _lib.check(self.lib.adrt_solve_batch(self.handle, C.byref(desc), C.byref(ins),
+                                             C.byref(outs), s))
+
+    def solve_uneven(self, columns: list, stream=None) -> None:
+        """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
+        arr = (_abi.ColumnDesc * len(columns))()
+        for i, (desc, di, do) in enumerate(columns):
+            arr[i].desc = desc
+            for f in _abi.INPUT_FIELDS:
+                setattr(arr[i].inp, f, _ptr(di.get(f)))
+            for f in _abi.OUTPUT_FIELDS:
+                setattr(arr[i].out, f, _ptr(do.get(f)))
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        _lib.check(self.lib.adrt_solve_batch_uneven(self.handle, arr, len(columns), s))
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data
+    if not t.is_contiguous():
+        raise ValueError("device arrays must be contiguous")
+    import torch
+    if t.dtype != torch.float64:
+        raise TypeError("device arrays must be float64")
+    return t.data_ptr()
+
+
+def to_device(batch: Batch, device="cuda") -> dict:
+    import torch
+    return {k: torch.from_numpy(v).to(device) for k, v in batch.arrays.items()}
+
+
+def alloc_device_outputs(batch: Batch, which=_abi.OUTPUT_FIELDS, device="cuda") -> dict:
+    import torch
+    nint = batch.L + 1
+    out = {}
+    for f in which:
+        n = batch.W * nint if f in _abi.INTERFACE_OUTPUTS else batch.W
+        out[f] = torch.zeros(n, dtype=torch.float64, device=device)
+    return out

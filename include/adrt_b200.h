@@ -1,0 +1,199 @@
+/*
+ * adrt_b200.h -- C ABI of the B200 adding-doubling radiative-transfer engine.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point returns
+ * an int status (ADRT_OK == 0, negative on error); a human-readable detail of
+ * the last error on the calling thread is returned by adrt_last_status_detail().
+ *
+ * What each entry point replaces in the reference (NewStrangeWorlds/
+ * AddingDoublingRT):
+ *
+ *   adrt_solve_batch         adrt::cuda::solveBatch(const BatchConfig&, const DeviceData&,
+ *                            cudaStream_t)                         src_cuda/cuda_solver.cuh:77-80
+ *                            (device buffers, stream ordered, no host sync).  Outputs are
+ *                            per interface (src/adding_doubling.hpp:32-50), not TOA only.
+ *   adrt_solve_batch_host    adrt::cuda::solveBatchHost(...)      src_cuda/cuda_solver.cuh:85-98
+ *                            (host buffers; copies in, solves, copies out, synchronises).
+ *   adrt_solve_column        adrt::solve(const ADConfig&)          src/adding_doubling.hpp:258
+ *                            (one column, host buffers, RTOutput layout).
+ *   adrt_validate_column     ADConfig::validate()                  src/adding_doubling.hpp:123-174
+ *   adrt_engine_create/...   SolverWorkspaceGPU                    src_cuda/cuda_solver.cuh:140-156
+ *                            (the engine owns every device work buffer; nothing is
+ *                            allocated inside a solve once adrt_engine_reserve succeeded).
+ *
+ * Array layouts (all row-major, wavenumber-major, TOA = layer/level 0 unless
+ * index_from_bottom is set, exactly as the reference's DeviceData SoA layout
+ * "array[wav * stride + layer_or_level]", src_cuda/cuda_solver.cuh:44):
+ *   delta_tau, single_scat_albedo          [W * L]
+ *   phase_moments                          see adrt_moment_layout
+ *   temperature                            [L+1] shared, or [W * (L+1)]
+ *   planck_levels                          [W * (L+1)]
+ *   per-wavenumber scalars (optional)      [W]
+ *   outputs flux_up/flux_down/flux_direct/
+ *           mean_intensity/flux_divergence [W * (L+1)]   (NULL = not written)
+ *   outputs toa_flux_up/toa_flux_down/
+ *           boa_flux_direct                [W]           (reference DeviceData outputs)
+ */
+#ifndef ADRT_B200_H_
+#define ADRT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+enum adrt_status {
+  ADRT_OK = 0,
+  ADRT_ERR_INVALID_ARGUMENT = -1, /* ADConfig::validate() failure, bad sizes / pointers */
+  ADRT_ERR_UNSUPPORTED = -2,      /* e.g. num_quadrature outside 2..32 on the GPU path */
+  ADRT_ERR_CUDA = -3,             /* a CUDA runtime call failed */
+  ADRT_ERR_OUT_OF_MEMORY = -4,    /* device work-buffer allocation failed */
+  ADRT_ERR_WORKSPACE = -5,        /* the reserved work buffer is too small (capture mode) */
+  ADRT_ERR_NUMERICAL = -6         /* device status word reported a numerical fault */
+};
+
+/* Device status word bits (adrt_engine_read_status). */
+enum adrt_device_flag {
+  ADRT_FLAG_SINGULAR_PIVOT = 1, /* an LU pivot was exactly zero (reference: silent inv=0) */
+  ADRT_FLAG_NONFINITE = 2,      /* a non-finite flux was produced */
+  ADRT_FLAG_BAD_INPUT = 4       /* tau < 0, omega outside [0,1], T < 0 seen on the device */
+};
+
+/* ---------------------------------------------------------------- config */
+enum adrt_precision {
+  ADRT_PRECISION_FP64 = 0, /* every operation in FP64 (the plain GPU form) */
+  ADRT_PRECISION_MIXED = 1 /* FP32 products, FP64 where conditioning needs it */
+};
+
+enum adrt_moment_layout {
+  ADRT_MOMENTS_SHARED = 0,        /* [L * M]: same for every wavenumber (reference
+                                     DeviceData::phase_moments_shared = true) */
+  ADRT_MOMENTS_PER_WAVENUMBER = 1,/* [W * M]: one set per wavenumber, same for every layer */
+  ADRT_MOMENTS_PER_LAYER = 2      /* [W * L * M]: per wavenumber and layer (reference
+                                     phase_moments_shared = false) */
+};
+
+/* Scalars shared by every wavenumber of a batch.  Field meanings follow
+ * adrt::ADConfig (src/adding_doubling.hpp:63-94) and adrt::cuda::BatchConfig
+ * (src_cuda/cuda_solver.cuh:18-40). */
+typedef struct adrt_batch_desc {
+  int num_wavenumbers; /* W >= 1 */
+  int num_layers;      /* L >= 1 */
+  int num_quadrature;  /* N, 2..32 */
+  int num_moments;     /* M >= 1 Legendre moments per set */
+  int moment_layout;   /* enum adrt_moment_layout */
+  int precision;       /* enum adrt_precision */
+
+  int use_thermal_emission;   /* Planck levels from temperature (band-integrated) */
+  int use_delta_m;            /* delta-M scaling (truncation fraction = chi[2N] when M > 2N) */
+  int use_diffusion_lower_bc; /* diffusion-approximation lower boundary */
+  int index_from_bottom;      /* user arrays indexed BOA (0) -> TOA */
+  int temperature_per_wavenumber; /* temperature is [W*(L+1)] instead of shared [L+1] */
+
+  double surface_albedo;      /* used when inputs.surface_albedo == NULL */
+  double surface_emission;    /* raw, when !use_thermal_emission and inputs.surface_emission == NULL */
+  double surface_temperature; /* >= 0 with thermal: surface emits B(T_s) */
+  double top_emission;        /* raw, when !use_thermal_emission and inputs.top_emission == NULL */
+  double top_temperature;     /* >= 0 with thermal: TOA downwelling B(T_top) */
+  double solar_flux;          /* F0 */
+  double solar_mu;            /* used when inputs.solar_mu == NULL */
+  double wavenumber_low;      /* band, used when inputs.wavenumber_low == NULL */
+  double wavenumber_high;
+  double spectrum_scaling;    /* applied to toa_flux_up only (reference BatchConfig) */
+} adrt_batch_desc;
+
+/* Inputs (device pointers for adrt_solve_batch, host pointers for the
+ * *_host entry points).  FP64 throughout so that near-conservative albedos
+ * (1 - omega down to 1e-7) are represented exactly. */
+typedef struct adrt_inputs {
+  const double* delta_tau;          /* [W*L] */
+  const double* single_scat_albedo; /* [W*L] */
+  const double* phase_moments;      /* see moment_layout */
+  const double* temperature;        /* [L+1] or [W*(L+1)]; thermal only */
+  const double* planck_levels;      /* [W*(L+1)] or NULL; non-thermal sources */
+  const double* surface_albedo;     /* [W] or NULL */
+  const double* solar_mu;           /* [W] or NULL */
+  const double* wavenumber_low;     /* [W] or NULL */
+  const double* wavenumber_high;    /* [W] or NULL */
+  const double* surface_emission;   /* [W] or NULL */
+  const double* top_emission;       /* [W] or NULL */
+} adrt_inputs;
+
+typedef struct adrt_outputs {
+  double* flux_up;         /* [W*(L+1)] diffuse upward flux per interface */
+  double* flux_down;       /* [W*(L+1)] diffuse downward flux */
+  double* flux_direct;     /* [W*(L+1)] attenuated direct beam */
+  double* mean_intensity;  /* [W*(L+1)] J including the direct beam */
+  double* flux_divergence; /* [W*(L+1)] 4 pi (1 - omega) (J - B) */
+  double* toa_flux_up;     /* [W] flux_up[0] * spectrum_scaling */
+  double* toa_flux_down;   /* [W] flux_down[0] */
+  double* boa_flux_direct; /* [W] flux_direct[L] */
+} adrt_outputs;
+
+/* ---------------------------------------------------------------- engine */
+typedef struct adrt_engine adrt_engine;
+
+typedef struct adrt_engine_opts {
+  int device;                  /* CUDA device ordinal; -1 = current device */
+  size_t max_workspace_bytes;  /* 0 = no limit on the device work buffer */
+} adrt_engine_opts;
+
+int adrt_engine_create(const adrt_engine_opts* opts, adrt_engine** out);
+int adrt_engine_destroy(adrt_engine* engine);
+
+/* Pre-size the engine's device work buffer for batches up to this shape, so
+ * that later adrt_solve_batch calls allocate nothing (and can be captured in
+ * a CUDA graph). */
+int adrt_engine_reserve(adrt_engine* engine, const adrt_batch_desc* desc);
+
+/* Bytes of device work buffer the engine currently holds. */
+int adrt_engine_workspace_bytes(const adrt_engine* engine, size_t* bytes);
+
+/* Synchronise the engine's last stream and read (and clear) the device status
+ * word (enum adrt_device_flag bits). */
+int adrt_engine_read_status(adrt_engine* engine, int* flags);
+
+/* ---------------------------------------------------------------- solves */
+
+/* Batched solve, device buffers, stream ordered; returns after enqueueing. */
+int adrt_solve_batch(adrt_engine* engine, const adrt_batch_desc* desc,
+                     const adrt_inputs* in, const adrt_outputs* out, void* cuda_stream);
+
+/* Batched solve from host buffers: host->device copies, solve, device->host
+ * copies, stream synchronised before return. */
+int adrt_solve_batch_host(adrt_engine* engine, const adrt_batch_desc* desc,
+                          const adrt_inputs* host_in, const adrt_outputs* host_out);
+
+/* Validate a batch description and (host) inputs with the rules of
+ * ADConfig::validate() (src/adding_doubling.hpp:123-174) applied to every
+ * wavenumber.  Returns ADRT_ERR_INVALID_ARGUMENT with a detail message. */
+int adrt_validate_batch(const adrt_batch_desc* desc, const adrt_inputs* host_in);
+
+/* ------------------------------------------------------- uneven batches */
+
+/* One column of an uneven batch (reference: several solveBatch calls).
+ * Every pointer is a device pointer; arrays follow adrt_inputs / adrt_outputs
+ * for this column's own W, L, N and M. */
+typedef struct adrt_column_desc {
+  adrt_batch_desc desc;
+  adrt_inputs in;
+  adrt_outputs out;
+} adrt_column_desc;
+
+/* Solve many columns of different W, L, N in ONE launch of the persistent
+ * solver kernel.  The column table is copied to the device by the engine. */
+int adrt_solve_batch_uneven(adrt_engine* engine, const adrt_column_desc* cols, int ncols,
+                            void* cuda_stream);
+
+/* --------------------------------------------------------------- errors */
+const char* adrt_last_status_detail(void);
+const char* adrt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ADRT_B200_H_ */

@@ -1,0 +1,153 @@
+"""TEST INFRASTRUCTURE: Python access to the two CPU oracles.
+
+* `liboracle.so`  -- the C restatement in adrt_oracle.c (the parity checker).
+* `_ref/libadrt_ref.so` -- the reference's own CPU solver (src/solver.cpp and
+  friends, compiled unmodified against the project-written Eigen subset);
+  used to generate the golden vectors and as the timed CPU baseline.
+
+Only tests/, bench.py's CPU-baseline leg and __graft_entry__.smoke() import
+this module.  Nothing in the engine does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+from addingdoublingrt_b200 import _abi
+from addingdoublingrt_b200.workloads import Batch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lock = threading.Lock()
+_libs = {}
+
+
+def _make(target: str) -> None:
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+def oracle_lib(fma: bool = False) -> C.CDLL:
+    """The C restatement, built on first use if absent (gcc only).  `fma=True`
+    gives the same code compiled with FMA contraction (sensitivity probe)."""
+    key = "oracle_fma" if fma else "oracle"
+    name = "liboracle_fma.so" if fma else "liboracle.so"
+    with _lock:
+        if key not in _libs:
+            path = os.path.join(HERE, name)
+            if not os.path.exists(path):
+                _make(name)
+            lib = C.CDLL(path)
+            sig = [C.POINTER(_abi.BatchDesc), C.POINTER(_abi.Inputs), C.POINTER(_abi.Outputs)]
+            lib.oracle_solve_batch.argtypes = sig + [C.c_int]
+            lib.oracle_solve_batch_range.argtypes = sig + [C.c_int, C.c_int, C.c_int]
+            lib.oracle_last_error.restype = C.c_char_p
+            lib.oracle_planck.restype = C.c_double
+            lib.oracle_planck.argtypes = [C.c_double] * 3
+            lib.oracle_planck_deriv.restype = C.c_double
+            lib.oracle_planck_deriv.argtypes = [C.c_double] * 3
+            lib.oracle_gauss_legendre.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+            lib.oracle_num_doublings.argtypes = [C.c_double, C.c_double]
+            lib.oracle_ipow0.argtypes = [C.c_double]
+            lib.oracle_flops_batch.restype = C.c_double
+            lib.oracle_flops_batch.argtypes = [C.POINTER(_abi.BatchDesc),
+                                               C.POINTER(_abi.Inputs), C.c_int, C.c_int]
+            _libs[key] = lib
+        return _libs[key]
+
+
+def ref_available(strict: bool = False) -> bool:
+    name = "libadrt_ref_strict.so" if strict else "libadrt_ref.so"
+    return os.path.exists(os.path.join(HERE, "_ref", name))
+
+
+def ref_lib(strict: bool = False) -> C.CDLL:
+    """The reference's own solver (oracle/_ref); raises if it was not built.
+    `strict=True`: the build without FMA contraction (golden vectors)."""
+    key = "ref_strict" if strict else "ref"
+    name = "libadrt_ref_strict.so" if strict else "libadrt_ref.so"
+    with _lock:
+        if key not in _libs:
+            path = os.path.join(HERE, "_ref", name)
+            if not os.path.exists(path):
+                raise FileNotFoundError(
+                    f"{path} missing: build it with `make -C oracle ref` where the "
+                    "reference sources are present")
+            lib = C.CDLL(path)
+            sig = [C.POINTER(_abi.BatchDesc), C.POINTER(_abi.Inputs), C.POINTER(_abi.Outputs)]
+            lib.ref_solve_batch.argtypes = sig + [C.c_int]
+            lib.ref_solve_batch_range.argtypes = sig + [C.c_int, C.c_int, C.c_int]
+            lib.ref_last_error.restype = C.c_char_p
+            lib.ref_planck.restype = C.c_double
+            lib.ref_planck.argtypes = [C.c_double] * 3
+            lib.ref_gauss_legendre.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+            lib.ref_solve_column_jacobian.argtypes = [
+                C.POINTER(_abi.BatchDesc), C.POINTER(_abi.Inputs), C.c_int,
+                C.POINTER(_abi.Outputs)] + [C.c_void_p] * 4
+            _libs[key] = lib
+        return _libs[key]
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _run(fn, errfn, batch: Batch, nthreads: int, which, w0=None, w1=None) -> dict:
+    out = batch.alloc_outputs(which)
+    d = batch.desc
+    ins = batch.inputs_struct()
+    outs = Batch.outputs_struct(out)
+    if w0 is None:
+        rc = fn(C.byref(d), C.byref(ins), C.byref(outs), int(nthreads))
+    else:
+        rc = fn(C.byref(d), C.byref(ins), C.byref(outs), int(w0), int(w1), int(nthreads))
+    if rc != 0:
+        raise OracleError(errfn().decode())
+    return out
+
+
+def solve_oracle(batch: Batch, nthreads: int = 0, which=_abi.OUTPUT_FIELDS,
+                 fma: bool = False) -> dict:
+    """All outputs of `batch` from the C restatement."""
+    lib = oracle_lib(fma)
+    return _run(lib.oracle_solve_batch, lib.oracle_last_error, batch,
+                nthreads or os.cpu_count() or 1, which)
+
+
+def solve_reference(batch: Batch, nthreads: int = 0, which=_abi.OUTPUT_FIELDS,
+                    strict: bool = False) -> dict:
+    """All outputs of `batch` from the reference's own solver (oracle/_ref)."""
+    lib = ref_lib(strict)
+    return _run(lib.ref_solve_batch, lib.ref_last_error, batch,
+                nthreads or os.cpu_count() or 1, which)
+
+
+def flops(batch: Batch, w0: int = 0, w1: int | None = None) -> float:
+    """Algorithmic flops of wavenumbers [w0, w1) (reference branch counting)."""
+    lib = oracle_lib()
+    ins = batch.inputs_struct()
+    return lib.oracle_flops_batch(C.byref(batch.desc), C.byref(ins), int(w0),
+                                  int(batch.W if w1 is None else w1))
+
+
+def rel_error(x: np.ndarray, ref: np.ndarray) -> float:
+    """max |x - ref| / max(|ref|, 1e-12 max|ref|) over all elements."""
+    x = np.asarray(x, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    scale = np.max(np.abs(ref)) if ref.size else 0.0
+    if scale == 0.0:
+        return float(np.max(np.abs(x - ref))) if x.size else 0.0
+    den = np.maximum(np.abs(ref), 1e-12 * scale)
+    return float(np.max(np.abs(x - ref) / den))
+
+
+def norm_error(x: np.ndarray, ref: np.ndarray, per: int) -> float:
+    """max |x - ref| normalised by each wavenumber's largest |ref| (rows of `per`)."""
+    x = np.asarray(x, dtype=np.float64).reshape(-1, per)
+    ref = np.asarray(ref, dtype=np.float64).reshape(-1, per)
+    scale = np.max(np.abs(ref), axis=1, keepdims=True)
+    scale[scale == 0.0] = 1.0
+    return float(np.max(np.abs(x - ref) / scale))
