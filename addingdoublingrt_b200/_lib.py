@@ -27,6 +27,7 @@ EXPORTS = (
     "adrt_solve_batch_uneven",
     "adrt_last_status_detail",
     "adrt_version",
+    "adrt_probe_fma_tflops",
 )
 
 
@@ -61,6 +62,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                                 C.c_void_p]
         lib.adrt_last_status_detail.restype = C.c_char_p
         lib.adrt_version.restype = C.c_char_p
+        lib.adrt_probe_fma_tflops.argtypes = [P(C.c_double), P(C.c_double)]
         _lib = lib
         return lib
 

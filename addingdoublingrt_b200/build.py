@@ -18,7 +18,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libadrt_b200.so")
 
-SOURCES = ["adrt_engine.cu"]
+SOURCES = ["adrt_engine.cu", "adrt_probe.cu"]
 HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh"]
 
 NVCC_FLAGS = [

@@ -337,7 +337,7 @@ __device__ void solve_one(const ColumnDev& C, int w, char* slot, int lmax, const
     const int u = src_layer(l);
     double tau = C.dtau[(size_t)w * nL + u];
     double om = C.ssa[(size_t)w * nL + u];
-    if (tau < 0.0 || om < 0.0 || om > 1.0) bad = 1;
+    if (!(tau >= 0.0 && tau < 1e300) || !(om >= 0.0 && om <= 1.0)) bad = 1;
     lvOmu[l] = om;
     if (om > 0.0 && tau > 0.0 && C.delta_m && M > 2 * N) {
       const double f = chi_of(l)[2 * N];

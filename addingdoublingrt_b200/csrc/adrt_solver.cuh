@@ -470,7 +470,11 @@ __device__ __forceinline__ int ipow0(double omega) {
 // nn = max(1, trunc(ln tau / ln 2) + ipow0) (src/doubling.hpp:107-109).  An
 // exact power of two takes its exponent directly, so that the truncation
 // agrees with the host library on the inputs where ln(tau)/ln(2) is integral.
+// Non-finite or absurdly large optical depths are clamped to 64 doublings so a
+// bad input can never run the loop unbounded (the prologue flags it).
+constexpr int kMaxDoublings = 64;
 __device__ __forceinline__ int num_doublings(double tau, double omega) {
+  if (!(tau < 1e300)) return kMaxDoublings;
   int e;
   const double m = frexp(tau, &e);
   int lg;
@@ -479,7 +483,7 @@ __device__ __forceinline__ int num_doublings(double tau, double omega) {
   else
     lg = (int)(log(tau) / log(2.0));
   const int nn = lg + ipow0(omega);
-  return nn < 1 ? 1 : nn;
+  return nn < 1 ? 1 : (nn > kMaxDoublings ? kMaxDoublings : nn);
 }
 
 }  // namespace adrt_dev

@@ -1,0 +1,331 @@
+"""Benchmark: wavenumber-solves/s of the batched adding-doubling solve.
+
+Workload: 100,000 wavenumbers x 100 layers, N=16, thermal + solar, per-
+wavenumber double Henyey-Greenstein moments (32), band-integrated Planck
+levels over 500-3000 cm^-1 (seeded synthetic inputs, `workloads.config2`).
+
+    python bench.py [--gpus N --steps K --warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference      # the reference's CPU solver on the host cores
+
+One step = one solve of the whole batch with inputs resident in HBM (inputs
+of 190 MB exceed the 126 MB L2, so no flush is needed between steps).  `e2e`
+times the host entry point adrt_solve_batch_host (pinned host arrays in,
+host arrays out, host<->device copies inside the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from addingdoublingrt_b200 import _abi, workloads  # noqa: E402
+
+METRIC = "wavenumber-solves/s N=16 L=100: FP64 vs mixed @1e-6 rel err; adjoint/fwd time"
+WORKLOAD = "config2: W=100000 wavenumbers x L=100 layers, N=16, M=32 per-wavenumber dHG moments, thermal+solar"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    p.add_argument("--wavenumbers", type=int, default=100_000)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-check", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(batch, seconds=12.0, threads=None):
+    """The reference's own CPU solver (oracle/_ref, compiled from the reference
+    sources) on the host cores, on a bounded sample of the same workload."""
+    from oracle import oracle
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    rng = np.random.default_rng(0)
+    n = max(threads * 2, 64)
+    rate = None
+    while True:
+        idx = np.sort(rng.choice(batch.W, size=min(n, batch.W), replace=False))
+        sub = batch.subset(idx)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            oracle.solve_reference(sub, threads)
+        else:
+            oracle.solve_oracle(sub, threads)
+        dt = time.perf_counter() - t0
+        rate = sub.W / dt
+        if dt >= seconds or n >= batch.W:
+            break
+        n = int(min(batch.W, max(n * 2, rate * seconds * 1.1)))
+    return {"value": rate, "unit": "wavenumber-solves/s", "cores": threads, "kind": kind,
+            "sample": f"{sub.W} random wavenumbers of the same workload ({dt:.1f} s on "
+                      f"{threads} threads)"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    batch = workloads.config2(W=args.wavenumbers)
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    rng = np.random.default_rng(1)
+    sample = max(4 * threads, 256)
+    solve = (lambda b: oracle.solve_reference(b, threads)) if kind == "reference" else \
+        (lambda b: oracle.solve_oracle(b, threads))
+    subs = [batch.subset(np.sort(rng.choice(batch.W, sample, replace=False)))
+            for _ in range(args.warmup + args.steps)]
+    for i in range(args.warmup):
+        solve(subs[i])
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        solve(subs[args.warmup + i])
+    dt = time.perf_counter() - t0
+    rate = sample * args.steps / dt
+    line = {
+        "metric": METRIC, "value": rate, "unit": "wavenumber-solves/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample_per_step": sample},
+        "cpu_baseline": {"value": rate, "unit": "wavenumber-solves/s", "cores": threads,
+                         "kind": kind,
+                         "sample": f"{sample} random wavenumbers per step, {threads} threads"},
+        "e2e": {"value": rate, "unit": "wavenumber-solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- engine arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from addingdoublingrt_b200.engine import Engine, alloc_device_outputs, to_device
+    from addingdoublingrt_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    eng = Engine(device=local)
+    results = {}
+    precisions = ["fp64", "mixed"]
+    for pname in precisions:
+        prec = _abi.PRECISION_FP64 if pname == "fp64" else _abi.PRECISION_MIXED
+        # weak scaling: every rank solves its own batch of the full size
+        b = workloads.config2(W=args.wavenumbers, seed=2 + rank, precision=prec)
+        di = to_device(b)
+        do = alloc_device_outputs(b, which=_abi.INTERFACE_OUTPUTS)
+        eng.reserve(b.desc)
+        stream = torch.cuda.current_stream()
+        for _ in range(args.warmup):
+            eng.solve_device(b.desc, di, do, stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                eng.solve_device(b.desc, di, do, stream)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        status = eng.read_status()
+        results[pname] = {"ms": ms, "clocks": clk.summary(), "status": status,
+                          "batch": b, "out": do}
+
+    # accuracy against the oracle on a sample (rank 0)
+    acc = {}
+    if rank == 0 and not args.no_check:
+        from oracle import oracle
+        idx = np.arange(0, args.wavenumbers, max(1, args.wavenumbers // 200))
+        ref = oracle.solve_oracle(results["fp64"]["batch"].subset(idx), os.cpu_count() or 1,
+                                  which=_abi.INTERFACE_OUTPUTS)
+        L = results["fp64"]["batch"].L
+        for pname in precisions:
+            out = {k: v.view(-1, L + 1)[torch.as_tensor(idx, device="cuda")].cpu().numpy().ravel()
+                   for k, v in results[pname]["out"].items()}
+            acc[pname] = {k: {"elementwise": oracle.rel_error(out[k], ref[k]),
+                              "normalized": oracle.norm_error(out[k], ref[k], L + 1)}
+                          for k in ("flux_up", "flux_down", "flux_direct", "mean_intensity")}
+
+    # e2e through the host entry point (pinned host buffers, copies timed)
+    pname = args.precision
+    if pname == "auto":
+        pname = "mixed" if acc and max(v["normalized"] for v in acc["mixed"].values()) <= 1e-6 else "fp64"
+    b = results[pname]["batch"]
+    hb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc))
+    pinned = {}
+    for k, v in b.arrays.items():
+        t = torch.from_numpy(v).pin_memory()
+        pinned[k] = t
+        hb.arrays[k] = t.numpy()
+    hout = {k: torch.zeros(b.W * (b.L + 1), dtype=torch.float64).pin_memory().numpy()
+            for k in _abi.INTERFACE_OUTPUTS}
+    eng.solve_host(hb, out=hout)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.solve_host(hb, out=hout)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = int(sum(v.nbytes for v in hb.arrays.values()))
+    d2h = int(sum(v.nbytes for v in hout.values()))
+
+    if rank == 0:
+        from oracle import oracle
+        fl = oracle.flops(b)  # algorithmic flops of the whole batch
+        ms = results[pname]["ms"]
+        peaks = measured_peaks(_lib.load())
+        pk = peaks["fp64_tflops"] if pname == "fp64" else peaks["fp32_tflops"]
+        achieved = fl / (ms * 1e-3) / 1e12
+        roof = {"bound": "fp64" if pname == "fp64" else "fp32", "achieved": achieved,
+                "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk if pk else None,
+                "traffic": None, "peak_source": peaks["source"],
+                "flops_per_launch": fl}
+        line = {
+            "metric": METRIC,
+            "value": args.wavenumbers * world / (ms * 1e-3),
+            "unit": "wavenumber-solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if pname == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": pname,
+                       "wavenumbers_per_gpu": args.wavenumbers,
+                       "l2": "inputs 190 MB > 126 MB L2, no flush",
+                       "parallelism": f"replicas x{world} (wavenumber shards)"},
+            "fp64_solves_per_s": args.wavenumbers * world / (results["fp64"]["ms"] * 1e-3),
+            "mixed_solves_per_s": args.wavenumbers * world / (results["mixed"]["ms"] * 1e-3),
+            "mixed_over_fp64": results["fp64"]["ms"] / results["mixed"]["ms"],
+            "accuracy_vs_oracle": acc,
+            "roofline": roof,
+            "e2e": {"value": args.wavenumbers * world / e2e_s, "unit": "wavenumber-solves/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "clocks": results[pname]["clocks"],
+            "device_status": {p: results[p]["status"] for p in precisions},
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(b)
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def measured_peaks(lib):
+    """FP64 / FP32 FMA peaks: MEASURED_PEAKS.json when it holds them, else the
+    engine's FMA-throughput probe run now on this GPU."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        mp = json.load(open(path))
+    except Exception:
+        mp = {}
+    if "fp64_tflops" in mp and "fp32_tflops" in mp:
+        return {"fp64_tflops": mp["fp64_tflops"], "fp32_tflops": mp["fp32_tflops"],
+                "source": "MEASURED_PEAKS.json"}
+    import ctypes as C
+    f64 = C.c_double()
+    f32 = C.c_double()
+    if hasattr(lib, "adrt_probe_fma_tflops") and \
+            lib.adrt_probe_fma_tflops(C.byref(f64), C.byref(f32)) == 0:
+        return {"fp64_tflops": f64.value, "fp32_tflops": f32.value,
+                "source": "measured live: FMA-throughput probe kernel"}
+    return {"fp64_tflops": None, "fp32_tflops": None, "source": "unavailable"}
+
+
+if __name__ == "__main__":
+    main()

@@ -14,9 +14,9 @@
  *                            per interface (src/adding_doubling.hpp:32-50), not TOA only.
  *   adrt_solve_batch_host    adrt::cuda::solveBatchHost(...)      src_cuda/cuda_solver.cuh:85-98
  *                            (host buffers; copies in, solves, copies out, synchronises).
- *   adrt_solve_column        adrt::solve(const ADConfig&)          src/adding_doubling.hpp:258
- *                            (one column, host buffers, RTOutput layout).
- *   adrt_validate_column     ADConfig::validate()                  src/adding_doubling.hpp:123-174
+ *   adrt_solve_batch_host    with W = 1 also serves adrt::solve(const ADConfig&)
+ *                            (src/adding_doubling.hpp:258; RTOutput per-interface layout).
+ *   adrt_validate_batch      ADConfig::validate()                  src/adding_doubling.hpp:123-174
  *   adrt_engine_create/...   SolverWorkspaceGPU                    src_cuda/cuda_solver.cuh:140-156
  *                            (the engine owns every device work buffer; nothing is
  *                            allocated inside a solve once adrt_engine_reserve succeeded).
@@ -187,6 +187,14 @@ typedef struct adrt_column_desc {
  * solver kernel.  The column table is copied to the device by the engine. */
 int adrt_solve_batch_uneven(adrt_engine* engine, const adrt_column_desc* cols, int ncols,
                             void* cuda_stream);
+
+/* ---------------------------------------------------------- utilities */
+
+/* Measured FP64 and FP32 FMA throughput (TFLOP/s) of the current device: the
+ * roofline denominators of the solver kernels, whose products and
+ * eliminations run on the CUDA-core FMA pipes.  Engine utility; the reference
+ * has no counterpart. */
+int adrt_probe_fma_tflops(double* fp64_tflops, double* fp32_tflops);
 
 /* --------------------------------------------------------------- errors */
 const char* adrt_last_status_detail(void);

@@ -1,0 +1,101 @@
+"""The C-ABI library loads and exports every entry point the header declares,
+and its host-side validation mirrors ADConfig::validate()
+(src/adding_doubling.hpp:123-174).  No GPU needed: nothing here launches."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from addingdoublingrt_b200 import _abi, _lib, workloads
+
+HEADER = os.path.join(ROOT, "include", "adrt_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(adrt_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_declares_the_abi():
+    syms = declared_symbols()
+    for s in ("adrt_engine_create", "adrt_solve_batch", "adrt_solve_batch_host",
+              "adrt_solve_batch_uneven", "adrt_last_status_detail"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(_lib.EXPORTS) <= set(declared_symbols())
+
+
+def test_struct_layouts_match_header():
+    # 11 ints + pad, then 10 doubles
+    assert C.sizeof(_abi.BatchDesc) == 11 * 4 + 4 + 10 * 8
+    assert C.sizeof(_abi.Inputs) == 11 * 8
+    assert C.sizeof(_abi.Outputs) == 8 * 8
+
+
+def _validate(b):
+    lib = _lib.load()
+    rc = lib.adrt_validate_batch(C.byref(b.desc), C.byref(b.inputs_struct()))
+    return rc, lib.adrt_last_status_detail().decode()
+
+
+def test_validate_accepts_workloads():
+    for b in (workloads.config1(W=10), workloads.config2(W=10), workloads.config3(W=10),
+              workloads.config5(W=10)):
+        rc, msg = _validate(b)
+        assert rc == 0, msg
+
+
+@pytest.mark.parametrize("mutate,match", [
+    (lambda b: b.arrays["delta_tau"].__setitem__(3, -0.1), "delta_tau"),
+    (lambda b: b.arrays["single_scat_albedo"].__setitem__(0, 1.5), "single_scat_albedo"),
+    (lambda b: setattr(b.desc, "num_layers", 0), "num_layers"),
+    (lambda b: setattr(b.desc, "num_quadrature", 1), "num_quadrature"),
+    (lambda b: b.set("surface_albedo", np.full(b.W, 1.2)), "surface_albedo"),
+    (lambda b: b.set("solar_mu", np.zeros(b.W)), "solar_mu"),
+    (lambda b: b.arrays["temperature"].__setitem__(0, -5.0), "temperature"),
+    (lambda b: b.set("wavenumber_high", np.zeros(b.W)), "wavenumber"),
+])
+def test_validate_rejects_like_the_reference(mutate, match):
+    b = workloads.config2(W=4)
+    mutate(b)
+    rc, msg = _validate(b)
+    assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT
+    assert match in msg
+
+
+def test_orders_above_32_are_unsupported():
+    b = workloads.config2(W=2)
+    b.desc.num_quadrature = 33
+    rc, msg = _validate(b)
+    assert rc == _abi.ADRT_ERR_UNSUPPORTED and "not supported" in msg
+
+
+def test_validate_requires_thermal_for_surface_temperature():
+    b = workloads.config1(W=2)
+    b.desc.surface_temperature = 300.0
+    rc, msg = _validate(b)
+    assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT and "requires use_thermal_emission" in msg
+    b = workloads.config1(W=2)
+    b.desc.top_temperature = 0.0
+    rc, msg = _validate(b)
+    assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT and "top_temperature" in msg
+
+
+def test_validate_diffusion_needs_sources():
+    b = workloads.config1(W=2)
+    b.desc.use_diffusion_lower_bc = 1
+    rc, msg = _validate(b)
+    assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT and "diffusion" in msg
+
+
+def test_version_string():
+    assert b"sm_100a" in _lib.load().adrt_version()

@@ -1,0 +1,216 @@
+"""Parity of the CUDA engine with the oracle (GPU).
+
+Tolerance.  The reference scheme amplifies round-off strongly in some layers
+(weakly scattering thick layers whose thin-layer start tau0 exceeds the
+smallest quadrature cosine; near-conservative thick layers), so two FP64
+evaluations of the same scheme that differ only in FMA contraction already
+disagree there.  Every FP64 comparison is therefore made per wavenumber and
+output, normalised by that wavenumber's largest |value|, and must satisfy
+
+    err <= 1e-9 + 30 * sens
+
+where `sens` is the same normalised difference between the oracle compiled
+without and with FMA contraction (the scheme's own FP64 sensitivity on that
+input).  On well-conditioned inputs sens ~ 1e-16 and the bound is 1e-9.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import cuda_available, golden_paths, load_golden
+from addingdoublingrt_b200 import _abi, workloads
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = golden_paths()
+OUTS = ("flux_up", "flux_down", "flux_direct", "mean_intensity", "flux_divergence")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    from addingdoublingrt_b200.engine import Engine
+    e = Engine()
+    yield e
+    e.close()
+
+
+def run_device(eng, b, which=_abi.OUTPUT_FIELDS):
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    di = to_device(b)
+    do = alloc_device_outputs(b, which)
+    eng.solve_device(b.desc, di, do)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in do.items()}
+
+
+def per_wav_norm_err(x, ref, per):
+    x = np.asarray(x).reshape(-1, per)
+    ref = np.asarray(ref).reshape(-1, per)
+    s = np.max(np.abs(ref), axis=1)
+    s[s == 0] = 1.0
+    return np.max(np.abs(x - ref), axis=1) / s
+
+
+def assert_fp64_parity(b, res, ref, sens_ref, tag):
+    per = b.L + 1
+    for k in OUTS:
+        e = per_wav_norm_err(res[k], ref[k], per)
+        s = per_wav_norm_err(sens_ref[k], ref[k], per)
+        bound = 1e-9 + 30.0 * s
+        bad = np.nonzero(e > bound)[0]
+        assert bad.size == 0, (tag, k, int(bad[0]), float(e[bad[0]]), float(bound[bad[0]]))
+    for k, idx in (("toa_flux_down", 0),):
+        if k in res:
+            assert np.allclose(res[k], ref[k], rtol=1e-9, atol=1e-12 * np.max(np.abs(ref[k]) + 1))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p)[:-4] for p in GOLDEN])
+def test_fp64_engine_matches_reference_golden(eng, path):
+    name, b, ref = load_golden(path)
+    sens = oracle.solve_oracle(b, 4, fma=True)
+    res = run_device(eng, b)
+    assert_fp64_parity(b, res, ref, sens, name)
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_BAD_INPUT) == 0
+
+
+@pytest.mark.parametrize("seed", range(300, 340))
+def test_fp64_engine_matches_oracle_random(eng, seed):
+    b = workloads.random_small(seed)
+    try:
+        ref = oracle.solve_oracle(b, 4)
+    except oracle.OracleError:
+        pytest.skip("configuration rejected by validate()")
+    sens = oracle.solve_oracle(b, 4, fma=True)
+    assert_fp64_parity(b, run_device(eng, b), ref, sens, seed)
+
+
+@pytest.mark.parametrize("name,make", [
+    ("config1", lambda: workloads.config1(W=1000).subset(np.arange(0, 1000, 7))),
+    ("config2", lambda: workloads.config2().subset(np.arange(0, 100_000, 631))),
+    ("config3", lambda: workloads.config3().subset(np.arange(0, 20_000, 997))),
+    ("config5", lambda: workloads.config5().subset(np.arange(0, 10_000, 173))),
+])
+def test_fp64_engine_on_workload_samples(eng, name, make):
+    b = make()
+    ref = oracle.solve_oracle(b, os.cpu_count() or 1)
+    sens = oracle.solve_oracle(b, os.cpu_count() or 1, fma=True)
+    assert_fp64_parity(b, run_device(eng, b), ref, sens, name)
+
+
+def test_full_size_config2_batch_is_consistent(eng):
+    """Full 100k x 100 batch: every wavenumber finite, identical wavenumbers give
+    identical results, the direct beam is exact, and a sample matches the oracle."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    b = workloads.config2()
+    W, L = b.W, b.L
+    # plant duplicates of wavenumber 0 at the end of the batch
+    for k in ("delta_tau", "single_scat_albedo", "phase_moments"):
+        a = b.arrays[k].reshape(W, -1)
+        a[-3:] = a[0]
+    for k in ("surface_albedo", "solar_mu", "wavenumber_low", "wavenumber_high"):
+        b.arrays[k][-3:] = b.arrays[k][0]
+    di = to_device(b)
+    do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+    eng.solve_device(b.desc, di, do)
+    torch.cuda.synchronize()
+    assert eng.read_status() & _abi.ADRT_FLAG_NONFINITE == 0
+    for k, v in do.items():
+        assert torch.isfinite(v).all(), k
+        v2 = v.view(W, L + 1)
+        assert torch.equal(v2[-1], v2[0]) and torch.equal(v2[-2], v2[0]), k
+    idx = np.arange(0, W, W // 64)
+    ref = oracle.solve_oracle(b.subset(idx), os.cpu_count() or 1, which=_abi.INTERFACE_OUTPUTS)
+    sens = oracle.solve_oracle(b.subset(idx), os.cpu_count() or 1, which=_abi.INTERFACE_OUTPUTS,
+                               fma=True)
+    res = {k: v.view(W, L + 1)[torch.as_tensor(idx, device=v.device)].cpu().numpy().ravel()
+           for k, v in do.items()}
+    assert_fp64_parity(b.subset(idx), res, ref, sens, "config2-full")
+
+
+def test_host_entry_equals_device_entry(eng):
+    b = workloads.config5(W=64)
+    dev = run_device(eng, b)
+    host = eng.solve_host(b)
+    for k in _abi.OUTPUT_FIELDS:
+        assert np.array_equal(dev[k], host[k]), k
+
+
+def test_toa_outputs_and_spectrum_scaling(eng):
+    b = workloads.config1(W=16)
+    b.desc.spectrum_scaling = 0.25
+    res = run_device(eng, b)
+    L = b.L
+    fu = res["flux_up"].reshape(-1, L + 1)
+    assert np.array_equal(res["toa_flux_up"], fu[:, 0] * 0.25)
+    assert np.array_equal(res["toa_flux_down"], res["flux_down"].reshape(-1, L + 1)[:, 0])
+    assert np.array_equal(res["boa_flux_direct"], res["flux_direct"].reshape(-1, L + 1)[:, L])
+
+
+def test_index_from_bottom_is_a_reversal(eng):
+    b = workloads.config2(W=8)
+    top = run_device(eng, b)
+    fb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+    fb.desc.index_from_bottom = 1
+    L = b.L
+    fb.set("delta_tau", b.arrays["delta_tau"].reshape(8, L)[:, ::-1])
+    fb.set("single_scat_albedo", b.arrays["single_scat_albedo"].reshape(8, L)[:, ::-1])
+    fb.set("temperature", b.arrays["temperature"][::-1])
+    bot = run_device(eng, fb)
+    for k in OUTS:
+        assert np.array_equal(bot[k].reshape(8, L + 1)[:, ::-1], top[k].reshape(8, L + 1)), k
+
+
+def test_mixed_precision_accuracy_bound(eng):
+    """The mixed form's normalised error on config-2 samples (recorded bound)."""
+    b = workloads.config2(precision=_abi.PRECISION_MIXED).subset(np.arange(0, 100_000, 997))
+    ref = oracle.solve_oracle(b, os.cpu_count() or 1)
+    res = run_device(eng, b)
+    for k in ("flux_up", "flux_down", "mean_intensity"):
+        e = oracle.norm_error(res[k], ref[k], b.L + 1)
+        assert e < 5e-3, (k, e)
+
+
+def test_invalid_arguments_raise(eng):
+    from addingdoublingrt_b200._lib import ADRTError
+    b = workloads.config1(W=4)
+    b.desc.num_layers = 0
+    with pytest.raises(ADRTError):
+        eng.solve_host(b)
+    b = workloads.config1(W=4)
+    b.desc.solar_mu = 0.0
+    with pytest.raises(ADRTError, match="solar_mu"):
+        eng.solve_host(b)
+
+
+def test_bad_values_set_the_device_status_flag(eng):
+    b = workloads.config1(W=4)
+    b.arrays["delta_tau"][5] = -1.0  # the device path reports instead of throwing
+    run_device(eng, b)
+    assert eng.read_status() & _abi.ADRT_FLAG_BAD_INPUT
+    assert eng.read_status() == 0  # read clears
+
+
+def test_uneven_batch_equals_separate_solves(eng):
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    cols = workloads.config4_columns(ncols=12, seed=4)
+    cols = [c for c in cols if c.N in (8, 16)][:6]
+    for c in cols:
+        c.desc.precision = _abi.PRECISION_FP64
+    groups = {}
+    for c in cols:
+        groups.setdefault(8 if c.N <= 8 else 16, []).append(c)
+    for np_, grp in groups.items():
+        dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in grp]
+        eng.solve_uneven(dev)
+        torch.cuda.synchronize()
+        for c, (_, _, do) in zip(grp, dev):
+            single = run_device(eng, c, _abi.INTERFACE_OUTPUTS)
+            for k in _abi.INTERFACE_OUTPUTS:
+                assert np.array_equal(do[k].cpu().numpy(), single[k]), k
