@@ -58,7 +58,8 @@ def build(verbose: bool = False, force: bool = False, extra=()) -> str:
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc(), "-shared", "-o", tmp, *objs, "-lcudart"], check=True)
+    subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp,
+                    *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
     return LIB
 
