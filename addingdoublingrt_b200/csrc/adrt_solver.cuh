@@ -53,9 +53,11 @@ struct Geo {
   static constexpr int LD = DIM + PAD;
   static constexpr int MAT = DIM * LD;                // Reals per smem matrix
   static constexpr int NW = G / 32;                   // warps per group
+  static constexpr int NMAT = 6;                      // smem matrix buffers per group
   // matvec lanes: warp 0 only; LPR lanes per row
   static constexpr int LPR = (32 / NP < NP) ? (32 / NP) : NP;
   static constexpr int KCH = NP / LPR;
+  static_assert(NP % TR == 0 && NP % TC == 0, "tiles must divide the padded order");
 };
 
 // Shared-memory layout of one group (byte offsets).
@@ -64,25 +66,24 @@ struct SmemLayout {
   using Real = typename Gm::Real;
   static constexpr int NP = Gm::NP;
   static constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-  // Real matrices
-  static constexpr size_t mats = 0;                                  // 4 x MAT Real
-  static constexpr size_t gj = align16(mats + 4 * sizeof(Real) * Gm::MAT);  // row/colA/colB x2, inv x2
+  static constexpr size_t mats = 0;  // NMAT x MAT Real
+  static constexpr size_t gj = align16(mats + Gm::NMAT * sizeof(Real) * Gm::MAT);
   static constexpr size_t vecs = align16(gj + sizeof(Real) * (6 * Gm::DIM + 4));
-  static constexpr int NVEC = 24;                                    // Real vectors of NP
-  static constexpr size_t dmats = align16(vecs + sizeof(Real) * NVEC * NP);  // Ppp, Ppm (double)
-  static constexpr size_t dvecs = align16(dmats + 2 * sizeof(double) * NP * NP);
-  static constexpr int NDVEC = 6;                                    // double vectors of NP
-  static constexpr size_t misc = align16(dvecs + sizeof(double) * NDVEC * NP);
+  static constexpr int NVEC = 20;  // Real vectors of NP
+  static constexpr size_t dvecs = align16(vecs + sizeof(Real) * NVEC * NP);
+  static constexpr int NDVEC = 6;  // double vectors of NP
+  static constexpr size_t col = align16(dvecs + sizeof(double) * NDVEC * NP);
+  static constexpr size_t misc = align16(col + sizeof(ColumnDev));
   static constexpr size_t bytes = align16(misc + 64);
 };
 
 // Vector slots (Real) inside SmemLayout::vecs.
 enum VecSlot {
   V_Y0 = 0, V_Y1, V_Z0, V_Z1, V_SU0, V_SU1, V_SD0, V_SD1,
-  V_RU, V_RD, V_UB, V_SDN, V_SUP, V_ID, V_IU, V_RHS, V_TMP, V_TMP2, V_T, V_X
+  V_RU, V_RD, V_UB, V_SDN, V_SUP, V_ID, V_IU, V_RHS, V_TMP, V_T, V_X
 };
-// Double vector slots inside SmemLayout::dvecs.
-enum DVecSlot { D_PP = 0, D_PM, D_COL, D_IBOT };
+// Double vector slots inside SmemLayout::dvecs: quadrature and solar phase.
+enum DVecSlot { D_MU = 0, D_WT, D_CW, D_HW, D_PP, D_PM };
 
 // ============================================================== sync / reductions
 template <int G>
@@ -113,27 +114,18 @@ __device__ __forceinline__ unsigned gmax_u32(unsigned key, unsigned* red, int pa
   }
 }
 
-// ============================================================== small helpers
-template <typename T>
-__device__ __forceinline__ T sel(const T* v, int idx, int n) {
-  T r = v[0];
-#pragma unroll
-  for (int i = 1; i < 8; ++i)
-    if (i < n && idx == i) r = v[i];
-  return r;
-}
-
+// ============================================================== vector smem access
 template <typename Real, int CNT>
-__device__ __forceinline__ void lds_vec(Real (&dst)[CNT], const Real* src) {
+__device__ __forceinline__ void lds_vec(Real* dst, const Real* src) {
   if constexpr (sizeof(Real) * CNT % 16 == 0) {
 #pragma unroll
     for (int i = 0; i < CNT; i += 16 / (int)sizeof(Real)) {
       if constexpr (sizeof(Real) == 8) {
-        double2 v = *reinterpret_cast<const double2*>(src + i);
+        const double2 v = *reinterpret_cast<const double2*>(src + i);
         dst[i] = v.x;
         dst[i + 1] = v.y;
       } else {
-        float4 v = *reinterpret_cast<const float4*>(src + i);
+        const float4 v = *reinterpret_cast<const float4*>(src + i);
         dst[i] = v.x;
         dst[i + 1] = v.y;
         dst[i + 2] = v.z;
@@ -141,7 +133,7 @@ __device__ __forceinline__ void lds_vec(Real (&dst)[CNT], const Real* src) {
       }
     }
   } else if constexpr (sizeof(Real) == 4 && CNT == 2) {
-    float2 v = *reinterpret_cast<const float2*>(src);
+    const float2 v = *reinterpret_cast<const float2*>(src);
     dst[0] = v.x;
     dst[1] = v.y;
   } else {
@@ -150,125 +142,162 @@ __device__ __forceinline__ void lds_vec(Real (&dst)[CNT], const Real* src) {
   }
 }
 
+template <typename Real, int CNT>
+__device__ __forceinline__ void sts_vec(Real* dst, const Real* src) {
+  if constexpr (sizeof(Real) * CNT % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < CNT; i += 16 / (int)sizeof(Real)) {
+      if constexpr (sizeof(Real) == 8) {
+        *reinterpret_cast<double2*>(dst + i) = make_double2(src[i], src[i + 1]);
+      } else {
+        *reinterpret_cast<float4*>(dst + i) = make_float4(src[i], src[i + 1], src[i + 2], src[i + 3]);
+      }
+    }
+  } else if constexpr (sizeof(Real) == 4 && CNT == 2) {
+    *reinterpret_cast<float2*>(dst) = make_float2(src[0], src[1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < CNT; ++i) dst[i] = src[i];
+  }
+}
+
 // ============================================================== tile algebra
+// Every matrix lives in shared memory (row-major "rm": s[r*LD + c], or
+// column-major "cm": s[c*LD + r]).  Thread t of the group owns the TR x TC
+// tile at rows rb*TR.., cols cb*TC.. of every operation's output; the
+// operations are non-inlined so each exists once in the binary.
 template <class Gm>
-struct TileOps {
+struct Tile {
   using Real = typename Gm::Real;
-  static constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, G = Gm::G;
-  using Tile = Real[TR][TC];
-
-  int t, rb, cb, bar;
-
-  __device__ __forceinline__ TileOps(int tid, int bar_id)
-      : t(tid), rb(tid / Gm::CB), cb(tid % Gm::CB), bar(bar_id) {}
-
+  static constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
+  int rb, cb;
+  __device__ __forceinline__ explicit Tile(int t) : rb(t / Gm::CB), cb(t % Gm::CB) {}
+  __device__ __forceinline__ bool valid() const { return rb * TR < NP && cb * TC < NP; }
   __device__ __forceinline__ int row(int a) const { return rb * TR + a; }
   __device__ __forceinline__ int col(int b) const { return cb * TC + b; }
-  __device__ __forceinline__ bool valid(int a, int b) const { return row(a) < NP && col(b) < NP; }
+  __device__ __forceinline__ void load_rm(Real (&X)[TR][TC], const Real* s) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a) lds_vec<Real, TC>(X[a], s + row(a) * LD + cb * TC);
+  }
+  __device__ __forceinline__ void store_rm(const Real (&X)[TR][TC], Real* s) const {
+#pragma unroll
+    for (int a = 0; a < TR; ++a) sts_vec<Real, TC>(s + row(a) * LD + cb * TC, X[a]);
+  }
+  __device__ __forceinline__ void store_cm(const Real (&X)[TR][TC], Real* s) const {
+#pragma unroll
+    for (int b = 0; b < TC; ++b) {
+      Real colv[TR];
+#pragma unroll
+      for (int a = 0; a < TR; ++a) colv[a] = X[a][b];
+      sts_vec<Real, TR>(s + col(b) * LD + rb * TR, colv);
+    }
+  }
+};
 
-  __device__ __forceinline__ void sync() const { gsync<G>(bar); }
-
-  __device__ __forceinline__ void zero(Tile& X) const {
+// out = [I -] X Y [+ add]: X column-major (XT[k*LD + r] = X[r][k]), Y and add
+// row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
+// alias out_rm (each thread reads its own tile before writing it).
+template <class Gm>
+__device__ __noinline__ void op_gemm(const typename Gm::Real* __restrict__ XT,
+                                     const typename Gm::Real* __restrict__ Y,
+                                     const typename Gm::Real* add, int id_minus,
+                                     typename Gm::Real* out_rm, typename Gm::Real* out_cm, int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real acc[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) acc[a][b] = Real(0);
+  const Real* xp = XT + tl.rb * TR;
+  const Real* yp = Y + tl.cb * TC;
+#pragma unroll 8
+  for (int k = 0; k < NP; ++k) {
+    Real xa[TR], yb[TC];
+    lds_vec<Real, TR>(xa, xp + k * LD);
+    lds_vec<Real, TC>(yb, yp + k * LD);
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
-      for (int b = 0; b < TC; ++b) X[a][b] = Real(0);
+      for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
   }
-  __device__ __forceinline__ void identity(Tile& X) const {
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-      for (int b = 0; b < TC; ++b) X[a][b] = (row(a) == col(b)) ? Real(1) : Real(0);
-  }
-  __device__ __forceinline__ void copy(Tile& D, const Tile& S) const {
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-      for (int b = 0; b < TC; ++b) D[a][b] = S[a][b];
-  }
-
-  // Row-major store of the tile into an smem matrix.
-  __device__ __forceinline__ void stage_rm(const Tile& X, Real* s) const {
+  if (id_minus) {
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
       for (int b = 0; b < TC; ++b)
-        if (valid(a, b)) s[row(a) * LD + col(b)] = X[a][b];
+        acc[a][b] = ((tl.row(a) == tl.col(b)) ? Real(1) : Real(0)) - acc[a][b];
   }
-  // Column-major store (s[c*LD + r] = X[r][c]).
-  __device__ __forceinline__ void stage_cm(const Tile& X, Real* s) const {
+  if (add) {
+    Real ad[TR][TC];
+    tl.load_rm(ad, add);
 #pragma unroll
-    for (int b = 0; b < TC; ++b)
+    for (int a = 0; a < TR; ++a)
 #pragma unroll
-      for (int a = 0; a < TR; ++a)
-        if (valid(a, b)) s[col(b) * LD + row(a)] = X[a][b];
+      for (int b = 0; b < TC; ++b) acc[a][b] = ad[a][b] + acc[a][b];
   }
+  if (out_rm) tl.store_rm(acc, out_rm);
+  if (out_cm) tl.store_cm(acc, out_cm);
+}
 
-  // acc (+)= X Y, with X given column-major (sXT[k*LD + r] = X[r][k]) and Y row-major.
-  template <bool ACC>
-  __device__ __forceinline__ void gemm(Tile& acc, const Real* sXT, const Real* sY) const {
-    if constexpr (!ACC) zero(acc);
-    const Real* xp = sXT + rb * TR;
-    const Real* yp = sY + cb * TC;
-#pragma unroll 4
-    for (int k = 0; k < NP; ++k) {
-      Real xa[TR], yb[TC];
-      lds_vec<Real, TR>(xa, xp + k * LD);
-      lds_vec<Real, TC>(yb, yp + k * LD);
+// X = B A^{-1} by Gauss-Jordan column elimination, with column pivoting on
+// the largest |entry| of the pivot row -- the pivot rule of the LU with
+// partial pivoting of A^T that the reference's right-solve performs
+// (src/matrix.hpp:120-124).  A and B are row-major in smem; when B is null
+// the right-hand side is the single row `bvec` (a vector solve).  The result
+// is written column-major to out_cm.  Returns nonzero if a pivot was exactly 0.
+template <class Gm>
+__device__ __noinline__ int op_gj(const typename Gm::Real* A_rm, const typename Gm::Real* B_rm,
+                                  const typename Gm::Real* bvec, typename Gm::Real* out_cm,
+                                  typename Gm::Real* gjbuf, unsigned* red, int t, int bar) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP, DIM = Gm::DIM;
+  constexpr int G = Gm::G;
+  const Tile<Gm> tl(t);
+  const bool tv = tl.valid();
+  Real A[TR][TC], B[TR][TC];
+  if (tv) {
+    tl.load_rm(A, A_rm);
+    if (B_rm) {
+      tl.load_rm(B, B_rm);
+    } else {
 #pragma unroll
       for (int a = 0; a < TR; ++a)
 #pragma unroll
-        for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+        for (int b = 0; b < TC; ++b) B[a][b] = (tl.row(a) == 0) ? bvec[tl.col(b)] : Real(0);
     }
-  }
-
-  // Tile to / from global memory in tile order (thread t owns TE contiguous Reals).
-  __device__ __forceinline__ void store_g(const Tile& X, Real* g) const {
-    Real* p = g + t * Gm::TE;
+  } else {
 #pragma unroll
     for (int a = 0; a < TR; ++a)
 #pragma unroll
-      for (int b = 0; b < TC; ++b) p[a * TC + b] = X[a][b];
+      for (int b = 0; b < TC; ++b) A[a][b] = B[a][b] = Real(0);
   }
-  __device__ __forceinline__ void load_g(Tile& X, const Real* g) const {
-    const Real* p = g + t * Gm::TE;
+  unsigned used = 0;
+  int q[TC];
 #pragma unroll
-    for (int a = 0; a < TR; ++a)
+  for (int b = 0; b < TC; ++b) q[b] = 0;
+  int singular = 0;
+  for (int kr = 0; kr * TR < NP; ++kr) {
 #pragma unroll
-      for (int b = 0; b < TC; ++b) X[a][b] = p[a * TC + b];
-  }
-
-  // X = B A^{-1} by Gauss-Jordan column elimination with column pivoting on
-  // the pivot row (the pivot rule of LU with partial pivoting of A^T).
-  // A and B are destroyed.  The result is written column-major to sXT.
-  // Returns nonzero (on every thread) if an exactly-zero pivot was met.
-  __device__ __forceinline__ int gj_right_solve(Tile& A, Tile& B, Real* sXT, Real* gjbuf,
-                                                unsigned* red) const {
-    constexpr int DIM = Gm::DIM;
-    unsigned used = 0;
-    int q[TC];
-#pragma unroll
-    for (int b = 0; b < TC; ++b) q[b] = 0;
-    int singular = 0;
-#pragma unroll
-    for (int k = 0; k < NP; ++k) {
+    for (int ka = 0; ka < TR; ++ka) {
+      const int k = kr * TR + ka;
       const int par = k & 1;
       Real* rowb = gjbuf + par * DIM;
       Real* colA = gjbuf + 2 * DIM + par * DIM;
       Real* colB = gjbuf + 4 * DIM + par * DIM;
       Real* invb = gjbuf + 6 * DIM + par;
-      const int kr = k / TR, ka = k % TR;
-      // 1. pivot search over the unused columns of row k
+      const bool own_row = tv && (tl.rb == kr);
+      // 1. pivot: largest |A[k][c]| over unused columns c
       unsigned key = 0;
-      if (rb == kr) {
+      if (own_row) {
 #pragma unroll
         for (int b = 0; b < TC; ++b) {
-          const int c = col(b);
-          if (c < NP && !((used >> c) & 1u)) {
-            float f = fabsf(static_cast<float>(A[ka][b]));
-            unsigned bits = __float_as_uint(f);
-            unsigned kk = (bits & ~63u) | 32u | (unsigned)c;
-            key = max(key, kk);
+          const int c = tl.col(b);
+          if (!((used >> c) & 1u)) {
+            const unsigned bits = __float_as_uint(fabsf(static_cast<float>(A[ka][b])));
+            key = max(key, (bits & ~63u) | 32u | (unsigned)c);
           }
         }
       }
@@ -277,12 +306,11 @@ struct TileOps {
       singular |= ((key >> 6) == 0u);
       used |= 1u << p;
       const int pb = p % TC;
+      const bool own_col = tv && (tl.cb == p / TC);
       // 2. publish row k, column p and 1/pivot
-      if (rb == kr) {
-#pragma unroll
-        for (int b = 0; b < TC; ++b)
-          if (col(b) < NP) rowb[col(b)] = A[ka][b];
-        if (cb == p / TC) {
+      if (own_row) {
+        sts_vec<Real, TC>(rowb + tl.cb * TC, A[ka]);
+        if (own_col) {
           Real piv = A[ka][0];
 #pragma unroll
           for (int b = 1; b < TC; ++b)
@@ -290,90 +318,105 @@ struct TileOps {
           *invb = Real(1) / piv;
         }
       }
-      if (cb == p / TC) {
+      if (own_col) {
+        Real va[TR], vb[TR];
 #pragma unroll
         for (int a = 0; a < TR; ++a) {
-          Real va = A[a][0], vb = B[a][0];
+          va[a] = A[a][0];
+          vb[a] = B[a][0];
 #pragma unroll
           for (int b = 1; b < TC; ++b)
             if (pb == b) {
-              va = A[a][b];
-              vb = B[a][b];
+              va[a] = A[a][b];
+              vb[a] = B[a][b];
             }
-          colA[row(a)] = va;
-          colB[row(a)] = vb;
         }
+        sts_vec<Real, TR>(colA + tl.rb * TR, va);
+        sts_vec<Real, TR>(colB + tl.rb * TR, vb);
       }
-      sync();
-      // 3. eliminate
-      const Real inv = *invb;
-      Real cA[TR], cB[TR], rv[TC];
-      lds_vec<Real, TR>(cA, colA + rb * TR);
-      lds_vec<Real, TR>(cB, colB + rb * TR);
-      lds_vec<Real, TC>(rv, rowb + cb * TC);
+      gsync<G>(bar);
+      // 3. eliminate column p from every other column
+      if (tv) {
+        const Real inv = *invb;
+        Real cA[TR], cB[TR], rv[TC];
+        lds_vec<Real, TR>(cA, colA + tl.rb * TR);
+        lds_vec<Real, TR>(cB, colB + tl.rb * TR);
+        lds_vec<Real, TC>(rv, rowb + tl.cb * TC);
 #pragma unroll
-      for (int a = 0; a < TR; ++a) {
-        cA[a] *= inv;
-        cB[a] *= inv;
-      }
-#pragma unroll
-      for (int a = 0; a < TR; ++a)
+        for (int a = 0; a < TR; ++a) {
+          cA[a] *= inv;
+          cB[a] *= inv;
+        }
 #pragma unroll
         for (int b = 0; b < TC; ++b) {
-          if (col(b) == p) {
-            A[a][b] = cA[a];
-            B[a][b] = cB[a];
-          } else {
-            A[a][b] = fma(-cA[a], rv[b], A[a][b]);
-            B[a][b] = fma(-cB[a], rv[b], B[a][b]);
+          const bool isp = (tl.col(b) == p);
+#pragma unroll
+          for (int a = 0; a < TR; ++a) {
+            const Real na = fma(-cA[a], rv[b], A[a][b]);
+            const Real nb = fma(-cB[a], rv[b], B[a][b]);
+            A[a][b] = isp ? cA[a] : na;
+            B[a][b] = isp ? cB[a] : nb;
           }
+          if (isp) q[b] = k;
         }
-#pragma unroll
-      for (int b = 0; b < TC; ++b)
-        if (col(b) == p) q[b] = k;
-    }
-    // write B A^{-1}: column c of the reduced B is column q[c] of the result
-#pragma unroll
-    for (int b = 0; b < TC; ++b)
-#pragma unroll
-      for (int a = 0; a < TR; ++a)
-        if (valid(a, b)) sXT[q[b] * LD + row(a)] = B[a][b];
-    return singular;
-  }
-};
-
-// ============================================================== matvec (warp 0)
-// y = X v for up to three vectors, X column-major in smem (sXT[k*LD+i] = X[i][k]).
-// Executed by warp 0 of the group; returns the sums on lanes with part == 0.
-template <class Gm, int NV>
-__device__ __forceinline__ void matvec_cm(const typename Gm::Real* sXT,
-                                          const typename Gm::Real* const (&v)[NV],
-                                          typename Gm::Real (&y)[NV], int lane) {
-  using Real = typename Gm::Real;
-  constexpr int NP = Gm::NP, LPR = Gm::LPR, KCH = Gm::KCH, LD = Gm::LD;
-  const int i = lane % NP, part = lane / NP;
-#pragma unroll
-  for (int n = 0; n < NV; ++n) y[n] = Real(0);
-  if (part < LPR) {
-#pragma unroll
-    for (int kk = 0; kk < KCH; ++kk) {
-      const int k = part * KCH + kk;
-      const Real x = sXT[k * LD + i];
-#pragma unroll
-      for (int n = 0; n < NV; ++n) y[n] = fma(x, v[n][k], y[n]);
+      }
     }
   }
+  // column c of the reduced B is column q[c] of B A^{-1}
+  if (tv) {
 #pragma unroll
-  for (int off = NP; off < NP * LPR; off <<= 1)
+    for (int b = 0; b < TC; ++b) {
+      Real colv[TR];
 #pragma unroll
-    for (int n = 0; n < NV; ++n) y[n] += __shfl_xor_sync(0xffffffffu, y[n], off);
+      for (int a = 0; a < TR; ++a) colv[a] = B[a][b];
+      sts_vec<Real, TR>(out_cm + q[b] * LD + tl.rb * TR, colv);
+    }
+  }
+  return singular;
 }
 
-// Same with X row-major (sX[i*LD+k]).
-template <class Gm, int NV>
-__device__ __forceinline__ void matvec_rm(const typename Gm::Real* sX,
-                                          const typename Gm::Real* const (&v)[NV],
-                                          typename Gm::Real (&y)[NV], int lane) {
+// Tile copies between the HBM scratch (tile order: thread t owns TE
+// contiguous Reals) and smem.
+template <class Gm>
+__device__ __noinline__ void op_g2s(const typename Gm::Real* g, typename Gm::Real* out_rm,
+                                    typename Gm::Real* out_cm, int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real X[TR][TC];
+  const Real* p = g + t * Gm::TE;
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) X[a][b] = p[a * TC + b];
+  if (out_rm) tl.store_rm(X, out_rm);
+  if (out_cm) tl.store_cm(X, out_cm);
+}
+
+template <class Gm>
+__device__ __noinline__ void op_s2g(const typename Gm::Real* in_rm, typename Gm::Real* g, int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real X[TR][TC];
+  tl.load_rm(X, in_rm);
+  Real* p = g + t * Gm::TE;
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) p[a * TC + b] = X[a][b];
+}
+
+// ============================================================== matvec (warp 0)
+// y = X v (NV vectors) with X in smem, column-major (CM) or row-major.
+// Executed by warp 0 of the group; every lane ends with the full sums of
+// row lane % NP.
+template <class Gm, bool CM, int NV>
+__device__ __forceinline__ void matvec(const typename Gm::Real* S,
+                                       const typename Gm::Real* const (&v)[NV],
+                                       typename Gm::Real (&y)[NV], int lane) {
   using Real = typename Gm::Real;
   constexpr int NP = Gm::NP, LPR = Gm::LPR, KCH = Gm::KCH, LD = Gm::LD;
   const int i = lane % NP, part = lane / NP;
@@ -383,7 +426,7 @@ __device__ __forceinline__ void matvec_rm(const typename Gm::Real* sX,
 #pragma unroll
     for (int kk = 0; kk < KCH; ++kk) {
       const int k = part * KCH + kk;
-      const Real x = sX[i * LD + k];
+      const Real x = CM ? S[k * LD + i] : S[i * LD + k];
 #pragma unroll
       for (int n = 0; n < NV; ++n) y[n] = fma(x, v[n][k], y[n]);
     }

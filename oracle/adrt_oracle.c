@@ -886,9 +886,12 @@ static int solve_one(const adrt_batch_desc* d, const adrt_inputs* in, const adrt
     if (out->flux_direct) memcpy(out->flux_direct + off, o.fdir, sizeof(double) * nint);
     if (out->mean_intensity) memcpy(out->mean_intensity + off, o.J, sizeof(double) * nint);
     if (out->flux_divergence) memcpy(out->flux_divergence + off, o.divF, sizeof(double) * nint);
-    if (out->toa_flux_up) out->toa_flux_up[w] = o.fu[0] * d->spectrum_scaling;
-    if (out->toa_flux_down) out->toa_flux_down[w] = o.fd[0];
-    if (out->boa_flux_direct) out->boa_flux_direct[w] = o.fdir[nint - 1];
+    /* outputs are in the caller's level order: TOA is the last level when
+       the arrays are indexed from the bottom */
+    const int toa = d->index_from_bottom ? nint - 1 : 0, boa = d->index_from_bottom ? 0 : nint - 1;
+    if (out->toa_flux_up) out->toa_flux_up[w] = o.fu[toa] * d->spectrum_scaling;
+    if (out->toa_flux_down) out->toa_flux_down[w] = o.fd[toa];
+    if (out->boa_flux_direct) out->boa_flux_direct[w] = o.fdir[boa];
   }
   free(buf);
   free_column(&c);

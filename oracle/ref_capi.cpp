@@ -87,9 +87,12 @@ void store(const adrt_batch_desc& d, const adrt_outputs& o, int w, const adrt::R
   put(o.flux_direct, r.flux_direct);
   put(o.mean_intensity, r.mean_intensity);
   put(o.flux_divergence, r.flux_divergence);
-  if (o.toa_flux_up) o.toa_flux_up[w] = r.flux_up[0] * d.spectrum_scaling;
-  if (o.toa_flux_down) o.toa_flux_down[w] = r.flux_down[0];
-  if (o.boa_flux_direct) o.boa_flux_direct[w] = r.flux_direct[n - 1];
+  // RTOutput is in the caller's level order; TOA is level n-1 when the
+  // arrays are indexed from the bottom (src/solver.cpp:711-719).
+  const size_t toa = d.index_from_bottom ? n - 1 : 0, boa = d.index_from_bottom ? 0 : n - 1;
+  if (o.toa_flux_up) o.toa_flux_up[w] = r.flux_up[toa] * d.spectrum_scaling;
+  if (o.toa_flux_down) o.toa_flux_down[w] = r.flux_down[toa];
+  if (o.boa_flux_direct) o.boa_flux_direct[w] = r.flux_direct[boa];
 }
 
 }  // namespace

@@ -13,6 +13,13 @@ where `sens` is the same normalised difference between the oracle compiled
 without and with FMA contraction (the scheme's own FP64 sensitivity on that
 input).  On well-conditioned inputs sens ~ 1e-16 and the bound is 1e-9.
 
+A scattering layer whose thin-layer start is unstable -- tau0 = tau 2^-nn
+larger than the smallest quadrature cosine, which the reference's nn rule
+gives weakly scattering thick layers (omega < 0.01) -- starts the doubling
+from T = I - tau0 Gpp with large negative diagonal entries and amplifies
+round-off by orders of magnitude; the FMA probe samples that amplification
+but does not bound it, so such wavenumbers get 1e-9 + 1000 * sens.
+
 Near-conservative thick layers (1 - omega < 1e-4 with tau > 1) make I - R^2
 nearly singular.  There the reference-order FP64 evaluation itself differs
 from an 80-bit evaluation of the same scheme by up to ~1e-7 (measured on the
@@ -68,13 +75,35 @@ def near_conservative(b):
     return np.any((om > 1.0 - 1e-4) & (tau > 1.0), axis=1)
 
 
+def unstable_start(b):
+    """Wavenumbers with a scattering layer whose thin-layer start tau0 exceeds
+    the smallest Gauss-Legendre cosine (src/doubling.hpp:107-127)."""
+    lib = oracle.oracle_lib()
+    n = b.N
+    x = np.zeros(n)
+    w = np.zeros(n)
+    lib.oracle_gauss_legendre(n, x.ctypes.data, w.ctypes.data)
+    tau = b.arrays["delta_tau"].reshape(b.W, b.L)
+    om = b.arrays["single_scat_albedo"].reshape(b.W, b.L)
+    out = np.zeros(b.W, dtype=bool)
+    for wi in range(b.W):
+        for l in range(b.L):
+            if tau[wi, l] > 0 and om[wi, l] > 0:
+                nn = lib.oracle_num_doublings(float(tau[wi, l]), float(min(om[wi, l], 1.0)))
+                if tau[wi, l] * 2.0 ** -nn > x.min():
+                    out[wi] = True
+                    break
+    return out
+
+
 def assert_fp64_parity(b, res, ref, sens_ref, tag):
     per = b.L + 1
     nc = near_conservative(b)
+    us = unstable_start(b)
     for k in OUTS:
         e = per_wav_norm_err(res[k], ref[k], per)
         s = per_wav_norm_err(sens_ref[k], ref[k], per)
-        bound = np.where(nc, 1e-6, 1e-9 + 30.0 * s)
+        bound = np.where(nc, 1e-6, 1e-9 + np.where(us, 1000.0, 30.0) * s)
         bad = np.nonzero(e > bound)[0]
         assert bad.size == 0, (tag, k, int(bad[0]), float(e[bad[0]]), float(bound[bad[0]]))
     for k, idx in (("toa_flux_down", 0),):
