@@ -10,7 +10,8 @@ import threading
 from . import _abi
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libadrt_b200.so")
+# ADRT_LIBRARY may point at another build of the same library (tuning variants).
+LIB_PATH = os.environ.get("ADRT_LIBRARY") or os.path.join(_PKG, "libadrt_b200.so")
 
 _lock = threading.Lock()
 _lib = None

@@ -45,23 +45,27 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(verbose: bool = False, force: bool = False, extra=()) -> str:
-    if not force and not _stale():
+def build(verbose: bool = False, force: bool = False, extra=(), out: str | None = None) -> str:
+    """Compile and link the engine.  `extra` adds nvcc flags (e.g. -D
+    tuning macros) and `out` redirects the library (variant builds)."""
+    target = out or LIB
+    if not force and out is None and not _stale():
         return LIB
     objs = []
+    tag = "" if out is None else "_" + os.path.basename(out).replace(".so", "")
     for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
+        obj = os.path.join(CSRC, src.replace(".cu", tag + ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    tmp = LIB + ".tmp"
+    tmp = target + ".tmp"
     subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp,
                     *objs, "-lcudart"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

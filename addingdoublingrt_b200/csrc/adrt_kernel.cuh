@@ -28,30 +28,39 @@ struct SlotLayout {
   }
 };
 
-// Pointers into one group's shared memory and slot.
+// Pointers into one group's shared memory.  Built inside every function
+// from the group's byte offset `goff` into adrt_smem, so the compiler sees
+// shared-space pointers; non-inlined calls receive (goff, t, bar).
 template <class Gm>
 struct Ctx {
   using Real = typename Gm::Real;
   using SL = SmemLayout<Gm>;
   static constexpr int NP = Gm::NP, MAT = Gm::MAT;
+  unsigned goff;
   int t, lane, warp, bar;
-  Real* m[Gm::NMAT];
-  Real *gjbuf, *vec;
+  Real *vec, *gjbuf;
   double* dvec;
   ColumnDev* col;
   unsigned* red;
   double* dmisc;
-  __device__ Ctx(char* smem, int t_, int bar_) : t(t_), lane(t_ & 31), warp(t_ >> 5), bar(bar_) {
-    Real* m0 = reinterpret_cast<Real*>(smem + SL::mats);
-#pragma unroll
-    for (int i = 0; i < Gm::NMAT; ++i) m[i] = m0 + i * MAT;
-    gjbuf = reinterpret_cast<Real*>(smem + SL::gj);
-    vec = reinterpret_cast<Real*>(smem + SL::vecs);
-    dvec = reinterpret_cast<double*>(smem + SL::dvecs);
-    col = reinterpret_cast<ColumnDev*>(smem + SL::col);
-    red = reinterpret_cast<unsigned*>(smem + SL::misc);
-    dmisc = reinterpret_cast<double*>(smem + SL::misc + 32);
+  __device__ __forceinline__ Ctx(unsigned goff_, int t_, int bar_)
+      : goff(goff_), t(t_), lane(t_ & 31), warp(t_ >> 5), bar(bar_) {
+    vec = sp<Real>(goff + SL::vecs);
+    gjbuf = sp<Real>(goff + SL::gj);
+    dvec = sp<double>(goff + SL::dvecs);
+    col = sp<ColumnDev>(goff + SL::col);
+    red = sp<unsigned>(goff + SL::misc);
+    dmisc = sp<double>(goff + SL::misc + 32);
   }
+  __device__ __forceinline__ unsigned mo(int i) const {
+    return goff + (unsigned)(SL::mats + (size_t)i * MAT * sizeof(Real));
+  }
+  __device__ __forceinline__ Real* m(int i) const { return sp<Real>(mo(i)); }
+  __device__ __forceinline__ unsigned vo(int s) const {
+    return goff + (unsigned)(SL::vecs + (size_t)s * NP * sizeof(Real));
+  }
+  __device__ __forceinline__ unsigned gjo() const { return goff + (unsigned)SL::gj; }
+  __device__ __forceinline__ unsigned redo() const { return goff + (unsigned)SL::misc; }
   __device__ __forceinline__ Real* V(int s) const { return vec + s * NP; }
   __device__ __forceinline__ double* DV(int s) const { return dvec + s * NP; }
   __device__ __forceinline__ void sync() const { gsync<Gm::G>(bar); }
@@ -64,10 +73,11 @@ struct Ctx {
 // 131-181) into D_PP / D_PM.  chi_l = (chi[l] - f) / (1 - f) when delta-M
 // truncation applies (f >= 0), chi[l] otherwise.
 template <class Gm>
-__device__ __noinline__ void build_phase(const Ctx<Gm>& X, const double* chi, int nuse, double f,
-                                         int N, const double* pl, bool solar, double mu0,
-                                         double* Ppp, double* Ppm) {
+__device__ __noinline__ void build_phase(unsigned goff, int t_, int bar, const double* chi,
+                                         int nuse, double f, int N, const double* pl, bool solar,
+                                         double mu0, double* Ppp, double* Ppm) {
   constexpr int NP = Gm::NP, G = Gm::G;
+  const Ctx<Gm> X(goff, t_, bar);
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
@@ -155,10 +165,12 @@ __device__ __noinline__ void build_phase(const Ctx<Gm>& X, const double* chi, in
 // m[1] (column-major), T in m[return value] (row-major, 2 or 3), and the
 // combined thermal + solar sources in V_SUP / V_SDN.
 template <class Gm>
-__device__ __noinline__ int doubling(const Ctx<Gm>& X, double tau, double om, double Bt, double Bb,
-                                     double tcum, int N, bool solar, double F0, double mu0,
-                                     const double* Ppp, const double* Ppm, int* singular) {
+__device__ __noinline__ int doubling(unsigned goff, int t_, int bar, double tau, double om,
+                                     double Bt, double Bb, double tcum, int N, bool solar,
+                                     double F0, double mu0, const double* Ppp, const double* Ppm,
+                                     int* singular) {
   using Real = typename Gm::Real;
+  const Ctx<Gm> X(goff, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC;
   const int t = X.t;
   const double* mu = X.DV(D_MU);
@@ -168,11 +180,12 @@ __device__ __noinline__ int doubling(const Ctx<Gm>& X, double tau, double om, do
   const int nn = num_doublings(tau, om);
   const double tau0 = ldexp(tau, -nn);
   const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
-  Real* Rrm = X.m[0];
-  Real* Rcm = X.m[1];
-  Real* Tb[2] = {X.m[2], X.m[3]};
-  Real* Am = X.m[4];  // I - R R, then TG R
-  Real* TGcm = X.m[5];
+  const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oTG = X.mo(5);
+  const unsigned oT[2] = {X.mo(2), X.mo(3)};
+  Real* Rrm = sp<Real>(oR);
+  Real* Rcm = sp<Real>(oRc);
+  Real* Am = sp<Real>(oA);  // I - R R, then TG R (column-major)
+  Real* TGcm = sp<Real>(oTG);
   // thin-layer start (FP64): T = I - tau0 Gpp, R = tau0 Gpm
   {
     const Tile<Gm> tl(t);
@@ -197,7 +210,7 @@ __device__ __noinline__ int doubling(const Ctx<Gm>& X, double tau, double om, do
         }
       tl.store_rm(Rt, Rrm);
       tl.store_cm(Rt, Rcm);
-      tl.store_rm(Tt, Tb[0]);
+      tl.store_rm(Tt, sp<Real>(oT[0]));
     }
   }
   if (X.warp == 0 && X.lane < NP) {
@@ -225,7 +238,7 @@ __device__ __noinline__ int doubling(const Ctx<Gm>& X, double tau, double om, do
     Real* z = X.V(V_Z0 + par);
     Real* su = X.V(V_SU0 + par);
     Real* sd = X.V(V_SD0 + par);
-    Real* T = Tb[cur];
+    const unsigned oTc = oT[cur];
     X.sync();  // R, T and the vectors of the previous step are complete
     if (solar && X.warp == 0) {  // ru = R sd + gam su, rd = gam R su + sd (old R)
       const Real* vv[2] = {sd, su};
@@ -236,14 +249,14 @@ __device__ __noinline__ int doubling(const Ctx<Gm>& X, double tau, double om, do
         X.V(V_RD)[X.lane] = gam * yv[1] + sd[X.lane];
       }
     }
-    op_gemm<Gm>(Rcm, Rrm, nullptr, 1, Am, nullptr, t);  // I - R^2
+    op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
     X.sync();
-    *singular |= op_gj<Gm>(Am, T, nullptr, TGcm, X.gjbuf, X.red, t, X.bar);  // TG = T (I-R^2)^-1
+    *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
     X.sync();
-    op_gemm<Gm>(TGcm, Rrm, nullptr, 0, nullptr, Am, t);  // TGR = TG R (column-major)
+    op_gemm<Gm>(oTG, oR, kNoMat, 0, kNoMat, oA, t);  // TGR = TG R (column-major)
     X.sync();
-    op_gemm<Gm>(Am, T, Rrm, 0, Rrm, Rcm, t);                     // R <- R + TGR T
-    op_gemm<Gm>(TGcm, T, nullptr, 0, Tb[cur ^ 1], nullptr, t);  // T <- TG T
+    op_gemm<Gm>(oA, oTc, oR, 0, oR, oRc, t);                 // R <- R + TGR T
+    op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], kNoMat, t);  // T <- TG T
     if (X.warp == 0) {
       Real* yn = X.V(V_Y0 + 1 - par);
       Real* zn = X.V(V_Z0 + 1 - par);
@@ -331,9 +344,10 @@ __device__ __forceinline__ void emit_interface(const Ctx<Gm>& X, const ColumnDev
 
 // ------------------------------------------------------------- one wavenumber
 template <class Gm>
-__device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int lmax,
+__device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, char* slot, int lmax,
                                        unsigned* status) {
   using Real = typename Gm::Real;
+  const Ctx<Gm> X(goff, t_, bar);
   using SLay = SlotLayout<Gm>;
   constexpr int NP = Gm::NP, G = Gm::G, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD;
   constexpr int TILE = SLay::TILE;
@@ -453,7 +467,7 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
     int nuse;
     double f;
     const double* chi = moments(0, nuse, f);
-    build_phase<Gm>(X, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+    build_phase<Gm>(X.goff, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
   }
 
   // ---------------- bottom composite: surface, or the lower boundary intensity
@@ -548,28 +562,30 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
         int nuse;
         double f;
         const double* chi = moments(l, nuse, f);
-        build_phase<Gm>(X, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+        build_phase<Gm>(X.goff, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
       }
-      tcur = doubling<Gm>(X, tau, om, Bt, Bb, lvTc[l], N, solar, F0, mu0, Ppp, Ppm, &singular);
+      tcur = doubling<Gm>(X.goff, t, X.bar, tau, om, Bt, Bb, lvTc[l], N, solar, F0, mu0, Ppp, Ppm,
+                          &singular);
       X.sync();
-      op_s2g<Gm>(X.m[0], rp, t);
-      op_s2g<Gm>(X.m[tcur], rp + TILE, t);
+      op_s2g<Gm>(X.mo(0), rp, t);
+      op_s2g<Gm>(X.mo(tcur), rp + TILE, t);
     }
     if (X.warp == 0 && X.lane < NP) rp[3 * TILE + X.lane] = X.V(V_SDN)[X.lane];
     if (t == 0) rp[3 * TILE + 2 * NP] = Real(scat);
 
     // adding: top = this layer, bottom = composite (src/adding.hpp:478-490)
-    Real* Rtm = X.m[tcur];  // layer T (row-major)
-    Real* spare = X.m[tcur ^ 1];
+    const unsigned oTl = X.mo(tcur);       // layer T (row-major)
+    const unsigned oSp = X.mo(tcur ^ 1);   // spare matrix
+    Real* Rtm = sp<Real>(oTl);
     if (!scat) {
       // non-scattering top (src/adding.hpp:349-406):
       // R_b <- t R_b t, U_b <- s_up + t (U_b + R_b s_dn)
-      op_g2s<Gm>(rb_below, nullptr, X.m[4], t);
+      op_g2s<Gm>(rb_below, kNoMat, X.mo(4), t);
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_SDN)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m[4], vv, yv, X.lane);
+        matvec<Gm, true, 1>(X.m(4), vv, yv, X.lane);
         if (X.lane < NP) {
           const int i = X.lane;
           X.V(V_UB)[i] = X.V(V_SUP)[i] + X.V(V_T)[i] * (X.V(V_UB)[i] + yv[0]);
@@ -594,33 +610,33 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
         __syncwarp();
         if (X.lane < NP) X.V(V_UB)[X.lane] = X.V(V_SUP)[X.lane] + yv[0];
       }
-      op_s2g<Gm>(X.m[0], rp + 2 * TILE, t);
+      op_s2g<Gm>(X.mo(0), rp + 2 * TILE, t);
       cs = 1;
     } else {
       // general (src/adding.hpp:301-342): A1 = I - R_b R, D1 = T A1^{-1},
       // U_b <- s_up + D1 (U_b + R_b s_dn), R_b <- R + (D1 R_b) T
-      op_g2s<Gm>(rb_below, X.m[5], X.m[4], t);  // R_b row-major (m5), column-major (m4)
+      op_g2s<Gm>(rb_below, X.mo(5), X.mo(4), t);  // R_b row-major (m5), column-major (m4)
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_SDN)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m[4], vv, yv, X.lane);
+        matvec<Gm, true, 1>(X.m(4), vv, yv, X.lane);
         if (X.lane < NP) X.V(V_TMP)[X.lane] = X.V(V_UB)[X.lane] + yv[0];
       }
-      op_gemm<Gm>(X.m[4], X.m[0], nullptr, 1, spare, nullptr, t);  // A1
+      op_gemm<Gm>(X.mo(4), X.mo(0), kNoMat, 1, oSp, kNoMat, t);  // A1
       X.sync();
-      singular |= op_gj<Gm>(spare, Rtm, nullptr, X.m[1], X.gjbuf, X.red, t, X.bar);  // D1 (cm)
+      singular |= op_gj<Gm>(oSp, oTl, kNoMat, X.mo(1), X.gjo(), X.redo(), t, X.bar);  // D1 (cm)
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_TMP)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m[1], vv, yv, X.lane);
+        matvec<Gm, true, 1>(X.m(1), vv, yv, X.lane);
         if (X.lane < NP) X.V(V_UB)[X.lane] = X.V(V_SUP)[X.lane] + yv[0];
       }
-      op_gemm<Gm>(X.m[1], X.m[5], nullptr, 0, nullptr, spare, t);  // D1 R_b (cm)
+      op_gemm<Gm>(X.mo(1), X.mo(5), kNoMat, 0, kNoMat, oSp, t);  // D1 R_b (cm)
       X.sync();
-      op_gemm<Gm>(spare, Rtm, X.m[0], 0, X.m[4], nullptr, t);  // R + (D1 R_b) T
-      op_s2g<Gm>(X.m[4], rp + 2 * TILE, t);
+      op_gemm<Gm>(oSp, oTl, X.mo(0), 0, X.mo(4), kNoMat, t);  // R + (D1 R_b) T
+      op_s2g<Gm>(X.mo(4), rp + 2 * TILE, t);
     }
     if (X.warp == 0) {
       __syncwarp();
@@ -631,14 +647,14 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
 
   // ---------------- downward pass and interface fluxes
   X.sync();
-  op_g2s<Gm>(recs + 2 * TILE, nullptr, X.m[0], t);  // R_base at the TOA (column-major)
+  op_g2s<Gm>(recs + 2 * TILE, kNoMat, X.mo(0), t);  // R_base at the TOA (column-major)
   X.sync();
   if (X.warp == 0) {
     if (X.lane < NP) X.V(V_ID)[X.lane] = (X.lane < N) ? static_cast<Real>(Btop) : Real(0);
     __syncwarp();
     const Real* vv[1] = {X.V(V_ID)};
     Real yv[1];
-    matvec<Gm, true, 1>(X.m[0], vv, yv, X.lane);
+    matvec<Gm, true, 1>(X.m(0), vv, yv, X.lane);
     if (X.lane < NP) X.V(V_IU)[X.lane] = yv[0] + X.V(V_UB)[X.lane];
     __syncwarp();
     if (X.lane == 0) emit_interface<Gm>(X, C, w, 0, N, solar, F0, mu0, lvTc, lvOmu, lvB, status);
@@ -649,9 +665,9 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
     const int scat = rl[3 * TILE + 2 * NP] != Real(0);
     const int cbase = rb[3 * TILE + 2 * NP + 1] != Real(0);
     X.sync();
-    op_g2s<Gm>(rl + TILE, nullptr, X.m[0], t);      // T (cm)
-    op_g2s<Gm>(rl, nullptr, X.m[1], t);             // R (cm)
-    op_g2s<Gm>(rb + 2 * TILE, X.m[2], nullptr, t);  // R_base (rm)
+    op_g2s<Gm>(rl + TILE, kNoMat, X.mo(0), t);      // T (cm)
+    op_g2s<Gm>(rl, kNoMat, X.mo(1), t);             // R (cm)
+    op_g2s<Gm>(rb + 2 * TILE, X.mo(2), kNoMat, t);  // R_base (rm)
     if (X.warp == 0 && X.lane < NP) {
       X.V(V_UB)[X.lane] = rb[3 * TILE + NP + X.lane];
       X.V(V_SDN)[X.lane] = rl[3 * TILE + X.lane];
@@ -662,8 +678,8 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
       const Real* v0[1] = {X.V(V_ID)};
       const Real* v1[1] = {X.V(V_UB)};
       Real a0[1], a1[1];
-      matvec<Gm, true, 1>(X.m[0], v0, a0, X.lane);
-      matvec<Gm, true, 1>(X.m[1], v1, a1, X.lane);
+      matvec<Gm, true, 1>(X.m(0), v0, a0, X.lane);
+      matvec<Gm, true, 1>(X.m(1), v1, a1, X.lane);
       if (X.lane < NP) X.V(V_RHS)[X.lane] = (a0[0] + a1[0]) + X.V(V_SDN)[X.lane];
     }
     X.sync();
@@ -671,11 +687,11 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
     int xstride = 1;
     if (scat && cbase) {
       // (I - R R_base) x = rhs, as x^T = rhs^T (I - R R_base)^{-T}
-      op_gemm<Gm>(X.m[2], X.m[1], nullptr, 1, X.m[3], nullptr, t);  // (I - R R_base)^T
+      op_gemm<Gm>(X.mo(2), X.mo(1), kNoMat, 1, X.mo(3), kNoMat, t);  // (I - R R_base)^T
       X.sync();
-      singular |= op_gj<Gm>(X.m[3], nullptr, X.V(V_RHS), X.m[4], X.gjbuf, X.red, t, X.bar);
+      singular |= op_gj<Gm>(X.mo(3), kNoMat, X.vo(V_RHS), X.mo(4), X.gjo(), X.redo(), t, X.bar);
       X.sync();
-      xsol = X.m[4];
+      xsol = X.m(4);
       xstride = LD;
     }
     if (X.warp == 0) {
@@ -683,7 +699,7 @@ __device__ __noinline__ void solve_one(const Ctx<Gm>& X, int w, char* slot, int 
       __syncwarp();
       const Real* vv[1] = {X.V(V_X)};
       Real yv[1];
-      matvec<Gm, false, 1>(X.m[2], vv, yv, X.lane);
+      matvec<Gm, false, 1>(X.m(2), vv, yv, X.lane);
       __syncwarp();
       if (X.lane < NP) {
         X.V(V_ID)[X.lane] = X.V(V_X)[X.lane];
@@ -703,16 +719,15 @@ template <int NP, typename Real>
 __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col0) {
   using Gm = Geo<NP, Real>;
   constexpr int G = Gm::G;
-  extern __shared__ __align__(16) char smem_raw[];
   const int gib = threadIdx.x / G;
   const int t = threadIdx.x % G;
-  char* smem = smem_raw + gib * SmemLayout<Gm>::bytes;
+  const unsigned goff = (unsigned)(gib * SmemLayout<Gm>::bytes);
   const int slot = blockIdx.x * (blockDim.x / G) + gib;
   char* sl = P.scratch + (size_t)slot * P.slot_bytes;
-  Ctx<Gm> X(smem, t, 1 + gib);
+  const Ctx<Gm> X(goff, t, 1 + gib);
   for (int i = t; i < 6 * Gm::DIM + 4; i += G) X.gjbuf[i] = Real(0);
   if (P.ncols <= 1 && t == 0) *X.col = col0;
-  long long* task_s = reinterpret_cast<long long*>(smem + SmemLayout<Gm>::misc + 48);
+  long long* task_s = sp<long long>(goff + SmemLayout<Gm>::misc + 48);
   int cur_col = -1;
   for (;;) {
     long long task;
@@ -742,7 +757,7 @@ __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col
       w = (int)(task - P.cols[lo].task_begin);
     }
     gsync<G>(1 + gib);
-    solve_one<Gm>(X, w, sl, P.max_layers, P.status);
+    solve_one<Gm>(goff, t, 1 + gib, w, sl, P.max_layers, P.status);
   }
 }
 

@@ -37,6 +37,26 @@
 
 namespace adrt_dev {
 
+#ifndef ADRT_DPAD
+#define ADRT_DPAD 2
+#endif
+#ifndef ADRT_GEMM_MMA
+#define ADRT_GEMM_MMA 1
+#endif
+
+// The block's dynamic shared memory.  Non-inlined operations take 32-bit
+// byte offsets into it (not pointers) and rebuild their pointers from this
+// symbol, so every shared access compiles to a 32-bit LDS/STS.
+extern __shared__ __align__(16) char adrt_smem[];
+
+template <typename T>
+__device__ __forceinline__ T* sp(unsigned off) {
+  return reinterpret_cast<T*>(adrt_smem + off);
+}
+__device__ __forceinline__ unsigned soff(const void* p) {
+  return static_cast<unsigned>(static_cast<const char*>(p) - adrt_smem);
+}
+
 // ============================================================== geometry
 template <int NP_, typename Real_>
 struct Geo {
@@ -49,7 +69,9 @@ struct Geo {
   static constexpr int TC = (NP + CB - 1) / CB;     // tile cols per thread
   static constexpr int TE = TR * TC;
   static constexpr int DIM = (RB * TR > CB * TC) ? RB * TR : CB * TC;
-  static constexpr int PAD = 16 / (int)sizeof(Real);  // rows stay 16-byte aligned
+  // Row padding keeps rows 16-byte aligned and spreads the rows of a column
+  // over the shared-memory banks.
+  static constexpr int PAD = (sizeof(Real) == 8) ? ADRT_DPAD : 4;
   static constexpr int LD = DIM + PAD;
   static constexpr int MAT = DIM * LD;                // Reals per smem matrix
   static constexpr int NW = G / 32;                   // warps per group
@@ -113,6 +135,9 @@ __device__ __forceinline__ unsigned gmax_u32(unsigned key, unsigned* red, int pa
     return r;
   }
 }
+
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 
 // ============================================================== vector smem access
 template <typename Real, int CNT>
@@ -194,16 +219,94 @@ struct Tile {
   }
 };
 
+// FP64 products on the tensor cores: mma.sync m8n8k4 f64 (the FP64 tensor
+// path of sm_100a; tcgen05 has no f64 kind).  Each warp owns WR x WC output
+// tiles of 8x8; lane (g = lane/4, q = lane%4) holds rows g, columns 2q, 2q+1
+// of each tile (the m8n8k4 accumulator fragment).
+template <class Gm>
+struct UseMMA {
+  static constexpr bool value =
+      ADRT_GEMM_MMA && sizeof(typename Gm::Real) == 8 && Gm::NP >= 8;
+};
+
+__device__ __forceinline__ void mma_f64_m8n8k4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <class Gm>
+__device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const double* __restrict__ Y,
+                                         const double* add, int id_minus, double* out_rm,
+                                         double* out_cm, int t) {
+  constexpr int NP = Gm::NP, LD = Gm::LD;
+  constexpr int NT = NP / 8;
+  constexpr int WR = (NT >= 2) ? 2 : 1, WC = WR;
+  constexpr int WPC = NT / WC;  // warps per tile-row band
+  static_assert((NT / WR) * WPC == Gm::G / 32, "warp grid must cover the tiles");
+  const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+  const int r0 = (warp / WPC) * WR * 8, c0 = (warp % WPC) * WC * 8;
+  double acc[WR][WC][2];
+#pragma unroll
+  for (int i = 0; i < WR; ++i)
+#pragma unroll
+    for (int j = 0; j < WC; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < NP / 4; ++ks) {
+    const int k = ks * 4 + q;
+    double a[WR], b[WC];
+#pragma unroll
+    for (int i = 0; i < WR; ++i) a[i] = XT[k * LD + r0 + i * 8 + g];
+#pragma unroll
+    for (int j = 0; j < WC; ++j) b[j] = Y[k * LD + c0 + j * 8 + g];
+#pragma unroll
+    for (int i = 0; i < WR; ++i)
+#pragma unroll
+      for (int j = 0; j < WC; ++j) mma_f64_m8n8k4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+  }
+#pragma unroll
+  for (int i = 0; i < WR; ++i)
+#pragma unroll
+    for (int j = 0; j < WC; ++j) {
+      const int r = r0 + i * 8 + g, c = c0 + j * 8 + 2 * q;
+      double v0 = acc[i][j][0], v1 = acc[i][j][1];
+      if (id_minus) {
+        v0 = ((r == c) ? 1.0 : 0.0) - v0;
+        v1 = ((r == c + 1) ? 1.0 : 0.0) - v1;
+      }
+      if (add) {
+        const double2 ad = *reinterpret_cast<const double2*>(add + r * LD + c);
+        v0 = ad.x + v0;
+        v1 = ad.y + v1;
+      }
+      if (out_rm) *reinterpret_cast<double2*>(out_rm + r * LD + c) = make_double2(v0, v1);
+      if (out_cm) {
+        out_cm[c * LD + r] = v0;
+        out_cm[(c + 1) * LD + r] = v1;
+      }
+    }
+}
+
 // out = [I -] X Y [+ add]: X column-major (XT[k*LD + r] = X[r][k]), Y and add
 // row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
 // alias out_rm (each thread reads its own tile before writing it).
+// Marks an absent optional operand (add / out_rm / out_cm / B / bvec).
+constexpr unsigned kNoMat = 0xffffffffu;
+
 template <class Gm>
-__device__ __noinline__ void op_gemm(const typename Gm::Real* __restrict__ XT,
-                                     const typename Gm::Real* __restrict__ Y,
-                                     const typename Gm::Real* add, int id_minus,
-                                     typename Gm::Real* out_rm, typename Gm::Real* out_cm, int t) {
+__device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned add_off,
+                                     int id_minus, unsigned orm_off, unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
+  const Real* __restrict__ XT = sp<Real>(xt_off);
+  const Real* __restrict__ Y = sp<Real>(y_off);
+  const Real* add = (add_off == kNoMat) ? nullptr : sp<Real>(add_off);
+  Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+  Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
+  if constexpr (UseMMA<Gm>::value) {
+    gemm_mma<Gm>(XT, Y, add, id_minus, out_rm, out_cm, t);
+    return;
+  }
   const Tile<Gm> tl(t);
   if (!tl.valid()) return;
   Real acc[TR][TC];
@@ -249,10 +352,16 @@ __device__ __noinline__ void op_gemm(const typename Gm::Real* __restrict__ XT,
 // the right-hand side is the single row `bvec` (a vector solve).  The result
 // is written column-major to out_cm.  Returns nonzero if a pivot was exactly 0.
 template <class Gm>
-__device__ __noinline__ int op_gj(const typename Gm::Real* A_rm, const typename Gm::Real* B_rm,
-                                  const typename Gm::Real* bvec, typename Gm::Real* out_cm,
-                                  typename Gm::Real* gjbuf, unsigned* red, int t, int bar) {
+__device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
+                                  unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
+                                  int bar) {
   using Real = typename Gm::Real;
+  const Real* A_rm = sp<Real>(a_off);
+  const Real* B_rm = (b_off == kNoMat) ? nullptr : sp<Real>(b_off);
+  const Real* bvec = (bvec_off == kNoMat) ? nullptr : sp<Real>(bvec_off);
+  Real* out_cm = sp<Real>(ocm_off);
+  Real* gjbuf = sp<Real>(gj_off);
+  unsigned* red = sp<unsigned>(red_off);
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP, DIM = Gm::DIM;
   constexpr int G = Gm::G;
   const Tile<Gm> tl(t);
@@ -315,7 +424,7 @@ __device__ __noinline__ int op_gj(const typename Gm::Real* A_rm, const typename 
 #pragma unroll
           for (int b = 1; b < TC; ++b)
             if (pb == b) piv = A[ka][b];
-          *invb = Real(1) / piv;
+          *invb = recip(piv);
         }
       }
       if (own_col) {
@@ -378,9 +487,11 @@ __device__ __noinline__ int op_gj(const typename Gm::Real* A_rm, const typename 
 // Tile copies between the HBM scratch (tile order: thread t owns TE
 // contiguous Reals) and smem.
 template <class Gm>
-__device__ __noinline__ void op_g2s(const typename Gm::Real* g, typename Gm::Real* out_rm,
-                                    typename Gm::Real* out_cm, int t) {
+__device__ __noinline__ void op_g2s(const typename Gm::Real* g, unsigned orm_off,
+                                    unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
+  Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+  Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
   constexpr int TR = Gm::TR, TC = Gm::TC;
   const Tile<Gm> tl(t);
   if (!tl.valid()) return;
@@ -395,8 +506,9 @@ __device__ __noinline__ void op_g2s(const typename Gm::Real* g, typename Gm::Rea
 }
 
 template <class Gm>
-__device__ __noinline__ void op_s2g(const typename Gm::Real* in_rm, typename Gm::Real* g, int t) {
+__device__ __noinline__ void op_s2g(unsigned in_off, typename Gm::Real* g, int t) {
   using Real = typename Gm::Real;
+  const Real* in_rm = sp<Real>(in_off);
   constexpr int TR = Gm::TR, TC = Gm::TC;
   const Tile<Gm> tl(t);
   if (!tl.valid()) return;
