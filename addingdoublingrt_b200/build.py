@@ -17,6 +17,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libadrt_b200.so")
+HOST_LIB = os.path.join(PKG, "libadrt_host.so")
+HOST_SOURCES = ["adrt_host.cpp"]
 
 SOURCES = ["adrt_engine.cu", "adrt_probe.cu"]
 HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh"]
@@ -37,12 +39,27 @@ def nvcc() -> str:
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(HOST_LIB):
         return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    t = min(os.path.getmtime(LIB), os.path.getmtime(HOST_LIB))
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS + HOST_SOURCES]
     deps.append(os.path.join(ROOT, "include", "adrt_b200.h"))
+    deps += [os.path.join(ROOT, "include", "adrt", f)
+             for f in ("adding_doubling.hpp", "cuda_solver.hpp", "constants.hpp")]
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build_host() -> str:
+    """The reference-compatible C++ API (adrt::solve, adrt::cuda::solveBatch)
+    over the C ABI: plain g++, linked against libadrt_b200.so."""
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "include")
+    tmp = HOST_LIB + ".tmp"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall",
+                    "-I", os.path.join(ROOT, "include"), "-I", cuda_inc,
+                    *[os.path.join(CSRC, f) for f in HOST_SOURCES],
+                    "-L", PKG, "-ladrt_b200", "-Wl,-rpath,$ORIGIN", "-o", tmp], check=True)
+    os.replace(tmp, HOST_LIB)
+    return HOST_LIB
 
 
 def build(verbose: bool = False, force: bool = False, extra=(), out: str | None = None) -> str:
@@ -65,6 +82,8 @@ def build(verbose: bool = False, force: bool = False, extra=(), out: str | None 
     subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp,
                     *objs, "-lcudart"], check=True)
     os.replace(tmp, target)
+    if out is None:
+        build_host()
     return target
 
 

@@ -71,29 +71,30 @@ void gauss_legendre01(int n, std::vector<double>& x, std::vector<double>& w) {
   }
 }
 
-// Kernel table: one instantiation per padded order and precision.
+// Kernel table: one instantiation per padded order and precision form.
 using LaunchFn = int (*)(const SolveParams&, const ColumnDev&, int grid, cudaStream_t);
 
-template <int NP, typename Real>
+template <int NP, int KIND>
 struct Kern {
-  using Gm = Geo<NP, Real>;
+  using GD = Geo<NP, double>;
   static constexpr int kThreads = 128;
-  static constexpr int kGroups = kThreads / Gm::G;
-  static size_t smem() { return (size_t)kGroups * SmemLayout<Gm>::bytes; }
-  static size_t slot_bytes(int lmax) { return SlotLayout<Gm>::bytes(lmax); }
+  static constexpr int kGroups = kThreads / GD::G;
+  static size_t smem() { return (size_t)kGroups * GroupLayout<NP, KIND>::bytes; }
+  // records are sized for FP64 (the mixed form's class-D wavenumbers)
+  static size_t slot_bytes(int lmax) { return SlotLayout<GD>::bytes(lmax); }
   static int max_blocks_per_sm() {
     static int cached = -1;
     if (cached < 0) {
-      cudaFuncSetAttribute(solve_kernel<NP, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(solve_kernel<NP, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem());
       int nb = 0;
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_kernel<NP, Real>, kThreads, smem());
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_kernel<NP, KIND>, kThreads, smem());
       cached = nb > 0 ? nb : 1;
     }
     return cached;
   }
   static int launch(const SolveParams& p, const ColumnDev& c0, int grid, cudaStream_t s) {
-    solve_kernel<NP, Real><<<grid, kThreads, smem(), s>>>(p, c0);
+    solve_kernel<NP, KIND><<<grid, kThreads, smem(), s>>>(p, c0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(ADRT_ERR_CUDA, "solve kernel launch: %s", cudaGetErrorString(e));
     return ADRT_OK;
@@ -107,10 +108,10 @@ struct KernInfo {
   LaunchFn launch;
 };
 
-template <int NP, typename Real>
+template <int NP, int KIND>
 KernInfo kinfo() {
-  return KernInfo{NP, Kern<NP, Real>::kGroups, &Kern<NP, Real>::slot_bytes,
-                  &Kern<NP, Real>::max_blocks_per_sm, &Kern<NP, Real>::launch};
+  return KernInfo{NP, Kern<NP, KIND>::kGroups, &Kern<NP, KIND>::slot_bytes,
+                  &Kern<NP, KIND>::max_blocks_per_sm, &Kern<NP, KIND>::launch};
 }
 
 int padded_order(int n) { return n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : 32; }
@@ -119,17 +120,17 @@ KernInfo pick(int n, int precision) {
   const int np = padded_order(n);
   if (precision == ADRT_PRECISION_MIXED) {
     switch (np) {
-      case 4: return kinfo<4, float>();
-      case 8: return kinfo<8, float>();
-      case 16: return kinfo<16, float>();
-      default: return kinfo<32, float>();
+      case 4: return kinfo<4, KIND_MIXED>();
+      case 8: return kinfo<8, KIND_MIXED>();
+      case 16: return kinfo<16, KIND_MIXED>();
+      default: return kinfo<32, KIND_MIXED>();
     }
   }
   switch (np) {
-    case 4: return kinfo<4, double>();
-    case 8: return kinfo<8, double>();
-    case 16: return kinfo<16, double>();
-    default: return kinfo<32, double>();
+    case 4: return kinfo<4, KIND_FP64>();
+    case 8: return kinfo<8, KIND_FP64>();
+    case 16: return kinfo<16, KIND_FP64>();
+    default: return kinfo<32, KIND_FP64>();
   }
 }
 
@@ -151,6 +152,9 @@ struct adrt_engine {
     int mmax = 0;
     QuadDev dev{};
   } quad[kMaxN + 1];
+  // FP64 staging of the FP32 entry point (grows outside stream capture only)
+  char* stage = nullptr;
+  size_t stage_bytes = 0;
   // host-entry staging buffers
   std::vector<void*> host_stage;
   std::mutex mu;
@@ -335,6 +339,69 @@ int ensure_scratch(adrt_engine* e, const KernInfo& k, int lmax, int* grid, size_
   return ADRT_OK;
 }
 
+// Element counts of the input (adrt_inputs field order) and output
+// (adrt_outputs field order) arrays of a batch.
+void input_counts(const adrt_batch_desc* d, size_t n[11]) {
+  const size_t W = d->num_wavenumbers, L = d->num_layers, M = d->num_moments;
+  n[0] = W * L;
+  n[1] = W * L;
+  n[2] = d->moment_layout == ADRT_MOMENTS_SHARED ? L * M
+         : d->moment_layout == ADRT_MOMENTS_PER_WAVENUMBER ? W * M : W * L * M;
+  n[3] = (d->temperature_per_wavenumber ? W : 1) * (L + 1);
+  n[4] = W * (L + 1);
+  for (int i = 5; i < 11; ++i) n[i] = W;
+}
+void output_counts(const adrt_batch_desc* d, size_t n[8]) {
+  const size_t W = d->num_wavenumbers, L = d->num_layers;
+  for (int i = 0; i < 5; ++i) n[i] = W * (L + 1);
+  for (int i = 5; i < 8; ++i) n[i] = W;
+}
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+__global__ void widen_kernel(const float* __restrict__ in, double* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+__global__ void narrow_kernel(const double* __restrict__ in, float* __restrict__ out, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = static_cast<float>(in[i]);
+}
+int cast_grid(size_t n, int num_sms) {
+  const size_t b = (n + 255) / 256;
+  const size_t cap = (size_t)num_sms * 8;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+// adrt_solve_batch after argument checks, with e->mu held.
+int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
+                 const adrt_outputs* out, cudaStream_t s) {
+  int rc;
+  if ((rc = set_device(e))) return rc;
+  e->last_stream = s;
+  if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
+  KernInfo k = pick(d->num_quadrature, d->precision);
+  int grid;
+  size_t sb;
+  if ((rc = ensure_scratch(e, k, d->num_layers, &grid, &sb))) return rc;
+  ColumnDev c0 = make_column(e, d, in, out);
+  SolveParams p{};
+  p.cols = nullptr;
+  p.ncols = 1;
+  p.ntasks = d->num_wavenumbers;
+  p.counter = e->counter;
+  p.status = e->status;
+  p.scratch = e->scratch;
+  p.slot_bytes = sb;
+  p.nslots = grid * k.groups;
+  p.max_layers = d->num_layers;
+  const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
+  grid = std::min(grid, need_blocks);
+  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+  return k.launch(p, c0, grid, s);
+}
+
 }  // namespace
 
 // ====================================================================== C ABI
@@ -383,6 +450,7 @@ int adrt_engine_destroy(adrt_engine* e) {
   cudaFree(e->d_cols);
   for (auto& q : e->quad) cudaFree(q.buf);
   for (void* p : e->host_stage) cudaFree(p);
+  cudaFree(e->stage);
   delete e;
   return ADRT_OK;
 }
@@ -460,29 +528,86 @@ int adrt_solve_batch(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs
   if ((rc = check_inputs(d, in))) return rc;
   if (!out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null outputs");
   std::lock_guard<std::mutex> lk(e->mu);
+  return solve_locked(e, d, in, out, static_cast<cudaStream_t>(stream_ptr));
+}
+
+int adrt_solve_batch_f32(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs_f32* in,
+                         const adrt_outputs_f32* out, void* stream_ptr) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  if (!in || !out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null inputs or outputs");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(e->mu);
   if ((rc = set_device(e))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
-  e->last_stream = s;
-  if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
-  KernInfo k = pick(d->num_quadrature, d->precision);
-  int grid;
-  size_t sb;
-  if ((rc = ensure_scratch(e, k, d->num_layers, &grid, &sb))) return rc;
-  ColumnDev c0 = make_column(e, d, in, out);
-  SolveParams p{};
-  p.cols = nullptr;
-  p.ncols = 1;
-  p.ntasks = d->num_wavenumbers;
-  p.counter = e->counter;
-  p.status = e->status;
-  p.scratch = e->scratch;
-  p.slot_bytes = sb;
-  p.nslots = grid * k.groups;
-  p.max_layers = d->num_layers;
-  const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
-  grid = std::min(grid, need_blocks);
-  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
-  return k.launch(p, c0, grid, s);
+  size_t nin[11], nout[8];
+  input_counts(d, nin);
+  output_counts(d, nout);
+  const float* const* fin = &in->delta_tau;
+  float* const* fout = &out->flux_up;
+  size_t need = 0;
+  for (int i = 0; i < 11; ++i)
+    if (fin[i]) need += align256(nin[i] * sizeof(double));
+  for (int i = 0; i < 8; ++i)
+    if (fout[i]) need += align256(nout[i] * sizeof(double));
+  if (need > e->stage_bytes) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE, "FP32 staging buffer too small during stream capture");
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->stage);
+    e->stage = nullptr;
+    e->stage_bytes = 0;
+    if (cudaMalloc(&e->stage, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "FP32 staging allocation of %zu B failed", need);
+    }
+    e->stage_bytes = need;
+  }
+  adrt_inputs din{};
+  adrt_outputs dout{};
+  const double** dinp = &din.delta_tau;
+  double** doutp = &dout.flux_up;
+  size_t off = 0;
+  for (int i = 0; i < 11; ++i) {
+    if (!fin[i]) continue;
+    double* dp = reinterpret_cast<double*>(e->stage + off);
+    off += align256(nin[i] * sizeof(double));
+    widen_kernel<<<cast_grid(nin[i], e->num_sms), 256, 0, s>>>(fin[i], dp, nin[i]);
+    dinp[i] = dp;
+  }
+  for (int i = 0; i < 8; ++i) {
+    if (!fout[i]) continue;
+    doutp[i] = reinterpret_cast<double*>(e->stage + off);
+    off += align256(nout[i] * sizeof(double));
+  }
+  CUDA_TRY(cudaGetLastError());
+  if ((rc = check_inputs(d, &din))) return rc;
+  if ((rc = solve_locked(e, d, &din, &dout, s))) return rc;
+  for (int i = 0; i < 8; ++i) {
+    if (!fout[i]) continue;
+    narrow_kernel<<<cast_grid(nout[i], e->num_sms), 256, 0, s>>>(doutp[i], fout[i], nout[i]);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return ADRT_OK;
+}
+
+int adrt_gauss_legendre(int n, double* nodes, double* weights) {
+  if (n < 1 || !nodes || !weights) return fail(ADRT_ERR_INVALID_ARGUMENT, "bad quadrature arguments");
+  std::vector<double> x, w;
+  gauss_legendre01(n, x, w);
+  std::copy(x.begin(), x.end(), nodes);
+  std::copy(w.begin(), w.end(), weights);
+  return ADRT_OK;
+}
+
+int adrt_planck_band(double lo, double hi, double temp, double* out) {
+  if (!out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null output");
+  if (temp < 0.0 || hi < lo || lo < 0.0)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "planckFunction: invalid arguments");
+  *out = planck_band(lo, hi, temp);
+  return ADRT_OK;
 }
 
 int adrt_solve_batch_uneven(adrt_engine* e, const adrt_column_desc* cols, int ncols,

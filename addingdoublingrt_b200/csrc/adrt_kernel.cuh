@@ -1,9 +1,53 @@
 // adrt_kernel.cuh -- per-wavenumber solve and the persistent batch kernel.
+//
+// Two precision forms share this code:
+//
+//   FP64    every operation in FP64, the doubling in the reference's own order
+//           (T-form: T <- T (I - R^2)^{-1} T, src/doubling.hpp:149-209).
+//   MIXED   per wavenumber, one of two classes (decided in the prologue):
+//     S     no ill-conditioned layer: every doubling in the FP32 Lambda-split
+//           form below, adding and interfaces in FP32;
+//     D     at least one ill-conditioned layer: those layers double in FP64
+//           (T-form), all others in FP32 Lambda-split form, and the adding,
+//           the composites and the interface solves run in FP64.
+//   A layer is ill-conditioned for FP32 when its first-order start is
+//   unstable (tau0 = tau 2^-nn above half the smallest quadrature cosine, so
+//   1 - tau0/mu is near zero or negative and the doubling amplifies
+//   round-off), when it is thick and near-conservative (1 - omega < 1e-2 with
+//   tau > 1: I - R^2 nearly singular), or when it needs more than 20
+//   doublings.
+//
+// Lambda-split doubling.  Write the layer transmission as T = Lambda + T'
+// with Lambda = diag((1 - tau0/mu_i)^(2^k)) (the first-order direct term,
+// squared exactly in FP64 at every doubling) and T' >= 0 the diffuse part.
+// With A = I - R^2 and G' = TG - Lambda = (Lambda R^2 + T') A^{-1}:
+//     TGR = Lambda R + G' R,      R <- R + TGR T,
+//     T'  <- G' T + Lambda T',    Lambda <- Lambda^2,   T = Lambda + T'.
+// The thermal recurrences (src/doubling.hpp:186-197) are carried in
+// a = z + g y >= 0 and b = z - g y <= 0, whose updates
+//     a <- TG (2a - b) - TGR b + a,   b <- TG b - TGR (2a - b) + 2b - a
+// and the solar ones are sums of same-signed terms, and the layer sources
+// follow as s_up = (a B_bot - b B_top)/tau + s_sol_up, s_dn = (a B_top -
+// b B_bot)/tau + s_sol_dn.  This is the reference's recurrence rewritten
+// exactly (equal in exact arithmetic); its FP32 evaluation keeps every
+// entry to FP32 relative accuracy for thin and thick streams alike, where
+// the reference-order FP32 evaluation loses (1 - T) for thin layers and the
+// small T of thick ones.  The beam factor gamma = exp(-tau0/mu0)^(2^k) is
+// squared in FP64.
 #pragma once
 
 #include "adrt_solver.cuh"
 
 namespace adrt_dev {
+
+constexpr int kFp64MaxDoublings = 20;           // more doublings -> FP64 layer
+constexpr double kFp64StartRatio = 0.5;         // tau0 > ratio * mu_min -> FP64 layer
+constexpr double kFp64NearConservative = 1e-2;  // 1 - omega below this ...
+constexpr double kFp64ThickTau = 1.0;           // ... with tau above this -> FP64 layer
+
+enum SolveMode { MODE_FP64 = 0, MODE_MIX_S = 1, MODE_MIX_D = 2 };
+enum KernelKind { KIND_FP64 = 0, KIND_MIXED = 1 };
+constexpr int kLevelArrays = 6;  // B, tau_cum, tau', omega', omega, FP64-layer flag
 
 // Per-slot HBM scratch of one thread group: level scalars, the phase
 // matrices of the current moment set, then one record per interface l =
@@ -18,7 +62,7 @@ struct SlotLayout {
   static constexpr int RALIGN = 16 / (int)sizeof(Real);
   static constexpr int REC = (REC_RAW + RALIGN - 1) / RALIGN * RALIGN;
   static __host__ __device__ size_t level_bytes(int lmax) {
-    return ((size_t)5 * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
+    return ((size_t)kLevelArrays * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t phase_bytes() {
     return ((size_t)2 * NP * NP * sizeof(double) + 255) & ~size_t(255);
@@ -28,42 +72,79 @@ struct SlotLayout {
   }
 };
 
-// Pointers into one group's shared memory.  Built inside every function
-// from the group's byte offset `goff` into adrt_smem, so the compiler sees
-// shared-space pointers; non-inlined calls receive (goff, t, bar).
+// Shared-memory bytes of one group for a kernel kind: the common prefix and
+// one typed region (FP64), or for the mixed kind the larger of the FP32
+// class-S layout and the class-D layout (FP64 vectors and buffers followed
+// by room for both the FP64 matrices and the FP32 Lambda-split region).
+template <int NP, int KIND>
+struct GroupLayout {
+  using GD = Geo<NP, double>;
+  using GF = Geo<NP, float>;
+  static constexpr size_t cbytes = CommonLayout<NP>::bytes;
+  static constexpr size_t fp64 = TypedLayout<GD, kMatsTForm>::bytes;
+  static constexpr size_t lamF = TypedLayout<GF, kMatsLam>::bytes;
+  static constexpr size_t dmats = TypedLayout<GD, kMatsTForm>::bytes - TypedLayout<GD, 0>::bytes;
+  static constexpr size_t classD = TypedLayout<GD, 0>::bytes + (dmats > lamF ? dmats : lamF);
+  static constexpr size_t typed = (KIND == KIND_FP64) ? fp64 : (classD > lamF ? classD : lamF);
+  static constexpr size_t bytes = align16(cbytes + typed);
+  // typed-region offset of the FP32 region inside a class-D group
+  static constexpr size_t lamF_in_D = TypedLayout<GD, 0>::bytes;
+};
+
+// Pointers into one group's shared memory: the common prefix at `goff`, the
+// typed region (Real view) at `tb` (both absolute byte offsets into
+// adrt_smem).  Built inside every function so the compiler sees
+// shared-space pointers; non-inlined calls receive (goff, tb, t, bar).
 template <class Gm>
 struct Ctx {
   using Real = typename Gm::Real;
-  using SL = SmemLayout<Gm>;
+  using CL = CommonLayout<Gm::NP>;
+  using TL = TypedLayout<Gm, 0>;
   static constexpr int NP = Gm::NP, MAT = Gm::MAT;
-  unsigned goff;
+  unsigned goff, tb;
   int t, lane, warp, bar;
   Real *vec, *gjbuf;
   double* dvec;
   ColumnDev* col;
   unsigned* red;
-  double* dmisc;
-  __device__ __forceinline__ Ctx(unsigned goff_, int t_, int bar_)
-      : goff(goff_), t(t_), lane(t_ & 31), warp(t_ >> 5), bar(bar_) {
-    vec = sp<Real>(goff + SL::vecs);
-    gjbuf = sp<Real>(goff + SL::gj);
-    dvec = sp<double>(goff + SL::dvecs);
-    col = sp<ColumnDev>(goff + SL::col);
-    red = sp<unsigned>(goff + SL::misc);
-    dmisc = sp<double>(goff + SL::misc + 32);
+  double* sc;
+  __device__ __forceinline__ Ctx(unsigned goff_, unsigned tb_, int t_, int bar_)
+      : goff(goff_), tb(tb_), t(t_), lane(t_ & 31), warp(t_ >> 5), bar(bar_) {
+    vec = sp<Real>(tb + TL::vecs);
+    gjbuf = sp<Real>(tb + TL::gj);
+    dvec = sp<double>(goff + CL::dvecs);
+    col = sp<ColumnDev>(goff + CL::col);
+    red = sp<unsigned>(goff + CL::misc);
+    sc = sp<double>(goff + CL::misc + 48);
   }
   __device__ __forceinline__ unsigned mo(int i) const {
-    return goff + (unsigned)(SL::mats + (size_t)i * MAT * sizeof(Real));
+    return tb + (unsigned)(TL::mats + (size_t)i * MAT * sizeof(Real));
   }
   __device__ __forceinline__ Real* m(int i) const { return sp<Real>(mo(i)); }
   __device__ __forceinline__ unsigned vo(int s) const {
-    return goff + (unsigned)(SL::vecs + (size_t)s * NP * sizeof(Real));
+    return tb + (unsigned)(TL::vecs + (size_t)s * NP * sizeof(Real));
   }
-  __device__ __forceinline__ unsigned gjo() const { return goff + (unsigned)SL::gj; }
-  __device__ __forceinline__ unsigned redo() const { return goff + (unsigned)SL::misc; }
+  __device__ __forceinline__ unsigned dvo(int s) const {
+    return goff + (unsigned)(CL::dvecs + (size_t)s * NP * sizeof(double));
+  }
+  __device__ __forceinline__ unsigned gjo() const { return tb + (unsigned)TL::gj; }
+  __device__ __forceinline__ unsigned redo() const { return goff + (unsigned)CL::misc; }
   __device__ __forceinline__ Real* V(int s) const { return vec + s * NP; }
   __device__ __forceinline__ double* DV(int s) const { return dvec + s * NP; }
   __device__ __forceinline__ void sync() const { gsync<Gm::G>(bar); }
+};
+
+// Level arrays of one slot.
+struct Levels {
+  double *B, *tc, *tau, *om, *omu, *flag;
+  __device__ __forceinline__ Levels(char* slot, int lmax) {
+    B = reinterpret_cast<double*>(slot);
+    tc = B + (lmax + 1);
+    tau = tc + (lmax + 1);
+    om = tau + (lmax + 1);
+    omu = om + (lmax + 1);
+    flag = omu + (lmax + 1);
+  }
 };
 
 // ------------------------------------------------------------- phase matrices
@@ -73,11 +154,12 @@ struct Ctx {
 // 131-181) into D_PP / D_PM.  chi_l = (chi[l] - f) / (1 - f) when delta-M
 // truncation applies (f >= 0), chi[l] otherwise.
 template <class Gm>
-__device__ __noinline__ void build_phase(unsigned goff, int t_, int bar, const double* chi,
-                                         int nuse, double f, int N, const double* pl, bool solar,
-                                         double mu0, double* Ppp, double* Ppm) {
+__device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
+                                         const double* chi, int nuse, double f, int N,
+                                         const double* pl, bool solar, double mu0, double* Ppp,
+                                         double* Ppm) {
   constexpr int NP = Gm::NP, G = Gm::G;
-  const Ctx<Gm> X(goff, t_, bar);
+  const Ctx<Gm> X(goff, tb, t_, bar);
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
@@ -158,19 +240,19 @@ __device__ __noinline__ void build_phase(unsigned goff, int t_, int bar, const d
   X.sync();
 }
 
-// ------------------------------------------------------------- doubling
+// ------------------------------------------------------------- doubling (reference order)
 // One homogeneous scattering layer (src/doubling.hpp:79-229): first-order
 // thin-layer start at tau0 = tau 2^-nn, then nn doublings of R, T and of the
 // thermal (y, z) and solar sources.  On return R is in m[0] (row-major) and
 // m[1] (column-major), T in m[return value] (row-major, 2 or 3), and the
 // combined thermal + solar sources in V_SUP / V_SDN.
 template <class Gm>
-__device__ __noinline__ int doubling(unsigned goff, int t_, int bar, double tau, double om,
-                                     double Bt, double Bb, double tcum, int N, bool solar,
-                                     double F0, double mu0, const double* Ppp, const double* Ppm,
-                                     int* singular) {
+__device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
+                                     double om, double Bt, double Bb, double tcum, int N,
+                                     bool solar, double F0, double mu0, const double* Ppp,
+                                     const double* Ppm, int* singular) {
   using Real = typename Gm::Real;
-  const Ctx<Gm> X(goff, t_, bar);
+  const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC;
   const int t = X.t;
   const double* mu = X.DV(D_MU);
@@ -303,12 +385,216 @@ __device__ __noinline__ int doubling(unsigned goff, int t_, int bar, double tau,
   return 2 + cur;
 }
 
+// ------------------------------------------------------------- doubling (Lambda-split, FP32)
+// Same layer, same discrete scheme, evaluated in the Lambda-split form
+// described at the top of this file.  Buffers: m0/m1 R (row/column-major),
+// m2/m3 T (row-major, ping-pong), m4 I - R^2 then TGR (column-major), m5 G'
+// (column-major), m6/m7 T' (row-major, ping-pong), m8 the right-hand side
+// Lambda R^2 + T'.  Returns the T buffer index like doubling(); the layer
+// sources are left in V_SUP / V_SDN (Real) and, when src64 is given, also in
+// FP64 in src64[0..NP) (up) and src64[NP..2NP) (down).
+template <class Gm>
+__device__ __noinline__ int doubling_lam(unsigned goff, unsigned tb, int t_, int bar, double tau,
+                                         double om, double Bt, double Bb, double tcum, int N,
+                                         bool solar, double F0, double mu0, const double* Ppp,
+                                         const double* Ppm, int* singular, double* src64) {
+  using Real = typename Gm::Real;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC;
+  const int t = X.t;
+  const double* mu = X.DV(D_MU);
+  const double* wt = X.DV(D_WT);
+  om = om > 1.0 ? 1.0 : om;
+  const double con = 2.0 * om * kPi;
+  const int nn = num_doublings(tau, om);
+  const double tau0 = ldexp(tau, -nn);
+  const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
+  const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oG = X.mo(5), oRHS = X.mo(8);
+  const unsigned oT[2] = {X.mo(2), X.mo(3)};
+  const unsigned oTp[2] = {X.mo(6), X.mo(7)};
+  const unsigned oLam[2] = {X.dvo(D_LAM0), X.dvo(D_LAM1)};
+  // first-order start: R = tau0 Gpm, T' = tau0 con Ppp w / mu, Lambda = 1 - tau0/mu
+  {
+    const Tile<Gm> tl(t);
+    if (tl.valid()) {
+      Real Rt[TR][TC], Tp[TR][TC], Tt[TR][TC];
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          const int r = tl.row(a), c = tl.col(b);
+          double rv = 0.0, tp = 0.0, tv = (r == c) ? 1.0 : 0.0;
+          if (r < N && c < N) {
+            rv = tau0 * (con * (Ppm[r * NP + c] * wt[c]) / mu[r]);
+            tp = tau0 * (con * (Ppp[r * NP + c] * wt[c]) / mu[r]);
+            tv = tp + ((r == c) ? 1.0 - tau0 / mu[r] : 0.0);
+          }
+          Rt[a][b] = static_cast<Real>(rv);
+          Tp[a][b] = static_cast<Real>(tp);
+          Tt[a][b] = static_cast<Real>(tv);
+        }
+      tl.store_rm(Rt, sp<Real>(oR));
+      tl.store_cm(Rt, sp<Real>(oRc));
+      tl.store_rm(Tp, sp<Real>(oTp[0]));
+      tl.store_rm(Tt, sp<Real>(oT[0]));
+    }
+  }
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane;
+    double a = 0.0, su = 0.0, sd = 0.0, lam = 1.0;
+    if (i < N) {
+      lam = 1.0 - tau0 / mu[i];
+      a = 0.5 * tau0 * ((1.0 - om) * tau0 / mu[i]);  // g y at the start
+      if (solar) {
+        const double base = om * tau0 / mu[i] * Ftop;
+        su = base * X.DV(D_PM)[i];
+        sd = base * X.DV(D_PP)[i];
+      }
+    }
+    X.DV(D_LAM0)[i] = lam;
+    X.V(V_Y0)[i] = static_cast<Real>(a);
+    X.V(V_Z0)[i] = static_cast<Real>(-a);
+    X.V(V_SU0)[i] = static_cast<Real>(su);
+    X.V(V_SD0)[i] = static_cast<Real>(sd);
+  }
+  double gam = solar ? exp(-tau0 / mu0) : 0.0;
+  int cur = 0;
+  for (int k = 0; k < nn; ++k) {
+    const int par = k & 1;
+    Real* av = X.V(V_Y0 + par);
+    Real* bv = X.V(V_Z0 + par);
+    Real* su = X.V(V_SU0 + par);
+    Real* sd = X.V(V_SD0 + par);
+    const double* lam = X.DV(D_LAM0 + par);
+    const Real gm = static_cast<Real>(gam);
+    X.sync();  // R, T, T', Lambda and the vectors of the previous step are complete
+    if (solar && X.warp == 0) {  // ru = R sd + gam su, rd = gam R su + sd (old R)
+      const Real* vv[2] = {sd, su};
+      Real yv[2];
+      matvec<Gm, true, 2>(sp<Real>(oRc), vv, yv, X.lane);
+      if (X.lane < NP) {
+        X.V(V_RU)[X.lane] = yv[0] + gm * su[X.lane];
+        X.V(V_RD)[X.lane] = gm * yv[1] + sd[X.lane];
+      }
+    }
+    // A = I - R^2, RHS = Lambda R^2 + T'
+    op_gemm_lam<Gm>(oRc, oR, oTp[cur], oLam[par], kLamR2, oA, kNoMat, oRHS, t);
+    X.sync();
+    *singular |= op_gj<Gm>(oA, oRHS, kNoMat, oG, X.gjo(), X.redo(), t, X.bar);  // G' (cm)
+    X.sync();
+    op_gemm_lam<Gm>(oG, oR, oR, oLam[par], kLamAdd, kNoMat, oA, kNoMat, t);  // TGR (cm)
+    X.sync();
+    op_gemm<Gm>(oA, oT[cur], oR, 0, oR, oRc, t);  // R <- R + TGR T
+    // T' <- G' T + Lambda T', T <- T' + Lambda^2
+    op_gemm_lam<Gm>(oG, oT[cur], oTp[cur], oLam[par], kLamAdd, oTp[cur ^ 1], kNoMat, oT[cur ^ 1],
+                    t);
+    if (X.warp == 0) {
+      Real* an = X.V(V_Y0 + 1 - par);
+      Real* bn = X.V(V_Z0 + 1 - par);
+      Real* sun = X.V(V_SU0 + 1 - par);
+      Real* sdn = X.V(V_SD0 + 1 - par);
+      if (X.lane < NP) X.V(V_TMP)[X.lane] = Real(2) * av[X.lane] - bv[X.lane];
+      __syncwarp();
+      const Real* vc[2] = {X.V(V_TMP), bv};
+      Real gv[2], rv[2];
+      matvec<Gm, true, 2>(sp<Real>(oG), vc, gv, X.lane);  // G' c, G' b
+      matvec<Gm, true, 2>(sp<Real>(oA), vc, rv, X.lane);  // TGR c, TGR b
+      Real gs[2] = {Real(0), Real(0)};
+      if (solar) {
+        const Real* vs[2] = {X.V(V_RU), X.V(V_RD)};
+        matvec<Gm, true, 2>(sp<Real>(oG), vs, gs, X.lane);
+      }
+      if (X.lane < NP) {
+        const int i = X.lane;
+        const Real l = static_cast<Real>(lam[i]);
+        const Real c = X.V(V_TMP)[i], a = av[i], b = bv[i];
+        an[i] = ((l * c + gv[0]) - rv[1]) + a;
+        bn[i] = ((l * b + gv[1]) - rv[0]) + (Real(2) * b - a);
+        if (solar) {
+          sun[i] = (l * X.V(V_RU)[i] + gs[0]) + su[i];
+          sdn[i] = (l * X.V(V_RD)[i] + gs[1]) + gm * sd[i];
+        } else {
+          sun[i] = Real(0);
+          sdn[i] = Real(0);
+        }
+        X.DV(D_LAM0 + 1 - par)[i] = lam[i] * lam[i];
+      }
+    }
+    gam = gam * gam;
+    cur ^= 1;
+  }
+  X.sync();
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane, par = nn & 1;
+    const double a = X.V(V_Y0 + par)[i], b = X.V(V_Z0 + par)[i];
+    const double su = X.V(V_SU0 + par)[i], sd = X.V(V_SD0 + par)[i];
+    double up = 0.0, dn = 0.0;
+    if (i < N) {
+      up = (a * Bb - b * Bt) / tau + su;
+      dn = (a * Bt - b * Bb) / tau + sd;
+    }
+    X.V(V_SUP)[i] = static_cast<Real>(up);
+    X.V(V_SDN)[i] = static_cast<Real>(dn);
+    if (src64) {
+      src64[i] = up;
+      src64[NP + i] = dn;
+    }
+  }
+  return 2 + cur;
+}
+
+// Class-D layers that double in FP32: run doubling_lam in the FP32 region
+// at `tbF` (which overlays this group's FP64 matrices), then widen R, T and
+// the sources into the FP64 buffers the adding reads (R -> m0 row-major,
+// T -> m2 row-major, sources -> V_SUP / V_SDN).  src64 is 2 NP doubles of
+// global scratch that carry the FP64 sources across.
+template <class GmD>
+__device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsigned tbF, int t_,
+                                              int bar, double tau, double om, double Bt,
+                                              double Bb, double tcum, int N, bool solar,
+                                              double F0, double mu0, const double* Ppp,
+                                              const double* Ppm, int* singular,
+                                              double* src64) {
+  using GmF = Geo<GmD::NP, float>;
+  constexpr int TR = GmD::TR, TC = GmD::TC, NP = GmD::NP;
+  static_assert(GmF::TR == TR && GmF::TC == TC && GmF::G == GmD::G, "tile maps must agree");
+  const int tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0,
+                                   Ppp, Ppm, singular, src64);
+  const Ctx<GmF> XF(goff, tbF, t_, bar);
+  const Ctx<GmD> XD(goff, tbD, t_, bar);
+  XD.sync();
+  const Tile<GmF> tf(XF.t);
+  const Tile<GmD> td(XD.t);
+  float Rf[TR][TC], Tf[TR][TC];
+  if (tf.valid()) {
+    tf.load_rm(Rf, XF.m(0));
+    tf.load_rm(Tf, XF.m(tF));
+  }
+  XD.sync();  // the FP64 buffers overlay the FP32 region
+  if (td.valid()) {
+    double Rd[TR][TC], Td[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) {
+        Rd[a][b] = Rf[a][b];
+        Td[a][b] = Tf[a][b];
+      }
+    td.store_rm(Rd, XD.m(0));
+    td.store_rm(Td, XD.m(2));
+  }
+  if (XD.warp == 0 && XD.lane < NP) {
+    XD.V(V_SUP)[XD.lane] = src64[XD.lane];
+    XD.V(V_SDN)[XD.lane] = src64[NP + XD.lane];
+  }
+  return 2;
+}
+
 // ------------------------------------------------------------- interface output
 template <class Gm>
 __device__ __forceinline__ void emit_interface(const Ctx<Gm>& X, const ColumnDev* C, int w, int l,
                                                int N, bool solar, double F0, double mu0,
-                                               const double* lvTc, const double* lvOmu,
-                                               const double* lvB, unsigned* status) {
+                                               const Levels& lv, unsigned* status) {
   const typename Gm::Real* iu = X.V(V_IU);
   const typename Gm::Real* id = X.V(V_ID);
   const double* cw = X.DV(D_CW);
@@ -322,12 +608,12 @@ __device__ __forceinline__ void emit_interface(const Ctx<Gm>& X, const ColumnDev
   }
   double fdir = 0.0;
   if (solar) {
-    fdir = (l == 0) ? F0 * mu0 : F0 * mu0 * exp(-lvTc[l] / mu0);
+    fdir = (l == 0) ? F0 * mu0 : F0 * mu0 * exp(-lv.tc[l] / mu0);
     J += fdir * (1.0 / (4.0 * kPi * mu0));
   }
   const int nL = C->L;
   const int lyr = (l == 0) ? 0 : l - 1;
-  const double divF = 4.0 * kPi * (1.0 - lvOmu[lyr]) * (J - lvB[l]);
+  const double divF = 4.0 * kPi * (1.0 - lv.omu[lyr]) * (J - lv.B[l]);
   const size_t oi = (size_t)w * (nL + 1) + (C->from_bottom ? nL - l : l);
   if (C->fu) C->fu[oi] = fu;
   if (C->fd) C->fd[oi] = fd;
@@ -342,38 +628,25 @@ __device__ __forceinline__ void emit_interface(const Ctx<Gm>& X, const ColumnDev
   if (!isfinite(fu) || !isfinite(fd) || !isfinite(J)) atomicOr(status, 2u);
 }
 
-// ------------------------------------------------------------- one wavenumber
-template <class Gm>
-__device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, char* slot, int lmax,
-                                       unsigned* status) {
-  using Real = typename Gm::Real;
-  const Ctx<Gm> X(goff, t_, bar);
-  using SLay = SlotLayout<Gm>;
-  constexpr int NP = Gm::NP, G = Gm::G, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD;
-  constexpr int TILE = SLay::TILE;
+// ------------------------------------------------------------- prologue
+// Quadrature constants, Planck levels, delta-M scaled optical properties
+// (src/solver.cpp:385-514), cumulative scaled tau and the boundary sources;
+// with `mixed`, also the per-layer FP64 flags of the mixed form.  Returns
+// (group-uniform) whether any layer is flagged.
+template <int NP>
+__device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, char* slot,
+                                         int lmax, unsigned* status, int mixed) {
+  using Gm = Geo<NP, double>;
+  constexpr int G = Gm::G;
+  const Ctx<Gm> X(goff, goff, t_, bar);  // common prefix only
   const ColumnDev* C = X.col;
   const int t = X.t;
   const int N = C->N, nL = C->L, M = C->M, layout = C->moment_layout;
   const int from_bottom = C->from_bottom;
-
-  const double A = C->albedo_w ? C->albedo_w[w] : C->surface_albedo;
-  const double mu0 = C->mu0_w ? C->mu0_w[w] : C->solar_mu;
   const double wlo = C->wlo_w ? C->wlo_w[w] : C->wn_lo;
   const double whi = C->whi_w ? C->whi_w[w] : C->wn_hi;
-  const double F0 = C->solar_flux;
-  const bool solar = (F0 > 0.0 && mu0 > 0.0);
+  const Levels lv(slot, lmax);
 
-  double* lvB = reinterpret_cast<double*>(slot);
-  double* lvTc = lvB + (lmax + 1);
-  double* lvTau = lvTc + (lmax + 1);
-  double* lvOm = lvTau + (lmax + 1);
-  double* lvOmu = lvOm + (lmax + 1);
-  double* Ppp = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
-  double* Ppm = Ppp + NP * NP;
-  Real* recs = reinterpret_cast<Real*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
-  const double* chi_base = C->moments;
-
-  // ---------------- quadrature constants for this column
   if (t < NP) {
     double mu = 1.0, wt = 0.0;
     if (t < N) {
@@ -385,8 +658,6 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
     X.DV(D_CW)[t] = 2.0 * kPi * wt * mu;
     X.DV(D_HW)[t] = 0.5 * wt;
   }
-
-  // ---------------- prologue: Planck levels, scaled optical properties
   unsigned bad = 0;
   for (int l = t; l <= nL; l += G) {
     const int ul = from_bottom ? nL - l : l;
@@ -398,18 +669,20 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
     } else if (C->planck) {
       Bv = C->planck[(size_t)w * (nL + 1) + ul];
     }
-    lvB[l] = Bv;
+    lv.B[l] = Bv;
   }
+  const double mu_min = C->quad.mu[0];
+  unsigned flagged = 0;
   for (int l = t; l < nL; l += G) {
     const int u = from_bottom ? nL - 1 - l : l;
     double tau = C->dtau[(size_t)w * nL + u];
     double om = C->ssa[(size_t)w * nL + u];
     if (!(tau >= 0.0 && tau < 1e300) || !(om >= 0.0 && om <= 1.0)) bad = 1;
-    lvOmu[l] = om;
+    lv.omu[l] = om;
     if (om > 0.0 && tau > 0.0 && C->delta_m && M > 2 * N) {
-      const double* chi = chi_base + (layout == 0 ? (size_t)u * M
-                                      : layout == 1 ? (size_t)w * M
-                                                    : ((size_t)w * nL + u) * M);
+      const double* chi = C->moments + (layout == 0 ? (size_t)u * M
+                                        : layout == 1 ? (size_t)w * M
+                                                      : ((size_t)w * nL + u) * M);
       const double f = chi[2 * N];
       if (f > 1e-12 && f < 1.0 - 1e-12) {
         const double of = om * f;
@@ -417,31 +690,75 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
         om = om * (1.0 - f) / (1.0 - of);
       }
     }
-    lvTau[l] = tau;
-    lvOm[l] = om;
+    lv.tau[l] = tau;
+    lv.om[l] = om;
+    double fl = 0.0;
+    if (mixed && tau > 0.0 && om > 0.0) {
+      const double omc = om > 1.0 ? 1.0 : om;
+      const int nn = num_doublings(tau, omc);
+      const double tau0 = ldexp(tau, -nn);
+      if (nn > kFp64MaxDoublings || tau0 > kFp64StartRatio * mu_min ||
+          (1.0 - omc < kFp64NearConservative && tau > kFp64ThickTau)) {
+        fl = 1.0;
+        flagged = 1;
+      }
+    }
+    lv.flag[l] = fl;
   }
   if (bad) atomicOr(status, 4u);
+  const unsigned any = gmax_u32<G>(flagged, X.red, 0, bar);
   X.sync();
   if (t == 0) {
     double tc = 0.0;
-    lvTc[0] = 0.0;
+    lv.tc[0] = 0.0;
     for (int l = 0; l < nL; ++l) {
-      tc += lvTau[l];
-      lvTc[l + 1] = tc;
+      tc += lv.tau[l];
+      lv.tc[l + 1] = tc;
     }
     double Bs, Btop;
     if (C->thermal) {
-      Bs = (C->surface_temperature >= 0.0) ? planck_band(wlo, whi, C->surface_temperature) : lvB[nL];
-      Btop = (C->top_temperature >= 0.0) ? planck_band(wlo, whi, C->top_temperature) : lvB[0];
+      Bs = (C->surface_temperature >= 0.0) ? planck_band(wlo, whi, C->surface_temperature)
+                                           : lv.B[nL];
+      Btop = (C->top_temperature >= 0.0) ? planck_band(wlo, whi, C->top_temperature) : lv.B[0];
     } else {
       Bs = C->semis_w ? C->semis_w[w] : C->surface_emission;
       Btop = C->temis_w ? C->temis_w[w] : C->top_emission;
     }
-    X.dmisc[0] = Bs;
-    X.dmisc[1] = Btop;
+    X.sc[S_BS] = Bs;
+    X.sc[S_BTOP] = Btop;
   }
   X.sync();
-  const double Bs = X.dmisc[0], Btop = X.dmisc[1];
+  return any != 0u;
+}
+
+// ------------------------------------------------------------- one wavenumber
+// Everything after the prologue, in the Real type of Gm: phase matrices,
+// bottom composite, upward doubling + adding, downward pass and fluxes.
+// MODE picks the doubling form per layer (see the top of this file); tbF is
+// the FP32 region of a class-D group.
+template <class Gm, int MODE>
+__device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, int t_, int bar,
+                                      int w, char* slot, int lmax, unsigned* status) {
+  using Real = typename Gm::Real;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  using SLay = SlotLayout<Gm>;
+  constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC;
+  constexpr int TILE = SLay::TILE;
+  const ColumnDev* C = X.col;
+  const int t = X.t;
+  const int N = C->N, nL = C->L, M = C->M, layout = C->moment_layout;
+  const int from_bottom = C->from_bottom;
+
+  const double A = C->albedo_w ? C->albedo_w[w] : C->surface_albedo;
+  const double mu0 = C->mu0_w ? C->mu0_w[w] : C->solar_mu;
+  const double F0 = C->solar_flux;
+  const bool solar = (F0 > 0.0 && mu0 > 0.0);
+  const Levels lv(slot, lmax);
+  double* Ppp = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
+  double* Ppm = Ppp + NP * NP;
+  Real* recs = reinterpret_cast<Real*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
+  const double* chi_base = C->moments;
+  const double Bs = X.sc[S_BS], Btop = X.sc[S_BTOP];
   const bool has_surface = !C->diffusion && (A > 0.0 || Bs > 0.0);
 
   // moment set of internal layer l: pointer, effective count, delta-M fraction
@@ -467,7 +784,8 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
     int nuse;
     double f;
     const double* chi = moments(0, nuse, f);
-    build_phase<Gm>(X.goff, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+    build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
+                    Ppm);
   }
 
   // ---------------- bottom composite: surface, or the lower boundary intensity
@@ -477,8 +795,8 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
     const double* wt = X.DV(D_WT);
     double dB = 0.0;
     if (C->diffusion) {
-      const double dt = lvTau[nL - 1];
-      dB = (dt > 0.0) ? (lvB[nL] - lvB[nL - 1]) / dt : 0.0;
+      const double dt = lv.tau[nL - 1];
+      dB = (dt > 0.0) ? (lv.B[nL] - lv.B[nL - 1]) / dt : 0.0;
     }
     Real* rp = recs + (size_t)nL * SLay::REC;
     const Tile<Gm> tl(t);
@@ -500,9 +818,9 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
       if (i < N) {
         if (has_surface) {
           u = (1.0 - A) * Bs;
-          if (solar && A > 0.0) u = u + (A / kPi) * F0 * mu0 * exp(-lvTc[nL] / mu0);
+          if (solar && A > 0.0) u = u + (A / kPi) * F0 * mu0 * exp(-lv.tc[nL] / mu0);
         } else if (C->diffusion) {
-          u = lvB[nL] + mu[i] * dB;
+          u = lv.B[nL] + mu[i] * dB;
         } else {
           u = Bs;
         }
@@ -517,8 +835,8 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
   // ---------------- upward: doubling + adding onto the composite below
   int singular = 0;
   for (int l = nL - 1; l >= 0; --l) {
-    const double tau = lvTau[l], om = lvOm[l];
-    const double Bt = lvB[l], Bb = lvB[l + 1];
+    const double tau = lv.tau[l], om = lv.om[l];
+    const double Bt = lv.B[l], Bb = lv.B[l + 1];
     const int scat = (tau > 0.0 && om > 0.0);
     Real* rp = recs + (size_t)l * SLay::REC;
     Real* rb_below = recs + (size_t)(l + 1) * SLay::REC + 2 * TILE;
@@ -562,10 +880,25 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
         int nuse;
         double f;
         const double* chi = moments(l, nuse, f);
-        build_phase<Gm>(X.goff, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+        build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
+                    Ppm);
       }
-      tcur = doubling<Gm>(X.goff, t, X.bar, tau, om, Bt, Bb, lvTc[l], N, solar, F0, mu0, Ppp, Ppm,
-                          &singular);
+      if constexpr (MODE == MODE_FP64) {
+        tcur = doubling<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
+                            Ppp, Ppm, &singular);
+      } else if constexpr (MODE == MODE_MIX_S) {
+        tcur = doubling_lam<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0,
+                                mu0, Ppp, Ppm, &singular, nullptr);
+      } else if (lv.flag[l] != 0.0) {
+        tcur = doubling<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
+                            Ppp, Ppm, &singular);
+      } else {
+        // the record's two source vectors (written later in this step) carry
+        // the FP64 layer sources out of the FP32 region
+        tcur = doubling_lam_wide<Gm>(X.goff, X.tb, tbF, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N,
+                                     solar, F0, mu0, Ppp, Ppm, &singular,
+                                     reinterpret_cast<double*>(rp + 3 * TILE));
+      }
       X.sync();
       op_s2g<Gm>(X.mo(0), rp, t);
       op_s2g<Gm>(X.mo(tcur), rp + TILE, t);
@@ -657,7 +990,7 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
     matvec<Gm, true, 1>(X.m(0), vv, yv, X.lane);
     if (X.lane < NP) X.V(V_IU)[X.lane] = yv[0] + X.V(V_UB)[X.lane];
     __syncwarp();
-    if (X.lane == 0) emit_interface<Gm>(X, C, w, 0, N, solar, F0, mu0, lvTc, lvOmu, lvB, status);
+    if (X.lane == 0) emit_interface<Gm>(X, C, w, 0, N, solar, F0, mu0, lv, status);
   }
   for (int l = 0; l < nL; ++l) {
     const Real* rl = recs + (size_t)l * SLay::REC;
@@ -692,7 +1025,7 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
       singular |= op_gj<Gm>(X.mo(3), kNoMat, X.vo(V_RHS), X.mo(4), X.gjo(), X.redo(), t, X.bar);
       X.sync();
       xsol = X.m(4);
-      xstride = LD;
+      xstride = Gm::LD;
     }
     if (X.warp == 0) {
       if (X.lane < NP) X.V(V_X)[X.lane] = xsol[X.lane * xstride];
@@ -707,7 +1040,7 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
       }
       __syncwarp();
       if (X.lane == 0)
-        emit_interface<Gm>(X, C, w, l + 1, N, solar, F0, mu0, lvTc, lvOmu, lvB, status);
+        emit_interface<Gm>(X, C, w, l + 1, N, solar, F0, mu0, lv, status);
     }
   }
   if (singular && t == 0) atomicOr(status, 1u);
@@ -715,19 +1048,25 @@ __device__ __noinline__ void solve_one(unsigned goff, int t_, int bar, int w, ch
 }
 
 // ------------------------------------------------------------- persistent kernel
-template <int NP, typename Real>
+template <int NP, int KIND>
 __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col0) {
-  using Gm = Geo<NP, Real>;
-  constexpr int G = Gm::G;
+  using GD = Geo<NP, double>;
+  using GF = Geo<NP, float>;
+  using GL = GroupLayout<NP, KIND>;
+  constexpr int G = GD::G;
   const int gib = threadIdx.x / G;
   const int t = threadIdx.x % G;
-  const unsigned goff = (unsigned)(gib * SmemLayout<Gm>::bytes);
+  const int bar = 1 + gib;
+  const unsigned goff = (unsigned)(gib * GL::bytes);
+  const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
   const int slot = blockIdx.x * (blockDim.x / G) + gib;
   char* sl = P.scratch + (size_t)slot * P.slot_bytes;
-  const Ctx<Gm> X(goff, t, 1 + gib);
-  for (int i = t; i < 6 * Gm::DIM + 4; i += G) X.gjbuf[i] = Real(0);
-  if (P.ncols <= 1 && t == 0) *X.col = col0;
-  long long* task_s = sp<long long>(goff + SmemLayout<Gm>::misc + 48);
+  for (unsigned i = (unsigned)t * 4u; i < (unsigned)GL::bytes; i += (unsigned)G * 4u)
+    *sp<unsigned>(goff + i) = 0u;
+  gsync<G>(bar);
+  ColumnDev* colp = sp<ColumnDev>(goff + CommonLayout<NP>::col);
+  if (P.ncols <= 1 && t == 0) *colp = col0;
+  long long* task_s = sp<long long>(goff + CommonLayout<NP>::misc + 32);
   int cur_col = -1;
   for (;;) {
     long long task;
@@ -736,9 +1075,9 @@ __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col
       if (t == 0) v = atomicAdd(P.counter, 1ull);
       task = (long long)__shfl_sync(0xffffffffu, v, 0);
     } else {
-      gsync<G>(1 + gib);
+      gsync<G>(bar);
       if (t == 0) *task_s = (long long)atomicAdd(P.counter, 1ull);
-      gsync<G>(1 + gib);
+      gsync<G>(bar);
       task = *task_s;
     }
     if (task >= P.ntasks) break;
@@ -750,14 +1089,23 @@ __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col
         if (P.cols[mid].task_begin <= task) lo = mid; else hi = mid - 1;
       }
       if (lo != cur_col) {
-        gsync<G>(1 + gib);
-        if (t == 0) *X.col = P.cols[lo];
+        gsync<G>(bar);
+        if (t == 0) *colp = P.cols[lo];
         cur_col = lo;
       }
       w = (int)(task - P.cols[lo].task_begin);
     }
-    gsync<G>(1 + gib);
-    solve_one<Gm>(goff, t, 1 + gib, w, sl, P.max_layers, P.status);
+    gsync<G>(bar);
+    const int any =
+        wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, KIND == KIND_MIXED);
+    if constexpr (KIND == KIND_FP64) {
+      wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+    } else if (!any) {
+      wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+    } else {
+      wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,
+                               P.max_layers, P.status);
+    }
   }
 }
 

@@ -75,37 +75,57 @@ struct Geo {
   static constexpr int LD = DIM + PAD;
   static constexpr int MAT = DIM * LD;                // Reals per smem matrix
   static constexpr int NW = G / 32;                   // warps per group
-  static constexpr int NMAT = 6;                      // smem matrix buffers per group
   // matvec lanes: warp 0 only; LPR lanes per row
   static constexpr int LPR = (32 / NP < NP) ? (32 / NP) : NP;
   static constexpr int KCH = NP / LPR;
   static_assert(NP % TR == 0 && NP % TC == 0, "tiles must divide the padded order");
 };
 
-// Shared-memory layout of one group (byte offsets).
-template <class Gm>
-struct SmemLayout {
-  using Real = typename Gm::Real;
-  static constexpr int NP = Gm::NP;
-  static constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-  static constexpr size_t mats = 0;  // NMAT x MAT Real
-  static constexpr size_t gj = align16(mats + Gm::NMAT * sizeof(Real) * Gm::MAT);
-  static constexpr size_t vecs = align16(gj + sizeof(Real) * (6 * Gm::DIM + 4));
-  static constexpr int NVEC = 20;  // Real vectors of NP
-  static constexpr size_t dvecs = align16(vecs + sizeof(Real) * NVEC * NP);
-  static constexpr int NDVEC = 6;  // double vectors of NP
-  static constexpr size_t col = align16(dvecs + sizeof(double) * NDVEC * NP);
-  static constexpr size_t misc = align16(col + sizeof(ColumnDev));
-  static constexpr size_t bytes = align16(misc + 64);
+constexpr size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Shared memory of one thread group = a precision-independent prefix
+// (CommonLayout: the column descriptor, scalars and FP64 vectors) followed by
+// one or two typed regions (TypedLayout: Real vectors, the Gauss-Jordan
+// buffers, then NMAT matrices).  Because the prefix is shared, an FP32 and an
+// FP64 view of the same group see the same column, quadrature and scalars,
+// which lets an FP64-adding wavenumber run FP32 doublings in a second typed
+// region placed over its own matrices.
+template <int NP>
+struct CommonLayout {
+  static constexpr size_t col = 0;
+  static constexpr size_t misc = align16(sizeof(ColumnDev));
+  // misc: [0,32) reduction words, [32,40) task index, [48,112) eight FP64
+  //       per-wavenumber scalars (MiscSlot)
+  static constexpr size_t dvecs = misc + 128;
+  static constexpr int NDVEC = 8;  // double vectors of NP (DVecSlot)
+  static constexpr size_t bytes = align16(dvecs + sizeof(double) * NDVEC * NP);
 };
 
-// Vector slots (Real) inside SmemLayout::vecs.
+template <class Gm, int NMAT>
+struct TypedLayout {
+  using Real = typename Gm::Real;
+  static constexpr int NVEC = 20;  // Real vectors of NP (VecSlot)
+  static constexpr size_t vecs = 0;
+  static constexpr size_t gj = align16(vecs + sizeof(Real) * NVEC * Gm::NP);
+  static constexpr size_t mats = align16(gj + sizeof(Real) * (6 * Gm::DIM + 4));
+  static constexpr size_t bytes = align16(mats + (size_t)NMAT * sizeof(Real) * Gm::MAT);
+};
+
+// Matrix buffers of the reference-order (T-form) doubling and the adding,
+// and of the FP32 Lambda-split doubling.
+constexpr int kMatsTForm = 6;
+constexpr int kMatsLam = 9;
+
+// Vector slots (Real) inside TypedLayout::vecs.
 enum VecSlot {
   V_Y0 = 0, V_Y1, V_Z0, V_Z1, V_SU0, V_SU1, V_SD0, V_SD1,
   V_RU, V_RD, V_UB, V_SDN, V_SUP, V_ID, V_IU, V_RHS, V_TMP, V_T, V_X
 };
-// Double vector slots inside SmemLayout::dvecs: quadrature and solar phase.
-enum DVecSlot { D_MU = 0, D_WT, D_CW, D_HW, D_PP, D_PM };
+// Double vector slots inside CommonLayout::dvecs: quadrature, solar phase and
+// the direct-transmission diagonal of the Lambda-split doubling (ping-pong).
+enum DVecSlot { D_MU = 0, D_WT, D_CW, D_HW, D_PP, D_PM, D_LAM0, D_LAM1 };
+// FP64 per-wavenumber scalars inside CommonLayout::misc (+48).
+enum MiscSlot { S_BS = 0, S_BTOP };
 
 // ============================================================== sync / reductions
 template <int G>
@@ -345,6 +365,84 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
   if (out_cm) tl.store_cm(acc, out_cm);
 }
 
+// Products of the Lambda-split doubling (FP32, register tiles).  lam is the
+// FP64 diagonal Lambda (smem byte offset of NP doubles); Z a row-major matrix.
+//   kLamR2:  acc = X Y;  out_rm = I - acc;  out2_rm = Lambda acc + Z
+//   kLamAdd: v = X Y + Lambda Z;  out_rm / out_cm = v;
+//            out2_rm (optional) = v + Lambda^2 on the diagonal
+// Every term is a sum of non-negative products for a non-negative phase
+// function, so each entry keeps FP32 relative accuracy.
+constexpr int kLamR2 = 0, kLamAdd = 1;
+
+template <class Gm>
+__device__ __noinline__ void op_gemm_lam(unsigned xt_off, unsigned y_off, unsigned z_off,
+                                         unsigned lam_off, int mode, unsigned orm_off,
+                                         unsigned ocm_off, unsigned o2_off, int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
+  const Real* __restrict__ XT = sp<Real>(xt_off);
+  const Real* __restrict__ Y = sp<Real>(y_off);
+  const Real* Z = sp<Real>(z_off);
+  const double* lam = sp<double>(lam_off);
+  Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+  Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
+  Real* out2 = (o2_off == kNoMat) ? nullptr : sp<Real>(o2_off);
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real acc[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) acc[a][b] = Real(0);
+  const Real* xp = XT + tl.rb * TR;
+  const Real* yp = Y + tl.cb * TC;
+#pragma unroll 8
+  for (int k = 0; k < NP; ++k) {
+    Real xa[TR], yb[TC];
+    lds_vec<Real, TR>(xa, xp + k * LD);
+    lds_vec<Real, TC>(yb, yp + k * LD);
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+  }
+  Real zt[TR][TC];
+  tl.load_rm(zt, Z);
+  Real lr[TR];
+#pragma unroll
+  for (int a = 0; a < TR; ++a) lr[a] = static_cast<Real>(lam[tl.row(a)]);
+  if (mode == kLamR2) {
+    Real o1[TR][TC], o2[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) {
+        o1[a][b] = ((tl.row(a) == tl.col(b)) ? Real(1) : Real(0)) - acc[a][b];
+        o2[a][b] = fma(lr[a], acc[a][b], zt[a][b]);
+      }
+    tl.store_rm(o1, out_rm);
+    tl.store_rm(o2, out2);
+  } else {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) acc[a][b] = fma(lr[a], zt[a][b], acc[a][b]);
+    if (out_rm) tl.store_rm(acc, out_rm);
+    if (out_cm) tl.store_cm(acc, out_cm);
+    if (out2) {
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b)
+          if (tl.row(a) == tl.col(b)) {
+            const double l = lam[tl.row(a)];
+            acc[a][b] = acc[a][b] + static_cast<Real>(l * l);
+          }
+      tl.store_rm(acc, out2);
+    }
+  }
+}
+
 // X = B A^{-1} by Gauss-Jordan column elimination, with column pivoting on
 // the largest |entry| of the pivot row -- the pivot rule of the LU with
 // partial pivoting of A^T that the reference's right-solve performs
@@ -554,9 +652,10 @@ __device__ __forceinline__ void matvec(const typename Gm::Real* S,
 // narrow bands, small-v polynomial / large-v exponential series otherwise.
 // Same algorithm and constants as the reference (src/planck.cpp:13-131) so
 // that the level sources agree to round-off.
-__device__ __forceinline__ double planck_kernel_v(double v) { return v * v * v / (exp(v) - 1.0); }
+__host__ __device__ __forceinline__ double planck_kernel_v(double v) { return v * v * v / (exp(v) - 1.0); }
 
-__device__ inline double planck_band(double wnumlo, double wnumhi, double temp) {
+// Host and device: the host copy serves adrt_planck_band().
+__host__ __device__ inline double planck_band(double wnumlo, double wnumhi, double temp) {
   const double C2 = 1.438786, SIGMA = 5.67032E-8, VCUT = 1.5;
   const double A1 = 1.0 / 3.0, A2 = -1.0 / 8.0, A3 = 1.0 / 60.0, A4 = -1.0 / 5040.0;
   const double A5 = 1.0 / 272160.0, A6 = -1.0 / 13305600.0;

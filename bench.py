@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--wavenumbers", type=int, default=100_000)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-check", action="store_true")
+    p.add_argument("--only", default=None, choices=["fp64", "mixed"],
+                   help="time one precision form only (profiling runs)")
     return p.parse_args()
 
 
@@ -190,7 +192,7 @@ def main():
 
     eng = Engine(device=local)
     results = {}
-    precisions = ["fp64", "mixed"]
+    precisions = [args.only] if args.only else ["fp64", "mixed"]
     for pname in precisions:
         prec = _abi.PRECISION_FP64 if pname == "fp64" else _abi.PRECISION_MIXED
         # weak scaling: every rank solves its own batch of the full size
@@ -227,9 +229,10 @@ def main():
     if rank == 0 and not args.no_check:
         from oracle import oracle
         idx = np.arange(0, args.wavenumbers, max(1, args.wavenumbers // 200))
-        ref = oracle.solve_oracle(results["fp64"]["batch"].subset(idx), os.cpu_count() or 1,
+        b0 = results[precisions[0]]["batch"]
+        ref = oracle.solve_oracle(b0.subset(idx), os.cpu_count() or 1,
                                   which=_abi.INTERFACE_OUTPUTS)
-        L = results["fp64"]["batch"].L
+        L = b0.L
         for pname in precisions:
             out = {k: v.view(-1, L + 1)[torch.as_tensor(idx, device="cuda")].cpu().numpy().ravel()
                    for k, v in results[pname]["out"].items()}
@@ -239,7 +242,9 @@ def main():
 
     # e2e through the host entry point (pinned host buffers, copies timed)
     pname = args.precision
-    if pname == "auto":
+    if args.only:
+        pname = args.only
+    elif pname == "auto":
         pname = "mixed" if acc and max(v["normalized"] for v in acc["mixed"].values()) <= 1e-6 else "fp64"
     b = results[pname]["batch"]
     hb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc))
@@ -287,9 +292,10 @@ def main():
                        "wavenumbers_per_gpu": args.wavenumbers,
                        "l2": "inputs 190 MB > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world} (wavenumber shards)"},
-            "fp64_solves_per_s": args.wavenumbers * world / (results["fp64"]["ms"] * 1e-3),
-            "mixed_solves_per_s": args.wavenumbers * world / (results["mixed"]["ms"] * 1e-3),
-            "mixed_over_fp64": results["fp64"]["ms"] / results["mixed"]["ms"],
+            **{f"{p}_solves_per_s": args.wavenumbers * world / (results[p]["ms"] * 1e-3)
+               for p in precisions},
+            "mixed_over_fp64": (results["fp64"]["ms"] / results["mixed"]["ms"]
+                                if len(precisions) == 2 else None),
             "accuracy_vs_oracle": acc,
             "roofline": roof,
             "e2e": {"value": args.wavenumbers * world / e2e_s, "unit": "wavenumber-solves/s",

@@ -167,6 +167,44 @@ int adrt_solve_batch(adrt_engine* engine, const adrt_batch_desc* desc,
 int adrt_solve_batch_host(adrt_engine* engine, const adrt_batch_desc* desc,
                           const adrt_inputs* host_in, const adrt_outputs* host_out);
 
+/* FP32 device arrays, the element type of the reference's DeviceData
+ * (src_cuda/cuda_solver.cuh:45-68).  Same fields and layouts as adrt_inputs /
+ * adrt_outputs. */
+typedef struct adrt_inputs_f32 {
+  const float* delta_tau;
+  const float* single_scat_albedo;
+  const float* phase_moments;
+  const float* temperature;
+  const float* planck_levels;
+  const float* surface_albedo;
+  const float* solar_mu;
+  const float* wavenumber_low;
+  const float* wavenumber_high;
+  const float* surface_emission;
+  const float* top_emission;
+} adrt_inputs_f32;
+
+typedef struct adrt_outputs_f32 {
+  float* flux_up;
+  float* flux_down;
+  float* flux_direct;
+  float* mean_intensity;
+  float* flux_divergence;
+  float* toa_flux_up;
+  float* toa_flux_down;
+  float* boa_flux_direct;
+} adrt_outputs_f32;
+
+/* Batched solve from FP32 device arrays, stream ordered: replaces
+ * adrt::cuda::solveBatch(const BatchConfig&, const DeviceData&, cudaStream_t)
+ * (src_cuda/cuda_solver.cuh:77-80) for callers holding FP32 data.  The inputs
+ * are widened into an engine-owned FP64 staging buffer on the stream, solved,
+ * and the requested outputs narrowed back.  Allocates only when the staging
+ * buffer must grow (never during stream capture: size it with one call first). */
+int adrt_solve_batch_f32(adrt_engine* engine, const adrt_batch_desc* desc,
+                         const adrt_inputs_f32* in, const adrt_outputs_f32* out,
+                         void* cuda_stream);
+
 /* Validate a batch description and (host) inputs with the rules of
  * ADConfig::validate() (src/adding_doubling.hpp:123-174) applied to every
  * wavenumber.  Returns ADRT_ERR_INVALID_ARGUMENT with a detail message. */
@@ -195,6 +233,16 @@ int adrt_solve_batch_uneven(adrt_engine* engine, const adrt_column_desc* cols, i
  * eliminations run on the CUDA-core FMA pipes.  Engine utility; the reference
  * has no counterpart. */
 int adrt_probe_fma_tflops(double* fp64_tflops, double* fp32_tflops);
+
+/* Gauss-Legendre nodes and weights on [0,1], the engine's own quadrature
+ * (replaces adrt::gaussLegendre, src/quadrature.cpp:11-51). */
+int adrt_gauss_legendre(int n, double* nodes, double* weights);
+
+/* Band-integrated Planck function on the host, the algorithm the engine runs
+ * on the device (replaces adrt::planckFunction, src/planck.cpp:35-131).
+ * ADRT_ERR_INVALID_ARGUMENT where the reference throws. */
+int adrt_planck_band(double wavenumber_low, double wavenumber_high, double temperature,
+                     double* out);
 
 /* --------------------------------------------------------------- errors */
 const char* adrt_last_status_detail(void);

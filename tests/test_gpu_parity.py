@@ -232,7 +232,7 @@ def test_invalid_arguments_raise(eng):
 
 def test_bad_values_set_the_device_status_flag(eng):
     b = workloads.config1(W=4)
-    b.arrays["delta_tau"][5] = -1.0  # the device path reports instead of throwing
+    b.arrays["delta_tau"].reshape(-1)[5] = -1.0  # the device path reports instead of throwing
     run_device(eng, b)
     assert eng.read_status() & _abi.ADRT_FLAG_BAD_INPUT
     assert eng.read_status() == 0  # read clears
