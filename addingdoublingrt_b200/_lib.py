@@ -29,6 +29,10 @@ EXPORTS = (
     "adrt_last_status_detail",
     "adrt_version",
     "adrt_probe_fma_tflops",
+    "adrt_solve_batch_f32",
+    "adrt_gauss_legendre",
+    "adrt_planck_band",
+    "adrt_solve_batch_noalloc",
 )
 
 
@@ -64,6 +68,12 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         lib.adrt_last_status_detail.restype = C.c_char_p
         lib.adrt_version.restype = C.c_char_p
         lib.adrt_probe_fma_tflops.argtypes = [P(C.c_double), P(C.c_double)]
+        lib.adrt_gauss_legendre.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        lib.adrt_planck_band.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double)]
+        lib.adrt_solve_batch_f32.argtypes = [C.c_void_p, P(_abi.BatchDesc), C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+        lib.adrt_solve_batch_noalloc.argtypes = [P(_abi.BatchDesc), P(_abi.Inputs),
+                                                 P(_abi.Outputs), C.c_void_p]
         _lib = lib
         return lib
 

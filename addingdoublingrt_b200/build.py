@@ -20,7 +20,7 @@ LIB = os.path.join(PKG, "libadrt_b200.so")
 HOST_LIB = os.path.join(PKG, "libadrt_host.so")
 HOST_SOURCES = ["adrt_host.cpp"]
 
-SOURCES = ["adrt_engine.cu", "adrt_probe.cu"]
+SOURCES = ["adrt_engine.cu", "adrt_probe.cu", "adrt_noalloc.cu"]
 HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh"]
 
 NVCC_FLAGS = [

@@ -34,6 +34,16 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+}  // namespace
+
+// Lets other translation units of the library report through
+// adrt_last_status_detail() (not exported).
+__attribute__((visibility("hidden"))) void adrt_internal_set_detail(const char* msg) {
+  g_detail = msg;
+}
+
+namespace {
+
 #define CUDA_TRY(expr)                                                             \
   do {                                                                             \
     cudaError_t e_ = (expr);                                                       \

@@ -210,6 +210,23 @@ int adrt_solve_batch_f32(adrt_engine* engine, const adrt_batch_desc* desc,
  * wavenumber.  Returns ADRT_ERR_INVALID_ARGUMENT with a detail message. */
 int adrt_validate_batch(const adrt_batch_desc* desc, const adrt_inputs* host_in);
 
+/* Batched solve that allocates no device memory (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc -- inside a framework
+ * whose caching allocator already holds the GPU's memory, on a latency-bound
+ * path where an allocation's implicit synchronisation is not acceptable, or
+ * in a plugin host that only hands over its own buffers.  Same arguments and
+ * results as adrt_solve_batch, without an engine: the work memory is one
+ * fixed 64 MiB array compiled into the library (present on every GPU that
+ * loads it, until the process exits).  The first call on a device looks up
+ * that array's device address; make it before any stream capture.  A batch
+ * whose per-wavenumber work memory (about (L+1) x 25 KB at N=32 in FP64)
+ * does not fit is rejected with ADRT_ERR_WORKSPACE.  All calls share the
+ * array and it keeps the last call's contents; each call resets what must
+ * start at zero, so calls that overlap on the GPU race and must not be
+ * issued.  The device status word is not reported by this entry point. */
+int adrt_solve_batch_noalloc(const adrt_batch_desc* desc, const adrt_inputs* in,
+                             const adrt_outputs* out, void* cuda_stream);
+
 /* ------------------------------------------------------- uneven batches */
 
 /* One column of an uneven batch (reference: several solveBatch calls).
