@@ -969,6 +969,9 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
       op_gemm<Gm>(X.mo(1), X.mo(5), kNoMat, 0, kNoMat, oSp, t);  // D1 R_b (cm)
       X.sync();
       op_gemm<Gm>(oSp, oTl, X.mo(0), 0, X.mo(4), kNoMat, t);  // R + (D1 R_b) T
+      // the tensor-core product writes in fragment order, the copy reads in
+      // tile order: other threads' elements must be complete
+      X.sync();
       op_s2g<Gm>(X.mo(4), rp + 2 * TILE, t);
     }
     if (X.warp == 0) {

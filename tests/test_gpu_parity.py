@@ -144,6 +144,20 @@ def test_fp64_engine_on_workload_samples(eng, name, make):
     assert_fp64_parity(b, run_device(eng, b), ref, sens, name)
 
 
+def test_many_wavenumbers_per_group_n32_is_deterministic_and_matches(eng):
+    """600 wavenumbers at N = 32 (four warps per wavenumber): thread groups
+    solve several wavenumbers each, so every cross-warp hand-off of the solve
+    is exercised; two runs must agree bit for bit and match the oracle."""
+    b = workloads.config3().subset(np.arange(0, 20_000, 33)[:600])
+    r1 = run_device(eng, b, _abi.INTERFACE_OUTPUTS)
+    r2 = run_device(eng, b, _abi.INTERFACE_OUTPUTS)
+    for k in _abi.INTERFACE_OUTPUTS:
+        assert np.array_equal(r1[k], r2[k]), k
+    ref = oracle.solve_oracle(b, os.cpu_count() or 1, which=_abi.INTERFACE_OUTPUTS)
+    sens = oracle.solve_oracle(b, os.cpu_count() or 1, which=_abi.INTERFACE_OUTPUTS, fma=True)
+    assert_fp64_parity(b, r1, ref, sens, "config3-600")
+
+
 def test_full_size_config2_batch_is_consistent(eng):
     """Full 100k x 100 batch: every wavenumber finite, identical wavenumbers give
     identical results, the direct beam is exact, and a sample matches the oracle."""
