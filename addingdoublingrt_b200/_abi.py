@@ -92,6 +92,19 @@ class Outputs(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
 
 
+COTANGENT_FIELDS = ("flux_up", "flux_down", "mean_intensity", "flux_direct")
+GRADIENT_FIELDS = ("delta_tau", "single_scat_albedo", "phase_moments", "temperature",
+                   "planck_levels")
+
+
+class Cotangents(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in COTANGENT_FIELDS]
+
+
+class Gradients(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in GRADIENT_FIELDS]
+
+
 class ColumnDesc(C.Structure):
     _fields_ = [("desc", BatchDesc), ("inp", Inputs), ("out", Outputs)]
 

@@ -33,6 +33,7 @@ EXPORTS = (
     "adrt_gauss_legendre",
     "adrt_planck_band",
     "adrt_solve_batch_noalloc",
+    "adrt_adjoint",
 )
 
 
@@ -74,6 +75,9 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                              C.c_void_p, C.c_void_p]
         lib.adrt_solve_batch_noalloc.argtypes = [P(_abi.BatchDesc), P(_abi.Inputs),
                                                  P(_abi.Outputs), C.c_void_p]
+        lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),
+                                     C.c_void_p, P(_abi.Cotangents), P(_abi.Gradients),
+                                     C.c_void_p]
         _lib = lib
         return lib
 

@@ -1,0 +1,1095 @@
+// adrt_adjoint.cuh -- hand-written reverse-mode adjoint of the column solve.
+//
+// Gradients of a loss L = sum over interfaces of c_up F_up + c_dn F_dn +
+// c_J J + c_dir F_dir (cotangents supplied per wavenumber and interface) with
+// respect to delta_tau, single_scat_albedo, the phase moments and the level
+// temperatures (or Planck levels), for the reference's discrete scheme at
+// fixed doubling counts nn (src/doubling.hpp:107-109 is piecewise constant).
+// FP64 throughout.  Per wavenumber, one thread group:
+//
+//   1. the forward solve (wav_body), which keeps every layer's R, T, s_up,
+//      s_dn, every composite R_base, U_base and the interface intensities
+//      (the per-layer checkpoints of the adding);
+//   2. the downward-pass adjoint, interface L-1 .. 0.  Every matrix
+//      cotangent it produces is rank one (b_rhs x^T), so it stores only two
+//      vectors per interface;
+//   3. the adding adjoint, layer 0 .. L-1 (reverse of the bottom-up build),
+//      which completes each layer's (dR, dT, ds_up, ds_dn); then that layer's
+//      doubling chain is recomputed with a record of every step (the chain is
+//      not stored across layers) and run backwards, then the phase matrices'
+//      adjoint and the Planck / beam chain rules.
+#pragma once
+
+#include "adrt_kernel.cuh"
+
+namespace adrt_dev {
+
+// dB/dT of the band integral in closed form: 4B/T minus the boundary terms of
+// d/dT of the integration limits v = c2 nu / T (the construction of the
+// reference's planckFunctionDeriv, src/planck.cpp:135-175).
+__host__ __device__ inline double planck_band_deriv(double lo, double hi, double T) {
+  const double C2 = 1.438786, SIGMA = 5.67032E-8;
+  if (T < 0.0 || hi < lo || lo < 0.0) return -1.0;
+  if (T < 1.e-4) return 0.0;
+  if (hi == lo) {
+    const double x = C2 * hi / T, em = exp(-x);
+    const double b = 1.1911e-8 * hi * hi * hi * em / (1.0 - em);
+    return b * (x / T) / (1.0 - em);
+  }
+  const double conc = 15.0 / (kPi * kPi * kPi * kPi);
+  const double v0 = C2 * lo / T, v1 = C2 * hi / T;
+  double f0, f1;
+  if (v0 < 1.e-6) {
+    f0 = v0 * v0;
+  } else {
+    const double em = exp(-v0);
+    f0 = v0 * v0 * v0 * em / (1.0 - em);
+  }
+  if (v1 < 1.e-6) {
+    f1 = v1 * v1;
+  } else {
+    const double em = exp(-v1);
+    f1 = v1 * v1 * v1 * em / (1.0 - em);
+  }
+  const double B = planck_band(lo, hi, T);
+  return 4.0 * B / T - (SIGMA / kPi) * conc * T * T * T * (v1 * f1 - v0 * f0);
+}
+
+// Sum of a double over the group (every thread gets the total).
+template <int G>
+__device__ __forceinline__ double gsum(double v, double* red, int bar) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if constexpr (G == 32) {
+    return v;
+  } else {
+    constexpr int NW = G / 32;
+    const int t = threadIdx.x % G;
+    gsync<G>(bar);
+    if ((t & 31) == 0) red[t >> 5] = v;
+    gsync<G>(bar);
+    double r = 0.0;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) r += red[i];
+    gsync<G>(bar);
+    return r;
+  }
+}
+
+// out (row-major and/or column-major) += sum_p alpha_p u_p v_p^T, with the
+// vectors u_p, v_p in shared memory (Real, NP entries; kNoMat = unused pair).
+template <class Gm>
+__device__ __noinline__ void op_rank(unsigned orm, unsigned ocm, unsigned u0, unsigned v0,
+                                     double a0, unsigned u1, unsigned v1, double a1, unsigned u2,
+                                     unsigned v2, double a2, unsigned u3, unsigned v3, double a3,
+                                     int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  const unsigned us[4] = {u0, u1, u2, u3}, vs[4] = {v0, v1, v2, v3};
+  const double al[4] = {a0, a1, a2, a3};
+  Real d[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) d[a][b] = Real(0);
+#pragma unroll
+  for (int p = 0; p < 4; ++p) {
+    if (us[p] == kNoMat) continue;
+    const Real* u = sp<Real>(us[p]);
+    const Real* v = sp<Real>(vs[p]);
+#pragma unroll
+    for (int a = 0; a < TR; ++a) {
+      const Real ua = static_cast<Real>(al[p]) * u[tl.row(a)];
+#pragma unroll
+      for (int b = 0; b < TC; ++b) d[a][b] = fma(ua, v[tl.col(b)], d[a][b]);
+    }
+  }
+  if (orm != kNoMat) {
+    Real* o = sp<Real>(orm);
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) o[tl.row(a) * LD + tl.col(b)] += d[a][b];
+  }
+  if (ocm != kNoMat) {
+    Real* o = sp<Real>(ocm);
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) o[tl.col(b) * LD + tl.row(a)] += d[a][b];
+  }
+}
+
+// Copy a row-major matrix into row-major and/or column-major buffers, scaled.
+template <class Gm>
+__device__ __noinline__ void op_copy(unsigned in_rm, unsigned orm, unsigned ocm, double scale,
+                                     int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real X[TR][TC];
+  tl.load_rm(X, sp<Real>(in_rm));
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) X[a][b] *= static_cast<Real>(scale);
+  if (orm != kNoMat) tl.store_rm(X, sp<Real>(orm));
+  if (ocm != kNoMat) tl.store_cm(X, sp<Real>(ocm));
+}
+
+// ---------------------------------------------------------------- buffers
+// Matrix buffers of the adjoint's typed region (row-major "r", column-major "c").
+enum AdjMat {
+  J_R = 0, J_Rc, J_Tc, J_TG, J_TGc, J_TGR, J_Ac, J_bR0, J_bR0c, J_bT0, J_bT0c, J_bR1, J_bR1c,
+  J_bT1, J_bT1c, J_bTGR, J_bTGRc, J_bTG, J_W, J_C, J_Cc, J_T1, J_T2, J_VEC,
+  kMatsAdj = J_VEC + 2  // J_VEC spans two buffers (18 vectors even at NP = 8)
+};
+// Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 18 NP).
+enum AdjVec {
+  A_BY = 0, A_BZ, A_BSU, A_BSD, A_H, A_RU, A_RD, A_BRU, A_BRD, A_BH, A_Y, A_Z, A_SU, A_SD,
+  A_BUP, A_BDN, A_T0, A_T1
+};
+
+// Adjoint slot in HBM: the forward slot (levels, phase, records), the
+// interface intensities, the downward-pass vectors, the doubling record and
+// the layout-1 phase-cotangent accumulators.
+template <class Gm>
+struct AdjSlot {
+  using SL = SlotLayout<Gm>;
+  using Tp = TapeLayout<Gm>;
+  static constexpr int NP = Gm::NP;
+  static __host__ __device__ size_t fwd(int lmax) { return (SL::bytes(lmax) + 255) & ~size_t(255); }
+  static __host__ __device__ size_t ivec(int lmax) {
+    return ((size_t)(lmax + 1) * 2 * NP * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t dvec(int lmax) { return ivec(lmax); }
+  static __host__ __device__ size_t tape() {
+    return ((size_t)kMaxDoublings * Tp::STEP * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t pacc() {
+    return ((size_t)2 * NP * NP * sizeof(double) + 2 * NP * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t brb() { return (Tp::TILE * sizeof(double) + 255) & ~size_t(255); }
+  static __host__ __device__ size_t acc(int lmax) {
+    return ((size_t)4 * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t bytes(int lmax) {
+    return fwd(lmax) + ivec(lmax) + dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256;
+  }
+};
+
+template <int NP>
+struct AdjGroup {
+  using GD = Geo<NP, double>;
+  static constexpr size_t bytes =
+      align16(CommonLayout<NP>::bytes + TypedLayout<GD, kMatsAdj>::bytes);
+};
+
+// Cotangent / gradient pointers of one batch (device).
+struct AdjDev {
+  const double *c_fu, *c_fd, *c_J, *c_fdir;  // [W*(L+1)] each, or null
+  double *g_tau, *g_ssa, *g_mom, *g_temp, *g_planck;
+};
+
+// ---------------------------------------------------------------- doubling adjoint
+// Reverse of doubling<Gm> for one layer.  On entry the layer cotangents are
+// in (J_bR0, J_bR0c), (J_bT0, J_bT0c) and vectors A_BUP / A_BDN; the phase
+// matrices in Ppp / Ppm and the solar phase vectors in D_PP / D_PM.  Writes
+// the phase-matrix cotangents to J_T1 (P++) and J_T2 (P+-), the solar phase
+// vector cotangents to A_T0 (p+) / A_T1 (p-), and returns the scalar
+// cotangents through out[0..4] = d tau, d omega, d B_top, d B_bot, d F_top.
+template <class Gm>
+__device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_, int bar,
+                                              double tau, double om, double Bt, double Bb,
+                                              double tcum, int N, bool solar, double F0,
+                                              double mu0, const double* Ppp, const double* Ppm,
+                                              double* tape, double* out, int* singular) {
+  using Real = typename Gm::Real;
+  static_assert(sizeof(Real) == 8, "the adjoint runs in FP64");
+  using Tp = TapeLayout<Gm>;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, G = Gm::G;
+  const int t = X.t;
+  double* red = reinterpret_cast<double*>(X.gjbuf) + 4;  // 4 doubles of reduction scratch
+  // 1. forward chain of this layer again, recorded (uses buffers 0..5 and V_*)
+  const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
+  const int tcur =
+      doubling<Gm>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
+                   singular, tape);
+  (void)tcur;
+  X.sync();
+  const double* mu = X.DV(D_MU);
+  const double* wt = X.DV(D_WT);
+  const double omc = om > 1.0 ? 1.0 : om;
+  const double con = 2.0 * omc * kPi;
+  const double tau0 = ldexp(tau, -nn);
+  const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
+  Real* vb = X.m(J_VEC);
+  auto VA = [&](int s) { return vb + s * NP; };
+  auto vo = [&](int s) { return X.mo(J_VEC) + (unsigned)(s * NP * sizeof(Real)); };
+  // 2. sources: up = y Bbar + z Bd + su, dn = y Bbar - z Bd + sd
+  const double Bbar = 0.5 * (Bb + Bt), Bd = (Bb - Bt) / tau;
+  const double* yF = nullptr;
+  (void)yF;
+  double pBbar = 0.0, pBd = 0.0;
+  {
+    // final y, z of the chain are the inputs of "step nn": rebuild them from the
+    // last record step (recompute one vector update is avoided by reading the
+    // forward's final vectors still in V_Y/V_Z of the FP64 view)
+    const int par = nn & 1;
+    if (X.warp == 0 && X.lane < NP) {
+      const int i = X.lane;
+      const double bu = VA(A_BUP)[i], bd = VA(A_BDN)[i];
+      const double y = X.V(V_Y0 + par)[i], z = X.V(V_Z0 + par)[i];
+      VA(A_BY)[i] = (bu + bd) * Bbar;
+      VA(A_BZ)[i] = (bu - bd) * Bd;
+      VA(A_BSU)[i] = bu;
+      VA(A_BSD)[i] = bd;
+      pBbar = (bu + bd) * y;
+      pBd = (bu - bd) * z;
+    }
+  }
+  pBbar = gsum<G>(pBbar, red, bar);
+  pBd = gsum<G>(pBd, red, bar);
+  double d_tau = -pBd * Bd / tau;
+  const double d_Bb = 0.5 * pBbar + pBd / tau, d_Bt = 0.5 * pBbar - pBd / tau;
+  double bg = 0.0, bgam = 0.0;
+  int cs = 0;  // which cotangent set holds the current dR, dT
+  for (int k = nn - 1; k >= 0; --k) {
+    const double* tk = tape + (size_t)k * Tp::STEP;
+    const double g = ldexp(tau0, k - 1);
+    const double gam = tk[3 * Tp::TILE + 4 * NP];
+    const unsigned bRr = X.mo(cs ? J_bR1 : J_bR0), bRc = X.mo(cs ? J_bR1c : J_bR0c);
+    const unsigned bTr = X.mo(cs ? J_bT1 : J_bT0), bTc = X.mo(cs ? J_bT1c : J_bT0c);
+    const unsigned nRr = X.mo(cs ? J_bR0 : J_bR1), nRc = X.mo(cs ? J_bR0c : J_bR1c);
+    const unsigned nTr = X.mo(cs ? J_bT0 : J_bT1), nTc = X.mo(cs ? J_bT0c : J_bT1c);
+    X.sync();
+    op_g2s<Gm>(tk, X.mo(J_R), X.mo(J_Rc), t);
+    op_g2s<Gm>(tk + Tp::TILE, kNoMat, X.mo(J_Tc), t);
+    op_g2s<Gm>(tk + 2 * Tp::TILE, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
+    if (X.warp == 0 && X.lane < NP) {
+      const int i = X.lane;
+      VA(A_Y)[i] = tk[3 * Tp::TILE + i];
+      VA(A_Z)[i] = tk[3 * Tp::TILE + NP + i];
+      VA(A_SU)[i] = tk[3 * Tp::TILE + 2 * NP + i];
+      VA(A_SD)[i] = tk[3 * Tp::TILE + 3 * NP + i];
+    }
+    X.sync();
+    op_gemm<Gm>(X.mo(J_Rc), X.mo(J_R), kNoMat, 1, kNoMat, X.mo(J_Ac), t);  // A = I - R R (cm)
+    op_gemm<Gm>(X.mo(J_TGc), X.mo(J_R), kNoMat, 0, X.mo(J_TGR), kNoMat, t);  // TGR = TG R
+    if (X.warp == 0) {  // h = z + g y, ru = R sd + gam su, rd = gam R su + sd
+      const Real* vv[2] = {VA(A_SD), VA(A_SU)};
+      Real yv[2];
+      matvec<Gm, true, 2>(X.m(J_Rc), vv, yv, X.lane);
+      if (X.lane < NP) {
+        const int i = X.lane;
+        VA(A_H)[i] = VA(A_Z)[i] + g * VA(A_Y)[i];
+        VA(A_RU)[i] = yv[0] + gam * VA(A_SU)[i];
+        VA(A_RD)[i] = gam * yv[1] + VA(A_SD)[i];
+      }
+    }
+    // dTGR = dR T^T - bz h^T + by y^T
+    op_gemm<Gm>(bRc, X.mo(J_Tc), kNoMat, 0, X.mo(J_bTGR), X.mo(J_bTGRc), t);
+    // dTG (partial) = dT T^T
+    op_gemm<Gm>(bTc, X.mo(J_Tc), kNoMat, 0, X.mo(J_T1), kNoMat, t);
+    X.sync();
+    op_rank<Gm>(X.mo(J_bTGR), X.mo(J_bTGRc), vo(A_BZ), vo(A_H), -1.0, vo(A_BY), vo(A_Y), 1.0,
+                kNoMat, kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+    X.sync();
+    // dTG = dT T^T + dTGR R^T + bz h^T + by y^T + bsu ru^T + bsd rd^T
+    op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Rc), X.mo(J_T1), 0, X.mo(J_bTG), kNoMat, t);
+    X.sync();
+    op_rank<Gm>(X.mo(J_bTG), kNoMat, vo(A_BZ), vo(A_H), 1.0, vo(A_BY), vo(A_Y), 1.0, vo(A_BSU),
+                vo(A_RU), 1.0, vo(A_BSD), vo(A_RD), 1.0, t);
+    X.sync();
+    // W = dTG A^{-T}   (Gauss-Jordan on A^T = the column-major buffer of A)
+    *singular |= op_gj<Gm>(X.mo(J_Ac), X.mo(J_bTG), kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
+                           X.mo(J_W));
+    X.sync();
+    // C = TG^T W  (= -dA);  dT' = TG^T dT + W + TGR^T dR
+    op_gemm<Gm>(X.mo(J_TG), X.mo(J_W), kNoMat, 0, X.mo(J_C), X.mo(J_Cc), t);
+    op_gemm<Gm>(X.mo(J_TG), bTr, X.mo(J_W), 0, X.mo(J_T1), kNoMat, t);
+    if (X.warp == 0) {  // vector cotangents of this step
+      const Real* v1[2] = {VA(A_BSU), VA(A_BSD)};
+      Real tgs[2];
+      matvec<Gm, true, 2>(X.m(J_TG), v1, tgs, X.lane);  // TG^T bsu, TG^T bsd
+      const Real* v2[2] = {VA(A_BZ), VA(A_BY)};
+      Real tgz[2], trz[2];
+      matvec<Gm, true, 2>(X.m(J_TG), v2, tgz, X.lane);   // TG^T bz, TG^T by
+      matvec<Gm, true, 2>(X.m(J_TGR), v2, trz, X.lane);  // TGR^T bz, TGR^T by
+      if (X.lane < NP) {
+        VA(A_BRU)[X.lane] = tgs[0];
+        VA(A_BRD)[X.lane] = tgs[1];
+        VA(A_BH)[X.lane] = tgz[0] - trz[0];
+        VA(A_T0)[X.lane] = tgz[1] + trz[1];  // (TG + TGR)^T by
+      }
+      __syncwarp();
+      const Real* v3[2] = {VA(A_BRD), VA(A_BRU)};
+      Real rt[2];
+      matvec<Gm, true, 2>(X.m(J_R), v3, rt, X.lane);  // R^T brd, R^T bru
+      const Real* v4[1] = {VA(A_SU)};
+      Real rsu[1];
+      matvec<Gm, true, 1>(X.m(J_Rc), v4, rsu, X.lane);  // R su
+      double pg = 0.0, pgam = 0.0;
+      if (X.lane < NP) {
+        const int i = X.lane;
+        const double bz = VA(A_BZ)[i], by = VA(A_BY)[i], bh = VA(A_BH)[i];
+        const double bsu = VA(A_BSU)[i], bsd = VA(A_BSD)[i];
+        const double y = VA(A_Y)[i], su = VA(A_SU)[i], sd = VA(A_SD)[i];
+        const double bru = VA(A_BRU)[i], brd = VA(A_BRD)[i];
+        pg = -y * bz + y * bh;
+        pgam = sd * bsd + su * bru + rsu[0] * brd;
+        VA(A_BZ)[i] = bz + bh;
+        VA(A_BY)[i] = -g * bz + VA(A_T0)[i] + by + g * bh;
+        VA(A_BSU)[i] = bsu + gam * bru + gam * rt[0];
+        VA(A_BSD)[i] = gam * bsd + rt[1] + brd;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        pg += __shfl_xor_sync(0xffffffffu, pg, o);
+        pgam += __shfl_xor_sync(0xffffffffu, pgam, o);
+      }
+      if (X.lane == 0) {
+        red[0] = pg;
+        red[1] = pgam;
+      }
+    }
+    X.sync();
+    op_gemm<Gm>(X.mo(J_TGR), bRr, X.mo(J_T1), 0, nTr, nTc, t);  // dT' = ... + TGR^T dR
+    // dR' = dR + TG^T dTGR + C R^T + R^T C + bru sd^T + gam brd su^T
+    op_gemm<Gm>(X.mo(J_TG), X.mo(J_bTGR), bRr, 0, X.mo(J_T2), kNoMat, t);
+    X.sync();
+    op_gemm<Gm>(X.mo(J_Cc), X.mo(J_Rc), X.mo(J_T2), 0, X.mo(J_T1), kNoMat, t);
+    X.sync();
+    op_gemm<Gm>(X.mo(J_R), X.mo(J_C), X.mo(J_T1), 0, nRr, nRc, t);
+    X.sync();
+    op_rank<Gm>(nRr, nRc, vo(A_BRU), vo(A_SD), 1.0, vo(A_BRD), vo(A_SU), gam, kNoMat, kNoMat, 0.0,
+                kNoMat, kNoMat, 0.0, t);
+    const double pg = red[0], pgam = red[1];
+    bgam = pgam + 2.0 * gam * bgam;
+    bg = pg + 2.0 * bg;
+    cs ^= 1;
+  }
+  X.sync();
+  // 3. first-order start: T0 = I - tau0 Gpp, R0 = tau0 Gpm, y0 = (1-om) tau0/mu,
+  //    su0 / sd0 = om tau0 Ftop p-/p+ / mu, g0 = tau0/2, gam0 = exp(-tau0/mu0)
+  const unsigned bRr = X.mo(cs ? J_bR1 : J_bR0), bTr = X.mo(cs ? J_bT1 : J_bT0);
+  double p_tau0 = 0.0, p_con = 0.0;
+  {
+    const Tile<Gm> tl(t);
+    if (tl.valid()) {
+      const Real* dR = sp<Real>(bRr);
+      const Real* dT = sp<Real>(bTr);
+      Real* dPpp = X.m(J_T1);
+      Real* dPpm = X.m(J_T2);
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          const int r = tl.row(a), c = tl.col(b);
+          double gp = 0.0, gm = 0.0;
+          if (r < N && c < N) {
+            const double dt = dT[r * Gm::LD + c], dr = dR[r * Gm::LD + c];
+            const double fw = wt[c] / mu[r];
+            const double pp = Ppp[r * NP + c], pm = Ppm[r * NP + c];
+            p_tau0 += dt * (con * pp * fw - ((r == c) ? 1.0 / mu[r] : 0.0)) + dr * con * pm * fw;
+            p_con += tau0 * fw * (dt * pp + dr * pm);
+            gp = dt * tau0 * con * fw;
+            gm = dr * tau0 * con * fw;
+          }
+          dPpp[r * Gm::LD + c] = gp;
+          dPpm[r * Gm::LD + c] = gm;
+        }
+    }
+  }
+  double p_om = 0.0, p_ftop = 0.0;
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane;
+    double dpp = 0.0, dpm = 0.0;
+    if (i < N) {
+      const double by = VA(A_BY)[i];
+      p_tau0 += by * (1.0 - omc) / mu[i];
+      p_om -= by * tau0 / mu[i];
+      if (solar) {
+        const double bsu = VA(A_BSU)[i], bsd = VA(A_BSD)[i];
+        const double pm = X.DV(D_PM)[i], pp = X.DV(D_PP)[i];
+        const double bb = bsu * pm + bsd * pp;
+        p_om += bb * tau0 * Ftop / mu[i];
+        p_tau0 += bb * omc * Ftop / mu[i];
+        p_ftop += bb * omc * tau0 / mu[i];
+        const double base = omc * tau0 / mu[i] * Ftop;
+        dpm = bsu * base;
+        dpp = bsd * base;
+      }
+    }
+    VA(A_T0)[i] = dpp;
+    VA(A_T1)[i] = dpm;
+  }
+  p_tau0 = gsum<G>(p_tau0, red, bar);
+  p_con = gsum<G>(p_con, red, bar);
+  p_om = gsum<G>(p_om, red, bar);
+  p_ftop = gsum<G>(p_ftop, red, bar);
+  p_tau0 += 0.5 * bg;
+  if (solar) p_tau0 += bgam * (-exp(-tau0 / mu0) / mu0);
+  p_om += 2.0 * kPi * p_con;
+  d_tau += p_tau0 * ldexp(1.0, -nn);
+  if (t == 0) {
+    out[0] = d_tau;
+    out[1] = (om > 1.0) ? 0.0 : p_om;
+    out[2] = d_Bt;
+    out[3] = d_Bb;
+    out[4] = p_ftop;
+  }
+  X.sync();
+}
+
+// ---------------------------------------------------------------- phase adjoint
+// Cotangents of the phase moments from those of P++ (J_T1), P+- (J_T2) and of
+// the solar phase vectors (A_T0 = p+, A_T1 = p-), through the Hansen column
+// renormalisation (src/phase_matrix.hpp:61-111, 131-181).  Adds into dchi[l]
+// for l < nuse (global, atomically).
+template <class Gm>
+__device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, int bar,
+                                           const double* chi, int nuse, int N, const double* pl,
+                                           bool solar, double mu0, double* dchi) {
+  using Real = typename Gm::Real;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  constexpr int NP = Gm::NP, G = Gm::G, LD = Gm::LD;
+  const int t = X.t;
+  const double* wt = X.DV(D_WT);
+  Real* dPpp = X.m(J_T1);
+  Real* dPpm = X.m(J_T2);
+  Real* Qpp = X.m(J_W);
+  Real* Qpm = X.m(J_C);
+  Real* vb = X.m(J_VEC);
+  Real* sarr = vb + A_BY * NP;   // column sums s_j
+  Real* carr = vb + A_BZ * NP;   // corr_j
+  Real* bsar = vb + A_BSU * NP;  // d s_j
+  Real* qp = vb + A_H * NP;
+  Real* qm = vb + A_RU * NP;
+  // un-normalised Q
+  for (int e = t; e < NP * NP; e += G) {
+    const int r = e / NP, c = e % NP;
+    double spp = 0.0, spm = 0.0;
+    if (r < N && c < N) {
+      double sign = 1.0;
+      for (int l = 0; l < nuse; ++l) {
+        const double term = (2 * l + 1) * chi[l] * pl[l * N + r] * pl[l * N + c];
+        spp += term;
+        spm += sign * term;
+        sign = -sign;
+      }
+    }
+    Qpp[r * LD + c] = spp / (2.0 * kPi);
+    Qpm[r * LD + c] = spm / (2.0 * kPi);
+  }
+  X.sync();
+  if (t < NP) {
+    const int c = t;
+    double s = 0.0, bc = 0.0;
+    for (int i = 0; i < N; ++i) s += (Qpp[i * LD + c] + Qpm[i * LD + c]) * wt[i];
+    const double corr = (s > 0.0) ? 1.0 / (2.0 * kPi * s) : 1.0;
+    for (int i = 0; i < N; ++i) bc += dPpp[i * LD + c] * Qpp[i * LD + c] + dPpm[i * LD + c] * Qpm[i * LD + c];
+    sarr[c] = s;
+    carr[c] = corr;
+    bsar[c] = (s > 0.0) ? -bc * corr / s : 0.0;
+  }
+  X.sync();
+  for (int e = t; e < NP * NP; e += G) {  // dQ = dP corr_j + w_i ds_j (in place)
+    const int r = e / NP, c = e % NP;
+    dPpp[r * LD + c] = dPpp[r * LD + c] * carr[c] + wt[r] * bsar[c];
+    dPpm[r * LD + c] = dPpm[r * LD + c] * carr[c] + wt[r] * bsar[c];
+  }
+  double bqscale = 0.0;
+  if (solar) {
+    // un-normalised solar vectors and their normalisation
+    if (t < NP) {
+      double sp = 0.0, sm = 0.0;
+      if (t < N) {
+        double sign = 1.0, p0 = 1.0, p1 = mu0;
+        for (int l = 0; l < nuse; ++l) {
+          double plm;
+          if (l == 0) {
+            plm = 1.0;
+          } else if (l == 1) {
+            plm = mu0;
+          } else {
+            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) / l;
+            p0 = p1;
+            p1 = plm;
+          }
+          const double term = (2 * l + 1) * chi[l] * pl[l * N + t] * plm;
+          sp += term;
+          sm += sign * term;
+          sign = -sign;
+        }
+      }
+      qp[t] = sp / (2.0 * kPi);
+      qm[t] = sm / (2.0 * kPi);
+    }
+    X.sync();
+    double ss = 0.0, bcs = 0.0;
+    for (int i = 0; i < N; ++i) ss += (qp[i] + qm[i]) * wt[i];
+    const double cs = (ss > 0.0) ? 1.0 / (2.0 * kPi * ss) : 1.0;
+    const Real* dpp = vb + A_T0 * NP;
+    const Real* dpm = vb + A_T1 * NP;
+    for (int i = 0; i < N; ++i) bcs += dpp[i] * qp[i] + dpm[i] * qm[i];
+    bqscale = (ss > 0.0) ? -bcs * cs / ss : 0.0;
+    X.sync();
+    if (t < NP) {  // dq = dp cs + w dss
+      qp[t] = dpp[t] * cs + wt[t] * bqscale;
+      qm[t] = dpm[t] * cs + wt[t] * bqscale;
+    }
+  }
+  X.sync();
+  // dchi_l = (2l+1)/(2 pi) [P_l^T (dQpp + s_l dQpm) P_l + p0_l P_l . (dqp + s_l dqm)]
+  for (int l = t; l < nuse; l += G) {
+    const double sg = (l & 1) ? -1.0 : 1.0;
+    double acc = 0.0;
+    for (int i = 0; i < N; ++i) {
+      double ri = 0.0;
+      for (int j = 0; j < N; ++j)
+        ri += (dPpp[i * LD + j] + sg * dPpm[i * LD + j]) * pl[l * N + j];
+      acc += pl[l * N + i] * ri;
+    }
+    if (solar) {
+      double p0 = 1.0, p1 = mu0, plm = 1.0;
+      for (int m = 0; m <= l; ++m) {
+        if (m == 0) {
+          plm = 1.0;
+        } else if (m == 1) {
+          plm = mu0;
+        } else {
+          plm = ((2 * m - 1) * mu0 * p1 - (m - 1) * p0) / m;
+          p0 = p1;
+          p1 = plm;
+        }
+      }
+      double sv = 0.0;
+      for (int i = 0; i < N; ++i) sv += pl[l * N + i] * (qp[i] + sg * qm[i]);
+      acc += plm * sv;
+    }
+    atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
+  }
+  X.sync();
+}
+
+
+// ---------------------------------------------------------------- one wavenumber
+// Runs after wav_body (FP64, with the interface intensities kept in `iv`).
+template <int NP>
+__device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int bar, int w,
+                                         char* slot, int lmax, unsigned* status, AdjDev AD) {
+  using Gm = Geo<NP, double>;
+  using Real = double;
+  using SLay = SlotLayout<Gm>;
+  using AS = AdjSlot<Gm>;
+  constexpr int TILE = SLay::TILE, REC = SLay::REC, G = Gm::G, TR = Gm::TR, TC = Gm::TC;
+  constexpr int LD = Gm::LD;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  const ColumnDev* C = X.col;
+  const int t = X.t;
+  const int N = C->N, nL = C->L, M = C->M, layout = C->moment_layout, fb = C->from_bottom;
+  const double Aalb = C->albedo_w ? C->albedo_w[w] : C->surface_albedo;
+  const double mu0 = C->mu0_w ? C->mu0_w[w] : C->solar_mu;
+  const double wlo = C->wlo_w ? C->wlo_w[w] : C->wn_lo;
+  const double whi = C->whi_w ? C->whi_w[w] : C->wn_hi;
+  const double F0 = C->solar_flux;
+  const bool solar = (F0 > 0.0 && mu0 > 0.0);
+  const Levels lv(slot, lmax);
+  double* Ppp = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
+  double* Ppm = Ppp + NP * NP;
+  double* recs = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
+  char* p = slot + AS::fwd(lmax);
+  double* iv = reinterpret_cast<double*>(p);                      // [L+1][Id, Iu]
+  double* dv = reinterpret_cast<double*>(p += AS::ivec(lmax));    // [L+1][brhs, u]
+  double* tape = reinterpret_cast<double*>(p += AS::dvec(lmax));
+  double* pacc = reinterpret_cast<double*>(p += AS::tape());      // dPpp, dPpm, dpp, dpm
+  double* brb = reinterpret_cast<double*>(p += AS::pacc());       // carried d R_base (tiles)
+  double* acc = reinterpret_cast<double*>(p += AS::brb());        // bB, btc, dtau, dom
+  double* scal = reinterpret_cast<double*>(p += AS::acc(lmax));   // 32 doubles
+  double* bB = acc;
+  double* btc = acc + (lmax + 1);
+  double* gtau = acc + 2 * (lmax + 1);
+  double* gom = acc + 3 * (lmax + 1);
+  const double Bs = X.sc[S_BS], Btop = X.sc[S_BTOP];
+  const bool has_surface = !C->diffusion && (Aalb > 0.0 || Bs > 0.0);
+  const double* cw = X.DV(D_CW);
+  const double* hw = X.DV(D_HW);
+  const size_t wo = (size_t)w * (nL + 1);
+  auto ui = [&](int l) { return fb ? nL - l : l; };  // user level index
+  auto cot = [&](const double* a, int l) { return a ? a[wo + ui(l)] : 0.0; };
+  Real* vb = X.m(J_VEC);
+  auto VA = [&](int s) { return vb + s * NP; };
+  auto vo = [&](int s) { return X.mo(J_VEC) + (unsigned)(s * NP * sizeof(Real)); };
+  const Tile<Gm> tl(t);
+  int singular = 0;
+
+  for (int l = t; l <= nL; l += G) {
+    bB[l] = 0.0;
+    btc[l] = 0.0;
+    gtau[l] = 0.0;
+    gom[l] = 0.0;
+  }
+  for (int e = t; e < 2 * NP * NP + 2 * NP; e += G) pacc[e] = 0.0;
+  X.sync();
+
+  // ======== 1. downward-pass adjoint (interface L-1 .. 0); bId carried in A_BDN
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane;
+    VA(A_BDN)[i] = (i < N) ? cot(AD.c_fd, nL) * cw[i] + cot(AD.c_J, nL) * hw[i] : 0.0;
+  }
+  for (int l = nL - 1; l >= 0; --l) {
+    const double* rl = recs + (size_t)l * REC;
+    const double* rb = recs + (size_t)(l + 1) * REC;
+    const int scat = rl[3 * TILE + 2 * NP] != 0.0;
+    const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
+    X.sync();
+    op_g2s<Gm>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);  // R_base(l+1)
+    op_g2s<Gm>(rl, X.mo(J_R), X.mo(J_Rc), t);               // R_l
+    op_g2s<Gm>(rl + TILE, X.mo(J_TG), kNoMat, t);           // T_l (rm)
+    X.sync();
+    if (X.warp == 0) {  // bIu(l+1), bx = Rb^T bIu + bId
+      if (X.lane < NP) {
+        const int i = X.lane;
+        VA(A_BUP)[i] = (i < N) ? cot(AD.c_fu, l + 1) * cw[i] + cot(AD.c_J, l + 1) * hw[i] : 0.0;
+      }
+      __syncwarp();
+      const Real* vv[1] = {VA(A_BUP)};
+      Real yv[1];
+      matvec<Gm, true, 1>(X.m(J_TGR), vv, yv, X.lane);  // Rb^T bIu
+      if (X.lane < NP) VA(A_Y)[X.lane] = yv[0] + VA(A_BDN)[X.lane];
+    }
+    X.sync();
+    const Real* brhs = VA(A_Y);
+    int bstride = 1;
+    if (scat && cb) {  // b_rhs = M^{-T} bx with M = I - R Rb, as b_rhs^T = bx^T M^{-1}
+      op_gemm<Gm>(X.mo(J_Rc), X.mo(J_TGR), kNoMat, 1, X.mo(J_T1), kNoMat, t);
+      X.sync();
+      singular |= op_gj<Gm>(X.mo(J_T1), kNoMat, vo(A_Y), X.mo(J_T2), X.gjo(), X.redo(), t, X.bar);
+      X.sync();
+      brhs = X.m(J_T2);
+      bstride = LD;
+    }
+    if (X.warp == 0) {
+      if (X.lane < NP) VA(A_Z)[X.lane] = brhs[X.lane * bstride];
+      __syncwarp();
+      const Real* vv[1] = {VA(A_Z)};
+      Real rt[1], tt[1];
+      matvec<Gm, true, 1>(X.m(J_R), vv, rt, X.lane);   // R^T b_rhs
+      matvec<Gm, true, 1>(X.m(J_TG), vv, tt, X.lane);  // T^T b_rhs
+      if (X.lane < NP) {
+        const int i = X.lane;
+        const double br = VA(A_Z)[i];
+        dv[(size_t)l * 2 * NP + i] = br;
+        dv[(size_t)(l + 1) * 2 * NP + NP + i] = VA(A_BUP)[i] + (scat ? rt[0] : 0.0);
+        VA(A_BDN)[i] = tt[0] + ((i < N) ? cot(AD.c_fd, l) * cw[i] + cot(AD.c_J, l) * hw[i] : 0.0);
+      }
+    }
+  }
+  X.sync();
+  // interface 0: Iu0 = Rb0 Id0 + Ub0, Id0 = Btop
+  op_g2s<Gm>(recs + 2 * TILE, X.mo(J_TGR), kNoMat, t);
+  X.sync();
+  double pBtop = 0.0;
+  if (X.warp == 0) {
+    if (X.lane < NP) {
+      const int i = X.lane;
+      VA(A_BUP)[i] = (i < N) ? cot(AD.c_fu, 0) * cw[i] + cot(AD.c_J, 0) * hw[i] : 0.0;
+      dv[NP + i] = VA(A_BUP)[i];
+    }
+    __syncwarp();
+    const Real* vv[1] = {VA(A_BUP)};
+    Real yv[1];
+    matvec<Gm, true, 1>(X.m(J_TGR), vv, yv, X.lane);
+    if (X.lane < N) pBtop = VA(A_BDN)[X.lane] + yv[0];
+  }
+  pBtop = gsum<G>(pBtop, reinterpret_cast<double*>(X.gjbuf) + 4, bar);
+  // beam outputs: F_dir and the beam term of J depend on the cumulative tau
+  if (solar && t == 0) {
+    for (int l = 1; l <= nL; ++l) {
+      const double e = F0 * mu0 * exp(-lv.tc[l] / mu0);
+      btc[l] += (cot(AD.c_fdir, l) + cot(AD.c_J, l) / (4.0 * kPi * mu0)) * e * (-1.0 / mu0);
+    }
+  }
+
+  // ======== 2. adding adjoint, layer 0 .. L-1, with each layer's own chain
+  // carried: d R_base(l) in brb (tiles), d U_base(l) in A_SU
+  {  // interface 0: d Rb0 = u0 Id0^T, d Ub0 = u0
+    double* tu = VA(A_BUP);
+    if (X.warp == 0 && X.lane < NP) {
+      tu[X.lane] = dv[NP + X.lane];
+      VA(A_SU)[X.lane] = dv[NP + X.lane];
+      VA(A_SD)[X.lane] = iv[X.lane];  // Id0
+    }
+    X.sync();
+    if (tl.valid()) {
+      double* pb = brb + t * Gm::TE;
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) pb[a * TC + b] = tu[tl.row(a)] * VA(A_SD)[tl.col(b)];
+    }
+  }
+  int nuse_l1 = M;
+  for (int l = 0; l < nL; ++l) {
+    const double* rl = recs + (size_t)l * REC;
+    const double* rb = recs + (size_t)(l + 1) * REC;
+    const int scat = rl[3 * TILE + 2 * NP] != 0.0;
+    const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
+    const double tau = lv.tau[l], om = lv.om[l];
+    X.sync();
+    op_g2s<Gm>(rl, X.mo(J_R), X.mo(J_Rc), t);
+    op_g2s<Gm>(rl + TILE, X.mo(J_TG), X.mo(J_Tc), t);
+    op_g2s<Gm>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);
+    op_g2s<Gm>(brb, X.mo(J_bTGR), X.mo(J_bTGRc), t);
+    if (X.warp == 0 && X.lane < NP) {
+      const int i = X.lane;
+      VA(A_Y)[i] = dv[(size_t)l * 2 * NP + i];                           // b_rhs(l)
+      VA(A_Z)[i] = iv[(size_t)l * 2 * NP + i];                           // Id(l)
+      VA(A_H)[i] = (scat && cb) ? iv[(size_t)(l + 1) * 2 * NP + NP + i]  // b_l
+                                : rb[3 * TILE + NP + i];
+      VA(A_RU)[i] = rb[3 * TILE + NP + i];  // U_base(l+1)
+      VA(A_RD)[i] = rl[3 * TILE + i];       // s_dn(l)
+      VA(A_BH)[i] = rl[3 * TILE + 2 * NP + 2 + i];  // s_up(l)
+      VA(A_BDN)[i] = VA(A_Y)[i];            // d s_dn starts at b_rhs
+      VA(A_BUP)[i] = VA(A_SU)[i];           // d s_up = d U_base(l)
+    }
+    X.sync();
+    if (scat && cb) {
+      // ---- general: A1 = I - Rb R, D1 = T A1^{-1}
+      op_gemm<Gm>(X.mo(J_TGc), X.mo(J_R), kNoMat, 1, X.mo(J_bR1), X.mo(J_bR1c), t);
+      X.sync();
+      singular |= op_gj<Gm>(X.mo(J_bR1), X.mo(J_TG), kNoMat, X.mo(J_bT1c), X.gjo(), X.redo(), t,
+                            X.bar, X.mo(J_bT1));
+      X.sync();
+      op_gemm<Gm>(X.mo(J_TGc), X.mo(J_TG), kNoMat, 0, X.mo(J_W), X.mo(J_Ac), t);   // Q = Rb T
+      op_gemm<Gm>(X.mo(J_bT1), X.mo(J_bTGR), kNoMat, 0, X.mo(J_C), X.mo(J_Cc), t);  // E = D1^T dRb
+      op_gemm<Gm>(X.mo(J_bT1c), X.mo(J_TGR), kNoMat, 0, X.mo(J_T1), kNoMat, t);     // F = D1 Rb
+      if (X.warp == 0) {
+        const Real* v1[1] = {VA(A_RD)};
+        Real rbd[1];
+        matvec<Gm, true, 1>(X.m(J_TGc), v1, rbd, X.lane);  // Rb s_dn
+        const Real* v2[1] = {VA(A_SU)};
+        Real bvv[1];
+        matvec<Gm, true, 1>(X.m(J_bT1), v2, bvv, X.lane);  // bv = D1^T dUb
+        if (X.lane < NP) {
+          VA(A_T0)[X.lane] = VA(A_RU)[X.lane] + rbd[0];  // v = Ub1 + Rb s_dn
+          VA(A_T1)[X.lane] = bvv[0];
+        }
+        __syncwarp();
+        const Real* v3[1] = {VA(A_T1)};
+        Real rtb[1];
+        matvec<Gm, true, 1>(X.m(J_TGR), v3, rtb, X.lane);  // Rb^T bv
+        if (X.lane < NP) VA(A_BDN)[X.lane] += rtb[0];
+      }
+      X.sync();
+      // dD1 = dRb Q^T + dUb v^T
+      op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Ac), kNoMat, 0, X.mo(J_bTG), kNoMat, t);
+      X.sync();
+      op_rank<Gm>(X.mo(J_bTG), kNoMat, vo(A_SU), vo(A_T0), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                  kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+      X.sync();
+      // W = dD1 A1^{-T}
+      singular |= op_gj<Gm>(X.mo(J_bR1c), X.mo(J_bTG), kNoMat, kNoMat, X.gjo(), X.redo(), t,
+                            X.bar, X.mo(J_T2));
+      X.sync();
+      // G1 = D1^T W (= -dA1);  dT = F^T dRb + W + b_rhs Id^T
+      op_gemm<Gm>(X.mo(J_bT1), X.mo(J_T2), kNoMat, 0, X.mo(J_W), X.mo(J_Ac), t);
+      op_gemm<Gm>(X.mo(J_T1), X.mo(J_bTGR), X.mo(J_T2), 0, X.mo(J_bT0), X.mo(J_bT0c), t);
+      X.sync();
+      // dRb(l+1) = E T^T + G1 R^T + bv s_dn^T (+ u(l+1) Id(l+1)^T below)
+      op_gemm<Gm>(X.mo(J_Cc), X.mo(J_Tc), kNoMat, 0, X.mo(J_T1), kNoMat, t);
+      X.sync();
+      op_gemm<Gm>(X.mo(J_Ac), X.mo(J_Rc), X.mo(J_T1), 0, X.mo(J_bR1), kNoMat, t);
+      // dR = dRb + Rb^T G1 + b_rhs b_l^T
+      op_gemm<Gm>(X.mo(J_TGR), X.mo(J_W), X.mo(J_bTGR), 0, X.mo(J_bR0), X.mo(J_bR0c), t);
+      X.sync();
+      op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_T1), vo(A_RD), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                  kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];  // d Ub(l+1) = bv
+    } else if (scat) {
+      // ---- base below reflects nothing: Ub = s_up + T Ub1, Rb = R
+      op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bR0), X.mo(J_bR0c), 1.0, t);
+      op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bT0), X.mo(J_bT0c), 0.0, t);
+      if (X.warp == 0) {
+        const Real* v1[1] = {VA(A_SU)};
+        Real ttb[1];
+        matvec<Gm, true, 1>(X.m(J_TG), v1, ttb, X.lane);  // T^T dUb
+        __syncwarp();
+        if (X.lane < NP) VA(A_T1)[X.lane] = ttb[0];
+      }
+      X.sync();
+      op_rank<Gm>(X.mo(J_bT0), X.mo(J_bT0c), vo(A_SU), vo(A_RU), 1.0, kNoMat, kNoMat, 0.0,
+                  kNoMat, kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+      op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bR1), kNoMat, 0.0, t);  // no dependence on Rb below
+      X.sync();  // the rank update above reads A_SU
+      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];
+    } else {
+      // ---- non-scattering layer: Ub = s_up + t (Ub1 + Rb s_dn), Rb = t Rb1 t
+      // its T is diagonal: only diag(dT) = dt is kept (in A_T0)
+      if (X.warp == 0) {
+        const Real* v1[1] = {VA(A_RD)};
+        Real rbd[1];
+        matvec<Gm, true, 1>(X.m(J_TGc), v1, rbd, X.lane);  // Rb s_dn
+        if (X.lane < NP) {
+          const int i = X.lane;
+          const double tv = X.m(J_TG)[i * LD + i];
+          const double v = VA(A_RU)[i] + rbd[0];
+          double dt = VA(A_SU)[i] * v + VA(A_Y)[i] * VA(A_Z)[i];  // + b_rhs Id (diag)
+          const Real* dRb = X.m(J_bTGR);
+          const Real* Rb1 = X.m(J_TGR);
+          for (int j = 0; j < NP; ++j) {
+            const double tj = X.m(J_TG)[j * LD + j];
+            dt += dRb[i * LD + j] * Rb1[i * LD + j] * tj + dRb[j * LD + i] * Rb1[j * LD + i] * tj;
+          }
+          VA(A_T0)[i] = dt;
+          VA(A_T1)[i] = tv * VA(A_SU)[i];  // bv
+        }
+        __syncwarp();
+        const Real* v3[1] = {VA(A_T1)};
+        Real rtb[1];
+        matvec<Gm, true, 1>(X.m(J_TGR), v3, rtb, X.lane);  // Rb^T bv
+        if (X.lane < NP) VA(A_BDN)[X.lane] += rtb[0];
+      }
+      X.sync();
+      if (tl.valid()) {  // dRb(l+1) = t dRb t (+ bv s_dn^T below)
+        const Real* dRb = X.m(J_bTGR);
+        Real* o = X.m(J_bR1);
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+          for (int b = 0; b < TC; ++b) {
+            const int r = tl.row(a), c = tl.col(b);
+            o[r * LD + c] = X.m(J_TG)[r * LD + r] * dRb[r * LD + c] * X.m(J_TG)[c * LD + c];
+          }
+      }
+      X.sync();
+      op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_T1), vo(A_RD), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                  kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];
+    }
+    X.sync();
+    // downward-pass contributions of interface l+1: dRb += u Id^T, dUb += u
+    if (X.warp == 0 && X.lane < NP) {
+      const int i = X.lane;
+      VA(A_SD)[i] = dv[(size_t)(l + 1) * 2 * NP + NP + i];      // u(l+1)
+      VA(A_BRU)[i] = iv[(size_t)(l + 1) * 2 * NP + i];          // Id(l+1)
+      VA(A_SU)[i] += VA(A_SD)[i];
+    }
+    X.sync();
+    op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_SD), vo(A_BRU), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+    X.sync();
+    op_s2g<Gm>(X.mo(J_bR1), brb, t);
+    // layer cotangents from the downward pass: dR += b_rhs b_l^T, dT += b_rhs Id^T
+    if (scat) {
+      op_rank<Gm>(X.mo(J_bR0), X.mo(J_bR0c), vo(A_Y), vo(A_H), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                  kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+      op_rank<Gm>(X.mo(J_bT0), X.mo(J_bT0c), vo(A_Y), vo(A_Z), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+                  kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+    }
+    X.sync();
+    // ---- this layer's own construction
+    const double Bt = lv.B[l], Bb = lv.B[l + 1];
+    if (scat) {
+      int nuse;
+      double f = -1.0;
+      const int u = fb ? nL - 1 - l : l;
+      const double* chi = C->moments + (layout == 0 ? (size_t)u * M
+                                        : layout == 1 ? (size_t)w * M
+                                                      : ((size_t)w * nL + u) * M);
+      nuse = C->delta_m ? ((M < 2 * N) ? M : 2 * N) : M;
+      nuse_l1 = nuse;
+      if (layout != 1)
+        build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+      doubling_adjoint<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
+                           Ppp, Ppm, tape, scal, &singular);
+      if (t == 0) {
+        gtau[l] += scal[0];
+        gom[l] += scal[1];
+        bB[l] += scal[2];
+        bB[l + 1] += scal[3];
+        if (solar) btc[l] += scal[4] * F0 * exp(-lv.tc[l] / mu0) * (-1.0 / mu0);
+      }
+      if (layout != 1) {
+        double* dchi = AD.g_mom ? AD.g_mom + (chi - C->moments) : nullptr;
+        if (dchi)
+          phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl, solar, mu0, dchi);
+      } else {  // one moment set per wavenumber: accumulate the phase cotangents
+        if (tl.valid()) {
+          double* aP = pacc + t * Gm::TE;
+          double* aM = pacc + NP * NP + t * Gm::TE;
+#pragma unroll
+          for (int a = 0; a < TR; ++a)
+#pragma unroll
+            for (int b = 0; b < TC; ++b) {
+              aP[a * TC + b] += X.m(J_T1)[tl.row(a) * LD + tl.col(b)];
+              aM[a * TC + b] += X.m(J_T2)[tl.row(a) * LD + tl.col(b)];
+            }
+        }
+        if (X.warp == 0 && X.lane < NP) {
+          pacc[2 * NP * NP + X.lane] += VA(A_T0)[X.lane];
+          pacc[2 * NP * NP + NP + X.lane] += VA(A_T1)[X.lane];
+        }
+      }
+    } else if (tau > 0.0) {
+      // pure absorption (src/doubling.hpp:56-77): t = exp(-tau/mu), linear-in-tau source
+      double pbar = 0.0, pd = 0.0, pt = 0.0;
+      const double Bbar = 0.5 * (Bb + Bt), Bd = (Bb - Bt) / tau;
+      if (X.warp == 0 && X.lane < N) {
+        const int i = X.lane;
+        const double mui = X.DV(D_MU)[i];
+        const double tex = -tau / mui;
+        const double tv = (tex > -200.0) ? exp(tex) : 0.0;
+        const double omt = 1.0 - tv, slope = mui * omt - 0.5 * tau * (1.0 + tv);
+        const double bu = VA(A_BUP)[i], bd = VA(A_BDN)[i];
+        double btv = VA(A_T0)[i];
+        pbar = (bu + bd) * omt;
+        pd = (bu - bd) * slope;
+        double bomt = (bu + bd) * Bbar;
+        const double bslope = (bu - bd) * Bd;
+        bomt += bslope * mui;
+        btv += bslope * (-0.5 * tau);
+        pt = bslope * (-0.5 * (1.0 + tv));
+        btv += -bomt;
+        pt += btv * tv * (-1.0 / mui);
+      }
+      double* red = reinterpret_cast<double*>(X.gjbuf) + 4;
+      pbar = gsum<G>(pbar, red, bar);
+      pd = gsum<G>(pd, red, bar);
+      pt = gsum<G>(pt, red, bar);
+      if (t == 0) {
+        bB[l + 1] += 0.5 * pbar + pd / tau;
+        bB[l] += 0.5 * pbar - pd / tau;
+        gtau[l] += pt - pd * Bd / tau;
+      }
+    }
+    X.sync();
+  }
+  // one moment set per wavenumber: its adjoint once
+  if (layout == 1 && AD.g_mom) {
+    op_g2s<Gm>(pacc, X.mo(J_T1), kNoMat, t);
+    op_g2s<Gm>(pacc + NP * NP, X.mo(J_T2), kNoMat, t);
+    if (X.warp == 0 && X.lane < NP) {
+      VA(A_T0)[X.lane] = pacc[2 * NP * NP + X.lane];
+      VA(A_T1)[X.lane] = pacc[2 * NP * NP + NP + X.lane];
+    }
+    X.sync();
+    const double* chi = C->moments + (size_t)w * M;
+    phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse_l1, N, C->quad.pl, solar, mu0,
+                      AD.g_mom + (size_t)w * M);
+  }
+  // ======== 3. lower boundary, beam and Planck chain rules
+  double pub = 0.0, pubmu = 0.0;
+  if (X.warp == 0 && X.lane < N) {
+    pub = VA(A_SU)[X.lane];
+    pubmu = VA(A_SU)[X.lane] * X.DV(D_MU)[X.lane];
+  }
+  double* red = reinterpret_cast<double*>(X.gjbuf) + 4;
+  pub = gsum<G>(pub, red, bar);
+  pubmu = gsum<G>(pubmu, red, bar);
+  if (t == 0) {
+    double bBs = 0.0;
+    if (has_surface) {
+      bBs = (1.0 - Aalb) * pub;
+      if (solar && Aalb > 0.0)
+        btc[nL] += pub * (Aalb / kPi) * F0 * mu0 * exp(-lv.tc[nL] / mu0) * (-1.0 / mu0);
+    } else if (C->diffusion) {
+      const double dt = lv.tau[nL - 1];
+      bB[nL] += pub;
+      if (dt > 0.0) {
+        const double dB = (lv.B[nL] - lv.B[nL - 1]) / dt;
+        bB[nL] += pubmu / dt;
+        bB[nL - 1] -= pubmu / dt;
+        gtau[nL - 1] += -pubmu * dB / dt;
+      }
+    } else {
+      bBs = pub;
+    }
+    if (C->thermal) {
+      if (C->surface_temperature < 0.0) bB[nL] += bBs;
+      if (C->top_temperature < 0.0) bB[0] += pBtop;
+    }
+    // cumulative tau: tc(l) = sum_{j<l} tau_j
+    double s = 0.0;
+    for (int l = nL; l >= 1; --l) {
+      s += btc[l];
+      gtau[l - 1] += s;
+    }
+  }
+  X.sync();
+  for (int l = t; l < nL; l += G) {
+    const int ul = fb ? nL - 1 - l : l;
+    const double om = lv.om[l];
+    if (AD.g_tau) AD.g_tau[(size_t)w * nL + ul] = gtau[l];
+    if (AD.g_ssa) AD.g_ssa[(size_t)w * nL + ul] = (om > 0.0 && om <= 1.0) ? gom[l] : 0.0;
+  }
+  for (int l = t; l <= nL; l += G) {
+    const int ul = fb ? nL - l : l;
+    if (C->thermal && AD.g_temp) {
+      const double Tv = C->temperature[(C->temp_per_wav ? wo : 0) + ul];
+      atomicAdd(&AD.g_temp[(C->temp_per_wav ? wo : 0) + ul], bB[l] * planck_band_deriv(wlo, whi, Tv));
+    } else if (!C->thermal && C->planck && AD.g_planck) {
+      AD.g_planck[wo + ul] = bB[l];
+    }
+  }
+  if (singular && t == 0) atomicOr(status, 1u);
+  X.sync();
+}
+
+// ---------------------------------------------------------------- kernel
+template <int NP>
+struct AdjKern {
+  using GD = Geo<NP, double>;
+  static constexpr size_t kMaxSmem = 227 * 1024;
+  static constexpr int G = GD::G;
+  static constexpr int kGroups =
+      (AdjGroup<NP>::bytes * 4 <= kMaxSmem) ? 4
+      : (AdjGroup<NP>::bytes * 3 <= kMaxSmem) ? 3
+      : (AdjGroup<NP>::bytes * 2 <= kMaxSmem) ? 2 : 1;
+  static constexpr int kThreads = kGroups * G;
+};
+
+template <int NP>
+__global__ void __launch_bounds__(128) adjoint_kernel(SolveParams P, ColumnDev col0, AdjDev AD) {
+  using GD = Geo<NP, double>;
+  constexpr int G = GD::G;
+  const int gib = threadIdx.x / G;
+  const int t = threadIdx.x % G;
+  const int bar = 1 + gib;
+  const unsigned goff = (unsigned)(gib * AdjGroup<NP>::bytes);
+  const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
+  const int slot = blockIdx.x * (blockDim.x / G) + gib;
+  char* sl = P.scratch + (size_t)slot * P.slot_bytes;
+  for (unsigned i = (unsigned)t * 4u; i < (unsigned)AdjGroup<NP>::bytes; i += (unsigned)G * 4u)
+    *sp<unsigned>(goff + i) = 0u;
+  gsync<G>(bar);
+  if (t == 0) *sp<ColumnDev>(goff + CommonLayout<NP>::col) = col0;
+  long long* task_s = sp<long long>(goff + CommonLayout<NP>::misc + 32);
+  for (;;) {
+    long long task;
+    if constexpr (G == 32) {
+      unsigned long long v = 0;
+      if (t == 0) v = atomicAdd(P.counter, 1ull);
+      task = (long long)__shfl_sync(0xffffffffu, v, 0);
+    } else {
+      gsync<G>(bar);
+      if (t == 0) *task_s = (long long)atomicAdd(P.counter, 1ull);
+      gsync<G>(bar);
+      task = *task_s;
+    }
+    if (task >= P.ntasks) break;
+    const int w = (int)task;
+    gsync<G>(bar);
+    wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, 0);
+    double* iv = reinterpret_cast<double*>(sl + AdjSlot<GD>::fwd(P.max_layers));
+    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status, iv);
+    wav_adjoint<NP>(goff, tb, t, bar, w, sl, P.max_layers, P.status, AD);
+  }
+}
+
+}  // namespace adrt_dev

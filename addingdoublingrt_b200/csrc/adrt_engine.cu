@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -16,7 +17,7 @@
 #include <vector>
 
 #include "../../include/adrt_b200.h"
-#include "adrt_kernel.cuh"
+#include "adrt_adjoint.cuh"
 
 using namespace adrt_dev;
 
@@ -152,6 +153,8 @@ struct adrt_engine {
   size_t max_ws = 0;
   cudaStream_t last_stream = nullptr;
   char* scratch = nullptr;
+  char* adj_scratch = nullptr;  // adjoint work buffer (larger slots)
+  size_t adj_scratch_bytes = 0;
   size_t scratch_bytes = 0;
   unsigned long long* counter = nullptr;
   unsigned int* status = nullptr;
@@ -461,6 +464,7 @@ int adrt_engine_destroy(adrt_engine* e) {
   for (auto& q : e->quad) cudaFree(q.buf);
   for (void* p : e->host_stage) cudaFree(p);
   cudaFree(e->stage);
+  cudaFree(e->adj_scratch);
   delete e;
   return ADRT_OK;
 }
@@ -617,6 +621,102 @@ int adrt_planck_band(double lo, double hi, double temp, double* out) {
   if (temp < 0.0 || hi < lo || lo < 0.0)
     return fail(ADRT_ERR_INVALID_ARGUMENT, "planckFunction: invalid arguments");
   *out = planck_band(lo, hi, temp);
+  return ADRT_OK;
+}
+
+int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
+                 const adrt_outputs* out, const adrt_cotangents* cot, const adrt_gradients* gr,
+                 void* stream_ptr) {
+  if (!e || !cot || !gr) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine, cotangents or gradients");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if ((rc = check_inputs(d, in))) return rc;
+  if (d->use_delta_m && d->num_moments > 2 * d->num_quadrature)
+    return fail(ADRT_ERR_UNSUPPORTED,
+                "adjoint: delta-M truncation (use_delta_m with num_moments > 2N) is not supported");
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = set_device(e))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  e->last_stream = s;
+  if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
+  const int np = padded_order(d->num_quadrature);
+  struct AK {
+    int groups, threads;
+    size_t smem, slot;
+    const void* fn;
+    void (*launch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
+  } k{};
+  auto make = [&](auto tag) {
+    constexpr int NP = decltype(tag)::value;
+    using GD = Geo<NP, double>;
+    k.groups = AdjKern<NP>::kGroups;
+    k.threads = AdjKern<NP>::kThreads;
+    k.smem = (size_t)k.groups * AdjGroup<NP>::bytes;
+    k.slot = (AdjSlot<GD>::bytes(d->num_layers) + 255) & ~size_t(255);
+    k.fn = reinterpret_cast<const void*>(adjoint_kernel<NP>);
+    k.launch = [](const SolveParams& p, const ColumnDev& c, const AdjDev& a, int grid, size_t smem,
+                  cudaStream_t st) {
+      adjoint_kernel<NP><<<grid, AdjKern<NP>::kThreads, smem, st>>>(p, c, a);
+    };
+  };
+  switch (np) {
+    case 4: make(std::integral_constant<int, 4>{}); break;
+    case 8: make(std::integral_constant<int, 8>{}); break;
+    case 16: make(std::integral_constant<int, 16>{}); break;
+    default: make(std::integral_constant<int, 32>{}); break;
+  }
+  CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+  int bps = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, k.threads, k.smem));
+  if (bps < 1) bps = 1;
+  int grid = bps * e->num_sms;
+  const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
+  grid = std::min(grid, need_blocks);
+  size_t need = (size_t)grid * k.groups * k.slot;
+  if (e->max_ws && need > e->max_ws) {
+    grid = (int)(e->max_ws / ((size_t)k.groups * k.slot));
+    if (grid < 1) return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint slot (%zu B)", k.slot);
+    need = (size_t)grid * k.groups * k.slot;
+  }
+  if (need > e->adj_scratch_bytes) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE, "adjoint work buffer too small during stream capture");
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->adj_scratch);
+    e->adj_scratch = nullptr;
+    e->adj_scratch_bytes = 0;
+    if (cudaMalloc(&e->adj_scratch, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "adjoint work buffer allocation of %zu B failed", need);
+    }
+    e->adj_scratch_bytes = need;
+  }
+  ColumnDev c0 = make_column(e, d, in, out);
+  SolveParams p{};
+  p.cols = nullptr;
+  p.ncols = 1;
+  p.ntasks = d->num_wavenumbers;
+  p.counter = e->counter;
+  p.status = e->status;
+  p.scratch = e->adj_scratch;
+  p.slot_bytes = k.slot;
+  p.nslots = grid * k.groups;
+  p.max_layers = d->num_layers;
+  AdjDev a{};
+  a.c_fu = cot->flux_up;
+  a.c_fd = cot->flux_down;
+  a.c_J = cot->mean_intensity;
+  a.c_fdir = cot->flux_direct;
+  a.g_tau = gr->delta_tau;
+  a.g_ssa = gr->single_scat_albedo;
+  a.g_mom = gr->phase_moments;
+  a.g_temp = gr->temperature;
+  a.g_planck = gr->planck_levels;
+  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+  k.launch(p, c0, a, grid, k.smem, s);
+  CUDA_TRY(cudaGetLastError());
   return ADRT_OK;
 }
 

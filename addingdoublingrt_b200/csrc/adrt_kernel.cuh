@@ -58,7 +58,8 @@ struct SlotLayout {
   using Real = typename Gm::Real;
   static constexpr int NP = Gm::NP;
   static constexpr int TILE = Gm::G * Gm::TE;  // Reals per matrix in tile order
-  static constexpr int REC_RAW = 3 * TILE + 2 * NP + 2;
+  // R, T, R_base tiles; s_dn, U_base; scat flag, base-reflects flag; s_up
+  static constexpr int REC_RAW = 3 * TILE + 3 * NP + 2;
   static constexpr int RALIGN = 16 / (int)sizeof(Real);
   static constexpr int REC = (REC_RAW + RALIGN - 1) / RALIGN * RALIGN;
   static __host__ __device__ size_t level_bytes(int lmax) {
@@ -70,6 +71,16 @@ struct SlotLayout {
   static __host__ __device__ size_t bytes(int lmax) {
     return level_bytes(lmax) + phase_bytes() + (size_t)(lmax + 1) * REC * sizeof(Real);
   }
+};
+
+// One step of the adjoint's doubling record (per layer, nn steps): R, T, TG
+// tiles (TG taken from its column-major buffer, i.e. TG^T in tile order),
+// then y, z, s_up, s_dn and gamma.
+template <class Gm>
+struct TapeLayout {
+  static constexpr int NP = Gm::NP;
+  static constexpr int TILE = Gm::G * Gm::TE;
+  static constexpr int STEP = (3 * TILE + 4 * NP + 1 + 1) / 2 * 2;
 };
 
 // Shared-memory bytes of one group for a kernel kind: the common prefix and
@@ -250,7 +261,8 @@ template <class Gm>
 __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
                                      double om, double Bt, double Bb, double tcum, int N,
                                      bool solar, double F0, double mu0, const double* Ppp,
-                                     const double* Ppm, int* singular) {
+                                     const double* Ppm, int* singular,
+                                     typename Gm::Real* tape = nullptr) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC;
@@ -335,6 +347,20 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     X.sync();
     *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
     X.sync();
+    if (tape) {  // the adjoint's record of this step: R, T, TG (stored from column-major) + vectors
+      using Tp = TapeLayout<Gm>;
+      Real* tk = tape + (size_t)k * Tp::STEP;
+      op_s2g<Gm>(oR, tk, t);
+      op_s2g<Gm>(oTc, tk + Tp::TILE, t);
+      op_s2g<Gm>(oTG, tk + 2 * Tp::TILE, t);
+      if (X.warp == 0 && X.lane < NP) {
+        tk[3 * Tp::TILE + X.lane] = y[X.lane];
+        tk[3 * Tp::TILE + NP + X.lane] = z[X.lane];
+        tk[3 * Tp::TILE + 2 * NP + X.lane] = su[X.lane];
+        tk[3 * Tp::TILE + 3 * NP + X.lane] = sd[X.lane];
+      }
+      if (t == 0) tk[3 * Tp::TILE + 4 * NP] = gam;
+    }
     op_gemm<Gm>(oTG, oR, kNoMat, 0, kNoMat, oA, t);  // TGR = TG R (column-major)
     X.sync();
     op_gemm<Gm>(oA, oTc, oR, 0, oR, oRc, t);                 // R <- R + TGR T
@@ -738,7 +764,8 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
 // the FP32 region of a class-D group.
 template <class Gm, int MODE>
 __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, int t_, int bar,
-                                      int w, char* slot, int lmax, unsigned* status) {
+                                      int w, char* slot, int lmax, unsigned* status,
+                                      double* ivec = nullptr) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   using SLay = SlotLayout<Gm>;
@@ -903,7 +930,10 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
       op_s2g<Gm>(X.mo(0), rp, t);
       op_s2g<Gm>(X.mo(tcur), rp + TILE, t);
     }
-    if (X.warp == 0 && X.lane < NP) rp[3 * TILE + X.lane] = X.V(V_SDN)[X.lane];
+    if (X.warp == 0 && X.lane < NP) {
+      rp[3 * TILE + X.lane] = X.V(V_SDN)[X.lane];
+      rp[3 * TILE + 2 * NP + 2 + X.lane] = X.V(V_SUP)[X.lane];
+    }
     if (t == 0) rp[3 * TILE + 2 * NP] = Real(scat);
 
     // adding: top = this layer, bottom = composite (src/adding.hpp:478-490)
@@ -993,6 +1023,10 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
     matvec<Gm, true, 1>(X.m(0), vv, yv, X.lane);
     if (X.lane < NP) X.V(V_IU)[X.lane] = yv[0] + X.V(V_UB)[X.lane];
     __syncwarp();
+    if (ivec && X.lane < NP) {  // interface intensities for the adjoint
+      ivec[X.lane] = X.V(V_ID)[X.lane];
+      ivec[NP + X.lane] = X.V(V_IU)[X.lane];
+    }
     if (X.lane == 0) emit_interface<Gm>(X, C, w, 0, N, solar, F0, mu0, lv, status);
   }
   for (int l = 0; l < nL; ++l) {
@@ -1042,6 +1076,10 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
         X.V(V_IU)[X.lane] = yv[0] + X.V(V_UB)[X.lane];
       }
       __syncwarp();
+      if (ivec && X.lane < NP) {
+        ivec[(size_t)(l + 1) * 2 * NP + X.lane] = X.V(V_ID)[X.lane];
+        ivec[(size_t)(l + 1) * 2 * NP + NP + X.lane] = X.V(V_IU)[X.lane];
+      }
       if (X.lane == 0)
         emit_interface<Gm>(X, C, w, l + 1, N, solar, F0, mu0, lv, status);
     }

@@ -290,9 +290,12 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
     for (int j = 0; j < WC; ++j) {
       const int r = r0 + i * 8 + g, c = c0 + j * 8 + 2 * q;
       double v0 = acc[i][j][0], v1 = acc[i][j][1];
-      if (id_minus) {
+      if (id_minus == 1) {
         v0 = ((r == c) ? 1.0 : 0.0) - v0;
         v1 = ((r == c + 1) ? 1.0 : 0.0) - v1;
+      } else if (id_minus == 2) {
+        v0 = -v0;
+        v1 = -v1;
       }
       if (add) {
         const double2 ad = *reinterpret_cast<const double2*>(add + r * LD + c);
@@ -307,7 +310,8 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
     }
 }
 
-// out = [I -] X Y [+ add]: X column-major (XT[k*LD + r] = X[r][k]), Y and add
+// out = [I -] X Y [+ add] (id_minus = 1), or -X Y [+ add] (id_minus = 2):
+// X column-major (XT[k*LD + r] = X[r][k]), Y and add
 // row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
 // alias out_rm (each thread reads its own tile before writing it).
 // Marks an absent optional operand (add / out_rm / out_cm / B / bvec).
@@ -351,7 +355,8 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
     for (int a = 0; a < TR; ++a)
 #pragma unroll
       for (int b = 0; b < TC; ++b)
-        acc[a][b] = ((tl.row(a) == tl.col(b)) ? Real(1) : Real(0)) - acc[a][b];
+        acc[a][b] = (id_minus == 2) ? -acc[a][b]
+                                    : ((tl.row(a) == tl.col(b)) ? Real(1) : Real(0)) - acc[a][b];
   }
   if (add) {
     Real ad[TR][TC];
@@ -452,7 +457,7 @@ __device__ __noinline__ void op_gemm_lam(unsigned xt_off, unsigned y_off, unsign
 template <class Gm>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
-                                  int bar) {
+                                  int bar, unsigned orm_off = 0xffffffffu) {
   using Real = typename Gm::Real;
   const Real* A_rm = sp<Real>(a_off);
   const Real* B_rm = (b_off == kNoMat) ? nullptr : sp<Real>(b_off);
@@ -576,7 +581,12 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
       Real colv[TR];
 #pragma unroll
       for (int a = 0; a < TR; ++a) colv[a] = B[a][b];
-      sts_vec<Real, TR>(out_cm + q[b] * LD + tl.rb * TR, colv);
+      if (ocm_off != 0xffffffffu) sts_vec<Real, TR>(out_cm + q[b] * LD + tl.rb * TR, colv);
+      if (orm_off != 0xffffffffu) {
+        Real* out_rm = sp<Real>(orm_off);
+#pragma unroll
+        for (int a = 0; a < TR; ++a) out_rm[tl.row(a) * LD + q[b]] = colv[a];
+      }
     }
   }
   return singular;

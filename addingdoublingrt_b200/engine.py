@@ -74,6 +74,32 @@ class Engine:
         _lib.check(self.lib.adrt_solve_batch(self.handle, C.byref(desc), C.byref(ins),
                                              C.byref(outs), s))
 
+    def adjoint(self, desc: _abi.BatchDesc, dev_inputs: dict, cotangents: dict, gradients: dict,
+                dev_outputs: dict | None = None, stream=None) -> None:
+        """adrt_adjoint on CUDA tensors: gradients of sum(cotangent * output) with respect to
+        the inputs named in `gradients` (delta_tau and single_scat_albedo are overwritten,
+        phase_moments / temperature / planck_levels are added to)."""
+        ins = _abi.Inputs()
+        for f in _abi.INPUT_FIELDS:
+            setattr(ins, f, _ptr(dev_inputs.get(f)))
+        cot = _abi.Cotangents()
+        for f in _abi.COTANGENT_FIELDS:
+            setattr(cot, f, _ptr(cotangents.get(f)))
+        gr = _abi.Gradients()
+        for f in _abi.GRADIENT_FIELDS:
+            setattr(gr, f, _ptr(gradients.get(f)))
+        outp = None
+        if dev_outputs is not None:
+            outs = _abi.Outputs()
+            for f in _abi.OUTPUT_FIELDS:
+                setattr(outs, f, _ptr(dev_outputs.get(f)))
+            outp = C.byref(outs)
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        _lib.check(self.lib.adrt_adjoint(self.handle, C.byref(desc), C.byref(ins), outp,
+                                         C.byref(cot), C.byref(gr), s))
+
     def solve_uneven(self, columns: list, stream=None) -> None:
         """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
         arr = (_abi.ColumnDesc * len(columns))()

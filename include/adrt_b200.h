@@ -227,6 +227,43 @@ int adrt_validate_batch(const adrt_batch_desc* desc, const adrt_inputs* host_in)
 int adrt_solve_batch_noalloc(const adrt_batch_desc* desc, const adrt_inputs* in,
                              const adrt_outputs* out, void* cuda_stream);
 
+/* ------------------------------------------------------------- adjoint */
+
+/* Cotangents of a scalar loss with respect to the per-interface outputs
+ * ([W*(L+1)] device arrays in the output layout, NULL = zero). */
+typedef struct adrt_cotangents {
+  const double* flux_up;
+  const double* flux_down;
+  const double* mean_intensity;
+  const double* flux_direct;
+} adrt_cotangents;
+
+/* Gradients (device arrays in the input layouts, NULL = not wanted).
+ * delta_tau and single_scat_albedo [W*L] are overwritten; phase_moments,
+ * temperature and planck_levels are ADDED to (shared layouts sum over the
+ * wavenumbers), so zero them first. */
+typedef struct adrt_gradients {
+  double* delta_tau;
+  double* single_scat_albedo;
+  double* phase_moments;
+  double* temperature;
+  double* planck_levels;
+} adrt_gradients;
+
+/* Reverse-mode adjoint of the batched solve: given the loss cotangents,
+ * the gradients with respect to delta_tau, single_scat_albedo, the phase
+ * moments and the level temperatures (through dB/dT, the reference's
+ * planckFunctionDeriv, src/planck.cpp:135-175) or the Planck levels.  The
+ * derivative is that of the discrete scheme at fixed doubling counts; it
+ * generalises the reference's analytic temperature Jacobian
+ * (src/solver.cpp:117-341) to all inputs.  FP64; every layer's doubling chain
+ * is recomputed in the backward pass (not stored).  `out` may be NULL or
+ * receive the forward outputs.  Not supported: delta-M truncation in effect
+ * (use_delta_m with num_moments > 2N). */
+int adrt_adjoint(adrt_engine* engine, const adrt_batch_desc* desc, const adrt_inputs* in,
+                 const adrt_outputs* out, const adrt_cotangents* cot,
+                 const adrt_gradients* grads, void* cuda_stream);
+
 /* ------------------------------------------------------- uneven batches */
 
 /* One column of an uneven batch (reference: several solveBatch calls).

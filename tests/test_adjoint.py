@@ -1,0 +1,193 @@
+"""The adjoint (adrt_adjoint) against central finite differences of the oracle
+and against the reference's own analytic temperature Jacobian (GPU).
+
+The loss is L = sum over wavenumbers and interfaces of c . (F_up, F_down, J,
+F_dir) with random cotangents c.  Finite differences perturb one input for all
+wavenumbers at once (wavenumbers are independent) and use the oracle (the C
+restatement, FP64).  The doubling count nn is piecewise constant in tau and
+omega (src/doubling.hpp:20-26, 107-109); the adjoint differentiates the scheme
+at fixed nn, so parameters whose perturbation would change nn are skipped.
+
+The reference computes dF/dT analytically (src/solver.cpp:117-341); the
+adjoint's temperature gradient contracted against the same cotangents must
+match it.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import cuda_available
+from addingdoublingrt_b200 import _abi, workloads
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+COT = ("flux_up", "flux_down", "mean_intensity", "flux_direct")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    from addingdoublingrt_b200.engine import Engine
+    e = Engine()
+    yield e
+    e.close()
+
+
+def small_batch(seed, N, W=5, L=7, layout=_abi.MOMENTS_SHARED, temp_per_wav=False):
+    """Config-5-like: thermal + solar, single-HG moments, 2N moments (delta-M no-op)."""
+    rng = np.random.default_rng(seed)
+    M = 2 * N
+    d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
+                       moment_layout=layout, use_thermal_emission=1, use_delta_m=1,
+                       surface_temperature=300.0, solar_flux=1.0,
+                       temperature_per_wavenumber=int(temp_per_wav))
+    b = workloads.Batch(d)
+    b.set("delta_tau", 10.0 ** rng.uniform(-2.5, 0.7, size=(W, L)))
+    om = rng.uniform(0.1, 0.95, size=(W, L))
+    om[:, 2] = 0.0  # one purely absorbing layer
+    b.set("single_scat_albedo", om)
+    nsets = {0: L, 1: W, 2: W * L}[layout]
+    b.set("phase_moments", workloads.hg_moments(rng.uniform(0.4, 0.85, size=nsets), M))
+    T = workloads.level_temperatures(rng, L)
+    b.set("temperature", np.tile(T, (W, 1)) + rng.normal(0, 1, (W, L + 1)) if temp_per_wav else T)
+    b.set("surface_albedo", rng.uniform(0.05, 0.3, size=W))
+    b.set("solar_mu", rng.uniform(0.3, 1.0, size=W))
+    lo = rng.uniform(600.0, 2000.0, size=W)
+    b.set("wavenumber_low", lo)
+    b.set("wavenumber_high", lo + 5.0)
+    return b
+
+
+def run_adjoint(eng, b, cot, which=("delta_tau", "single_scat_albedo", "phase_moments",
+                                    "temperature")):
+    import torch
+    from addingdoublingrt_b200.engine import to_device
+    di = to_device(b)
+    dc = {k: torch.from_numpy(v).cuda() for k, v in cot.items()}
+    dg = {k: torch.zeros_like(di[k]) for k in which}
+    eng.adjoint(b.desc, di, dc, dg)
+    torch.cuda.synchronize()
+    assert eng.read_status() == 0
+    return {k: v.cpu().numpy().reshape(b.arrays[k].shape) for k, v in dg.items()}
+
+
+def loss_per_wav(b, cot):
+    out = oracle.solve_oracle(b, 4, which=COT)
+    return sum((cot[k] * out[k]).reshape(b.W, -1).sum(axis=1) for k in COT)
+
+
+def nn_of(tau, om):
+    lib = oracle.oracle_lib()
+    return lib.oracle_num_doublings(float(tau), float(min(om, 1.0))) if tau > 0 and om > 0 else -1
+
+
+def fd_layer_param(b, cot, name, rel=1e-5):
+    """d loss / d name[w, l] by central differences (all wavenumbers at once);
+    NaN where the perturbation changes the doubling count."""
+    base = b.arrays[name].reshape(b.W, b.L)
+    tau = b.arrays["delta_tau"].reshape(b.W, b.L)
+    om = b.arrays["single_scat_albedo"].reshape(b.W, b.L)
+    g = np.full((b.W, b.L), np.nan)
+    for l in range(b.L):
+        h = rel * np.maximum(np.abs(base[:, l]), 1e-3)
+        ok = np.ones(b.W, bool)
+        vals = []
+        for sgn in (1.0, -1.0):
+            a = base.copy()
+            a[:, l] += sgn * h
+            for w in range(b.W):
+                t2 = a[w, l] if name == "delta_tau" else tau[w, l]
+                o2 = a[w, l] if name == "single_scat_albedo" else om[w, l]
+                if nn_of(t2, o2) != nn_of(tau[w, l], om[w, l]):
+                    ok[w] = False
+            bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+            bb.set(name, a)
+            vals.append(loss_per_wav(bb, cot))
+        g[:, l] = np.where(ok, (vals[0] - vals[1]) / (2 * h), np.nan)
+    return g
+
+
+def rel_err(ad, fd):
+    m = ~np.isnan(fd)
+    return float(np.max(np.abs(ad[m] - fd[m])) / np.max(np.abs(fd[m])))
+
+
+@pytest.mark.parametrize("N", [4, 8, 16])
+def test_adjoint_tau_and_omega_match_finite_differences(eng, N):
+    b = small_batch(11 + N, N)
+    rng = np.random.default_rng(N)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot)
+    for name in ("delta_tau", "single_scat_albedo"):
+        fd = fd_layer_param(b, cot, name)
+        e = rel_err(ad[name].reshape(b.W, b.L), fd)
+        assert e < 2e-5, (name, N, e)
+
+
+def test_adjoint_moments_and_temperatures_match_finite_differences(eng):
+    b = small_batch(3, 8, W=4, L=6)
+    rng = np.random.default_rng(3)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot)
+    M = b.desc.num_moments
+    chi = b.arrays["phase_moments"].reshape(b.L, M)
+    fd = np.zeros_like(chi)
+    h = 1e-5
+    for l in range(b.L):
+        for m in range(M):
+            vals = []
+            for sgn in (1.0, -1.0):
+                c = chi.copy()
+                c[l, m] += sgn * h
+                bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+                bb.set("phase_moments", c)
+                vals.append(loss_per_wav(bb, cot).sum())
+            fd[l, m] = (vals[0] - vals[1]) / (2 * h)
+    e = rel_err(ad["phase_moments"].reshape(b.L, M), fd)
+    assert e < 1e-4, ("phase_moments", e)
+    T = b.arrays["temperature"]
+    fdT = np.zeros_like(T)
+    for l in range(b.L + 1):
+        vals = []
+        for sgn in (1.0, -1.0):
+            a = T.copy()
+            a[l] += sgn * 1e-3
+            bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+            bb.set("temperature", a)
+            vals.append(loss_per_wav(bb, cot).sum())
+        fdT[l] = (vals[0] - vals[1]) / 2e-3
+    e = rel_err(ad["temperature"], fdT)
+    assert e < 1e-4, ("temperature", e)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference build (oracle/_ref) absent")
+def test_temperature_gradient_matches_reference_analytic_jacobian(eng):
+    """Per wavenumber, dL/dT_l from the adjoint equals cot . J_T of the reference's
+    analytic Jacobian (levels 0..L; the surface temperature column is not an input
+    gradient here)."""
+    import ctypes as C
+    b = small_batch(21, 8, W=3, L=6, temp_per_wav=True)
+    b.set("solar_mu", np.full(b.W, 0.6))
+    rng = np.random.default_rng(21)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot)["temperature"].reshape(b.W, b.L + 1)
+    lib = oracle.ref_lib()
+    L = b.L
+    for w in range(b.W):
+        jac = {k: np.zeros((L + 1) * (L + 2)) for k in ("flux_up", "flux_down", "mean_intensity")}
+        out = b.alloc_outputs()
+        ins = b.inputs_struct()
+        rc = lib.ref_solve_column_jacobian(C.byref(b.desc), C.byref(ins), w,
+                                           C.byref(workloads.Batch.outputs_struct(out)),
+                                           jac["flux_up"].ctypes.data, jac["flux_down"].ctypes.data,
+                                           jac["mean_intensity"].ctypes.data, None)
+        assert rc == 0, lib.ref_last_error()
+        g = np.zeros(L + 1)
+        for k in ("flux_up", "flux_down", "mean_intensity"):
+            J = jac[k].reshape(L + 1, L + 2)[:, :L + 1]
+            g += cot[k].reshape(b.W, L + 1)[w] @ J
+        e = np.max(np.abs(ad[w] - g)) / np.max(np.abs(g))
+        assert e < 1e-6, (w, e)
