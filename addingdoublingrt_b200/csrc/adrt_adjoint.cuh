@@ -147,10 +147,11 @@ enum AdjMat {
   J_bT1, J_bT1c, J_bTGR, J_bTGRc, J_bTG, J_W, J_C, J_Cc, J_T1, J_T2, J_VEC,
   kMatsAdj = J_VEC + 2  // J_VEC spans two buffers (18 vectors even at NP = 8)
 };
-// Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 18 NP).
+// Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 20 NP).
 enum AdjVec {
   A_BY = 0, A_BZ, A_BSU, A_BSD, A_H, A_RU, A_RD, A_BRU, A_BRD, A_BH, A_Y, A_Z, A_SU, A_SD,
-  A_BUP, A_BDN, A_T0, A_T1
+  A_BUP, A_BDN, A_T0, A_T1,
+  A_CUB  // the adding adjoint's carried d U_base (not touched by the layer adjoints)
 };
 
 // Adjoint slot in HBM: the forward slot (levels, phase, records), the
@@ -717,12 +718,12 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   }
 
   // ======== 2. adding adjoint, layer 0 .. L-1, with each layer's own chain
-  // carried: d R_base(l) in brb (tiles), d U_base(l) in A_SU
+  // carried: d R_base(l) in brb (tiles), d U_base(l) in A_CUB
   {  // interface 0: d Rb0 = u0 Id0^T, d Ub0 = u0
     double* tu = VA(A_BUP);
     if (X.warp == 0 && X.lane < NP) {
       tu[X.lane] = dv[NP + X.lane];
-      VA(A_SU)[X.lane] = dv[NP + X.lane];
+      VA(A_CUB)[X.lane] = dv[NP + X.lane];
       VA(A_SD)[X.lane] = iv[X.lane];  // Id0
     }
     X.sync();
@@ -756,7 +757,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       VA(A_RD)[i] = rl[3 * TILE + i];       // s_dn(l)
       VA(A_BH)[i] = rl[3 * TILE + 2 * NP + 2 + i];  // s_up(l)
       VA(A_BDN)[i] = VA(A_Y)[i];            // d s_dn starts at b_rhs
-      VA(A_BUP)[i] = VA(A_SU)[i];           // d s_up = d U_base(l)
+      VA(A_BUP)[i] = VA(A_CUB)[i];           // d s_up = d U_base(l)
     }
     X.sync();
     if (scat && cb) {
@@ -773,7 +774,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
         const Real* v1[1] = {VA(A_RD)};
         Real rbd[1];
         matvec<Gm, true, 1>(X.m(J_TGc), v1, rbd, X.lane);  // Rb s_dn
-        const Real* v2[1] = {VA(A_SU)};
+        const Real* v2[1] = {VA(A_CUB)};
         Real bvv[1];
         matvec<Gm, true, 1>(X.m(J_bT1), v2, bvv, X.lane);  // bv = D1^T dUb
         if (X.lane < NP) {
@@ -790,7 +791,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       // dD1 = dRb Q^T + dUb v^T
       op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Ac), kNoMat, 0, X.mo(J_bTG), kNoMat, t);
       X.sync();
-      op_rank<Gm>(X.mo(J_bTG), kNoMat, vo(A_SU), vo(A_T0), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
+      op_rank<Gm>(X.mo(J_bTG), kNoMat, vo(A_CUB), vo(A_T0), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
                   kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
       X.sync();
       // W = dD1 A1^{-T}
@@ -810,24 +811,24 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       X.sync();
       op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_T1), vo(A_RD), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
                   kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
-      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];  // d Ub(l+1) = bv
+      if (X.warp == 0 && X.lane < NP) VA(A_CUB)[X.lane] = VA(A_T1)[X.lane];  // d Ub(l+1) = bv
     } else if (scat) {
       // ---- base below reflects nothing: Ub = s_up + T Ub1, Rb = R
       op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bR0), X.mo(J_bR0c), 1.0, t);
       op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bT0), X.mo(J_bT0c), 0.0, t);
       if (X.warp == 0) {
-        const Real* v1[1] = {VA(A_SU)};
+        const Real* v1[1] = {VA(A_CUB)};
         Real ttb[1];
         matvec<Gm, true, 1>(X.m(J_TG), v1, ttb, X.lane);  // T^T dUb
         __syncwarp();
         if (X.lane < NP) VA(A_T1)[X.lane] = ttb[0];
       }
       X.sync();
-      op_rank<Gm>(X.mo(J_bT0), X.mo(J_bT0c), vo(A_SU), vo(A_RU), 1.0, kNoMat, kNoMat, 0.0,
+      op_rank<Gm>(X.mo(J_bT0), X.mo(J_bT0c), vo(A_CUB), vo(A_RU), 1.0, kNoMat, kNoMat, 0.0,
                   kNoMat, kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
       op_copy<Gm>(X.mo(J_bTGR), X.mo(J_bR1), kNoMat, 0.0, t);  // no dependence on Rb below
-      X.sync();  // the rank update above reads A_SU
-      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];
+      X.sync();  // the rank update above reads A_CUB
+      if (X.warp == 0 && X.lane < NP) VA(A_CUB)[X.lane] = VA(A_T1)[X.lane];
     } else {
       // ---- non-scattering layer: Ub = s_up + t (Ub1 + Rb s_dn), Rb = t Rb1 t
       // its T is diagonal: only diag(dT) = dt is kept (in A_T0)
@@ -839,7 +840,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
           const int i = X.lane;
           const double tv = X.m(J_TG)[i * LD + i];
           const double v = VA(A_RU)[i] + rbd[0];
-          double dt = VA(A_SU)[i] * v + VA(A_Y)[i] * VA(A_Z)[i];  // + b_rhs Id (diag)
+          double dt = VA(A_CUB)[i] * v + VA(A_Y)[i] * VA(A_Z)[i];  // + b_rhs Id (diag)
           const Real* dRb = X.m(J_bTGR);
           const Real* Rb1 = X.m(J_TGR);
           for (int j = 0; j < NP; ++j) {
@@ -847,7 +848,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
             dt += dRb[i * LD + j] * Rb1[i * LD + j] * tj + dRb[j * LD + i] * Rb1[j * LD + i] * tj;
           }
           VA(A_T0)[i] = dt;
-          VA(A_T1)[i] = tv * VA(A_SU)[i];  // bv
+          VA(A_T1)[i] = tv * VA(A_CUB)[i];  // bv
         }
         __syncwarp();
         const Real* v3[1] = {VA(A_T1)};
@@ -870,7 +871,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       X.sync();
       op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_T1), vo(A_RD), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
                   kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
-      if (X.warp == 0 && X.lane < NP) VA(A_SU)[X.lane] = VA(A_T1)[X.lane];
+      if (X.warp == 0 && X.lane < NP) VA(A_CUB)[X.lane] = VA(A_T1)[X.lane];
     }
     X.sync();
     // downward-pass contributions of interface l+1: dRb += u Id^T, dUb += u
@@ -878,7 +879,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       const int i = X.lane;
       VA(A_SD)[i] = dv[(size_t)(l + 1) * 2 * NP + NP + i];      // u(l+1)
       VA(A_BRU)[i] = iv[(size_t)(l + 1) * 2 * NP + i];          // Id(l+1)
-      VA(A_SU)[i] += VA(A_SD)[i];
+      VA(A_CUB)[i] += VA(A_SD)[i];
     }
     X.sync();
     op_rank<Gm>(X.mo(J_bR1), kNoMat, vo(A_SD), vo(A_BRU), 1.0, kNoMat, kNoMat, 0.0, kNoMat,
@@ -986,8 +987,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   // ======== 3. lower boundary, beam and Planck chain rules
   double pub = 0.0, pubmu = 0.0;
   if (X.warp == 0 && X.lane < N) {
-    pub = VA(A_SU)[X.lane];
-    pubmu = VA(A_SU)[X.lane] * X.DV(D_MU)[X.lane];
+    pub = VA(A_CUB)[X.lane];
+    pubmu = VA(A_CUB)[X.lane] * X.DV(D_MU)[X.lane];
   }
   double* red = reinterpret_cast<double*>(X.gjbuf) + 4;
   pub = gsum<G>(pub, red, bar);

@@ -93,15 +93,18 @@ def fd_layer_param(b, cot, name, rel=1e-5):
     g = np.full((b.W, b.L), np.nan)
     for l in range(b.L):
         h = rel * np.maximum(np.abs(base[:, l]), 1e-3)
-        ok = np.ones(b.W, bool)
+        # omega = 0 switches the layer to the pure-absorption branch: not differentiable
+        ok = base[:, l] > h if name == "single_scat_albedo" else np.ones(b.W, bool)
+        a_safe = base.copy()
+        a_safe[~ok, l] = 0.5 if name == "single_scat_albedo" else a_safe[~ok, l]
         vals = []
         for sgn in (1.0, -1.0):
-            a = base.copy()
+            a = a_safe.copy()
             a[:, l] += sgn * h
             for w in range(b.W):
                 t2 = a[w, l] if name == "delta_tau" else tau[w, l]
                 o2 = a[w, l] if name == "single_scat_albedo" else om[w, l]
-                if nn_of(t2, o2) != nn_of(tau[w, l], om[w, l]):
+                if ok[w] and nn_of(t2, o2) != nn_of(tau[w, l], om[w, l]):
                     ok[w] = False
             bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
             bb.set(name, a)
