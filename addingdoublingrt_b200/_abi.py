@@ -94,7 +94,7 @@ class Outputs(C.Structure):
 
 COTANGENT_FIELDS = ("flux_up", "flux_down", "mean_intensity", "flux_direct")
 GRADIENT_FIELDS = ("delta_tau", "single_scat_albedo", "phase_moments", "temperature",
-                   "planck_levels")
+                   "planck_levels", "surface_emission")
 
 
 class Cotangents(C.Structure):

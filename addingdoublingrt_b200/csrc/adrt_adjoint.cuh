@@ -192,7 +192,7 @@ struct AdjGroup {
 // Cotangent / gradient pointers of one batch (device).
 struct AdjDev {
   const double *c_fu, *c_fd, *c_J, *c_fdir;  // [W*(L+1)] each, or null
-  double *g_tau, *g_ssa, *g_mom, *g_temp, *g_planck;
+  double *g_tau, *g_ssa, *g_mom, *g_temp, *g_planck, *g_semis;
 };
 
 // ---------------------------------------------------------------- doubling adjoint
@@ -1014,6 +1014,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     if (C->thermal) {
       if (C->surface_temperature < 0.0) bB[nL] += bBs;
       if (C->top_temperature < 0.0) bB[0] += pBtop;
+    } else if (AD.g_semis) {
+      AD.g_semis[w] = bBs;
     }
     // cumulative tau: tc(l) = sum_{j<l} tau_j
     double s = 0.0;

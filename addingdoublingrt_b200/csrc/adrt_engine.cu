@@ -160,6 +160,8 @@ struct adrt_engine {
   unsigned int* status = nullptr;
   ColumnDev* d_cols = nullptr;
   size_t d_cols_cap = 0;
+  ColumnDev* h_cols = nullptr;       // pinned staging of the column table
+  cudaEvent_t cols_copied = nullptr;  // the last table upload has been read
   struct Quad {
     double* buf = nullptr;
     int mmax = 0;
@@ -461,6 +463,8 @@ int adrt_engine_destroy(adrt_engine* e) {
   cudaFree(e->counter);
   cudaFree(e->status);
   cudaFree(e->d_cols);
+  if (e->h_cols) cudaFreeHost(e->h_cols);
+  if (e->cols_copied) cudaEventDestroy(e->cols_copied);
   for (auto& q : e->quad) cudaFree(q.buf);
   for (void* p : e->host_stage) cudaFree(p);
   cudaFree(e->stage);
@@ -714,6 +718,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   a.g_mom = gr->phase_moments;
   a.g_temp = gr->temperature;
   a.g_planck = gr->planck_levels;
+  a.g_semis = gr->surface_emission;
   CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
   k.launch(p, c0, a, grid, k.smem, s);
   CUDA_TRY(cudaGetLastError());
@@ -724,63 +729,135 @@ int adrt_solve_batch_uneven(adrt_engine* e, const adrt_column_desc* cols, int nc
                             void* stream_ptr) {
   if (!e || !cols || ncols < 1) return fail(ADRT_ERR_INVALID_ARGUMENT, "bad uneven-batch arguments");
   int rc;
-  int np = -1, prec = -1, lmax = 0, mmax = 0;
+  int lmax_s = 0, lmax_l = 0, any_mixed_l = 0;
+  std::vector<int> small, large;
   for (int i = 0; i < ncols; ++i) {
     if ((rc = check_desc(&cols[i].desc))) return rc;
     if ((rc = check_inputs(&cols[i].desc, &cols[i].in))) return rc;
-    const int npi = padded_order(cols[i].desc.num_quadrature);
-    if (np >= 0 && (npi != np || cols[i].desc.precision != prec))
-      return fail(ADRT_ERR_UNSUPPORTED,
-                  "uneven batch: columns must share the padded quadrature class and precision");
-    np = npi;
-    prec = cols[i].desc.precision;
-    lmax = std::max(lmax, cols[i].desc.num_layers);
-    mmax = std::max(mmax, cols[i].desc.num_moments);
+    if (padded_order(cols[i].desc.num_quadrature) <= 16) {
+      small.push_back(i);
+      lmax_s = std::max(lmax_s, cols[i].desc.num_layers);
+    } else {
+      large.push_back(i);
+      lmax_l = std::max(lmax_l, cols[i].desc.num_layers);
+      any_mixed_l |= cols[i].desc.precision == ADRT_PRECISION_MIXED;
+    }
   }
+  // longest columns first (cost ~ L NP^3 per wavenumber), so the persistent
+  // kernel's dynamic task queue ends with short tasks
+  auto cost = [&](int i) {
+    const double np = padded_order(cols[i].desc.num_quadrature);
+    return (double)cols[i].desc.num_layers * np * np * np;
+  };
+  auto by_cost = [&](int a, int b) { return cost(a) > cost(b); };
+  std::stable_sort(small.begin(), small.end(), by_cost);
+  std::stable_sort(large.begin(), large.end(), by_cost);
   std::lock_guard<std::mutex> lk(e->mu);
   if ((rc = set_device(e))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
   e->last_stream = s;
-  std::vector<ColumnDev> h(ncols);
-  long long total = 0;
-  for (int i = 0; i < ncols; ++i) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  for (int i = 0; i < ncols; ++i)
     if ((rc = ensure_quad(e, cols[i].desc.num_quadrature, cols[i].desc.num_moments))) return rc;
-  }
-  for (int i = 0; i < ncols; ++i) {
-    h[i] = make_column(e, &cols[i].desc, &cols[i].in, &cols[i].out);
-    h[i].task_begin = total;
-    total += cols[i].desc.num_wavenumbers;
-  }
-  KernInfo k = pick(np, prec);
-  int grid;
-  size_t sb;
-  if ((rc = ensure_scratch(e, k, lmax, &grid, &sb))) return rc;
   if (e->d_cols_cap < (size_t)ncols) {
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(s, &cap);
     if (cap != cudaStreamCaptureStatusNone)
       return fail(ADRT_ERR_WORKSPACE, "column table too small during capture");
     CUDA_TRY(cudaDeviceSynchronize());
     cudaFree(e->d_cols);
+    if (e->h_cols) cudaFreeHost(e->h_cols);
     e->d_cols = nullptr;
-    if (cudaMalloc(&e->d_cols, sizeof(ColumnDev) * ncols) != cudaSuccess)
+    e->h_cols = nullptr;
+    e->d_cols_cap = 0;
+    if (cudaMalloc(&e->d_cols, sizeof(ColumnDev) * ncols) != cudaSuccess ||
+        cudaMallocHost(&e->h_cols, sizeof(ColumnDev) * ncols) != cudaSuccess)
       return fail(ADRT_ERR_OUT_OF_MEMORY, "column table allocation failed");
     e->d_cols_cap = ncols;
+    if (!e->cols_copied) CUDA_TRY(cudaEventCreateWithFlags(&e->cols_copied, cudaEventDisableTiming));
   }
-  CUDA_TRY(cudaMemcpyAsync(e->d_cols, h.data(), sizeof(ColumnDev) * ncols, cudaMemcpyHostToDevice, s));
-  CUDA_TRY(cudaStreamSynchronize(s));
-  SolveParams p{};
-  p.cols = e->d_cols;
-  p.ncols = ncols;
-  p.ntasks = total;
-  p.counter = e->counter;
-  p.status = e->status;
-  p.scratch = e->scratch;
-  p.slot_bytes = sb;
-  p.nslots = grid * k.groups;
-  p.max_layers = lmax;
-  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
-  return k.launch(p, h[0], grid, s);
+  // the previous upload must have left the pinned staging before it is rewritten
+  if (cap == cudaStreamCaptureStatusNone && e->cols_copied) CUDA_TRY(cudaEventSynchronize(e->cols_copied));
+  long long totals[2] = {0, 0};
+  int nsm = 0;
+  for (int part = 0; part < 2; ++part) {
+    const std::vector<int>& ids = part == 0 ? small : large;
+    for (int i : ids) {
+      ColumnDev c = make_column(e, &cols[i].desc, &cols[i].in, &cols[i].out);
+      c.task_begin = totals[part];
+      totals[part] += cols[i].desc.num_wavenumbers;
+      e->h_cols[nsm++] = c;
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_cols, e->h_cols, sizeof(ColumnDev) * ncols, cudaMemcpyHostToDevice, s));
+  if (e->cols_copied) CUDA_TRY(cudaEventRecord(e->cols_copied, s));
+  // columns of N <= 16: one launch of the multi-order kernel
+  if (!small.empty()) {
+    const size_t smem = 4 * kMultiGroupBytes;
+    static int bps = -1;
+    if (bps < 0) {
+      cudaFuncSetAttribute(solve_kernel_multi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, solve_kernel_multi<0>, 128, smem);
+      if (bps < 1) bps = 1;
+    }
+    const size_t sb = (SlotLayout<Geo<16, double>>::bytes(lmax_s) + 255) & ~size_t(255);
+    int blocks = bps * e->num_sms;
+    size_t need = (size_t)blocks * 4 * sb;
+    if (e->max_ws && need > e->max_ws) {
+      blocks = (int)(e->max_ws / (4 * sb));
+      if (blocks < 1) return fail(ADRT_ERR_WORKSPACE, "workspace limit below one slot (%zu B)", sb);
+      need = (size_t)blocks * 4 * sb;
+    }
+    if (need > e->scratch_bytes) {
+      if (cap != cudaStreamCaptureStatusNone)
+        return fail(ADRT_ERR_WORKSPACE, "work buffer too small during stream capture");
+      CUDA_TRY(cudaDeviceSynchronize());
+      cudaFree(e->scratch);
+      e->scratch = nullptr;
+      e->scratch_bytes = 0;
+      if (cudaMalloc(&e->scratch, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ADRT_ERR_OUT_OF_MEMORY, "work buffer allocation of %zu B failed", need);
+      }
+      e->scratch_bytes = need;
+    }
+    blocks = std::min<long long>(blocks, (long long)(e->scratch_bytes / (4 * sb)));
+    blocks = (int)std::min<long long>(blocks, (totals[0] + 3) / 4);
+    SolveParams p{};
+    p.cols = e->d_cols;
+    p.ncols = (int)small.size();
+    p.ntasks = totals[0];
+    p.counter = e->counter;
+    p.status = e->status;
+    p.scratch = e->scratch;
+    p.slot_bytes = sb;
+    p.nslots = blocks * 4;
+    p.max_layers = lmax_s;
+    CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+    solve_kernel_multi<0><<<blocks, 128, smem, s>>>(p);
+    CUDA_TRY(cudaGetLastError());
+  }
+  // columns of N > 16: one launch of the N = 32 kernel (per-column precision)
+  if (!large.empty()) {
+    KernInfo k = pick(32, any_mixed_l ? ADRT_PRECISION_MIXED : ADRT_PRECISION_FP64);
+    int grid;
+    size_t sb;
+    if ((rc = ensure_scratch(e, k, lmax_l, &grid, &sb))) return rc;
+    SolveParams p{};
+    p.cols = e->d_cols + small.size();
+    p.ncols = (int)large.size();  // 1: the kernel takes the column from c0
+    p.ntasks = totals[1];
+    p.counter = e->counter + 1;  // its own work counter
+    p.status = e->status;
+    p.scratch = e->scratch;
+    p.slot_bytes = sb;
+    p.nslots = grid * k.groups;
+    p.max_layers = lmax_l;
+    grid = (int)std::min<long long>(grid, totals[1]);
+    CUDA_TRY(cudaMemsetAsync(e->counter + 1, 0, sizeof(unsigned long long), s));
+    ColumnDev c0 = make_column(e, &cols[large[0]].desc, &cols[large[0]].in, &cols[large[0]].out);
+    if ((rc = k.launch(p, c0, grid, s))) return rc;
+  }
+  return ADRT_OK;
 }
 
 int adrt_solve_batch_host(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* hin,

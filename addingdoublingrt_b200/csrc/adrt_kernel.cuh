@@ -1141,11 +1141,83 @@ __global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col
         wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, KIND == KIND_MIXED);
     if constexpr (KIND == KIND_FP64) {
       wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+    } else if (colp->precision == 0) {  // an FP64 column of an uneven batch
+      wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else if (!any) {
       wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else {
       wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,
                                P.max_layers, P.status);
+    }
+  }
+}
+
+// ------------------------------------------------------------- uneven batches
+// Columns of any N <= 16 (padded orders 4, 8, 16: one warp per wavenumber in
+// every case) and either precision form in ONE persistent launch: each task
+// is dispatched on its column's padded order and precision.  The group's
+// shared memory and slot are sized for the largest order.
+template <int NP>
+__device__ __noinline__ void multi_task(unsigned goff, int t, int bar, int w, char* sl, int lmax,
+                                        unsigned* status, int precision) {
+  using GD = Geo<NP, double>;
+  using GF = Geo<NP, float>;
+  using GL = GroupLayout<NP, KIND_MIXED>;
+  const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
+  const int any = wav_prologue<NP>(goff, t, bar, w, sl, lmax, status, precision != 0);
+  if (precision == 0) {
+    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, lmax, status);
+  } else if (!any) {
+    wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, lmax, status);
+  } else {
+    wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl, lmax,
+                             status);
+  }
+}
+
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t kMultiGroupBytes =
+    cmax(GroupLayout<16, KIND_MIXED>::bytes,
+         cmax(GroupLayout<8, KIND_MIXED>::bytes, GroupLayout<4, KIND_MIXED>::bytes));
+
+template <int kUnused = 0>  // a template, so only the translation units that launch it hold it
+__global__ void __launch_bounds__(128) solve_kernel_multi(SolveParams P) {
+  constexpr int G = 32;
+  const int gib = threadIdx.x / G;
+  const int t = threadIdx.x % G;
+  const int bar = 1 + gib;
+  const unsigned goff = (unsigned)(gib * kMultiGroupBytes);
+  const int slot = blockIdx.x * (blockDim.x / G) + gib;
+  char* sl = P.scratch + (size_t)slot * P.slot_bytes;
+  for (unsigned i = (unsigned)t * 4u; i < (unsigned)kMultiGroupBytes; i += (unsigned)G * 4u)
+    *sp<unsigned>(goff + i) = 0u;
+  __syncwarp();
+  ColumnDev* colp = sp<ColumnDev>(goff);
+  int cur_col = -1;
+  for (;;) {
+    unsigned long long v = 0;
+    if (t == 0) v = atomicAdd(P.counter, 1ull);
+    const long long task = (long long)__shfl_sync(0xffffffffu, v, 0);
+    if (task >= P.ntasks) break;
+    int lo = 0, hi = P.ncols - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.cols[mid].task_begin <= task) lo = mid; else hi = mid - 1;
+    }
+    if (lo != cur_col) {
+      __syncwarp();
+      if (t == 0) *colp = P.cols[lo];
+      cur_col = lo;
+    }
+    __syncwarp();
+    const int w = (int)(task - colp->task_begin);
+    const int np = colp->NP, prec = colp->precision;
+    if (np <= 4) {
+      multi_task<4>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
+    } else if (np <= 8) {
+      multi_task<8>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
+    } else {
+      multi_task<16>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
     }
   }
 }

@@ -46,6 +46,10 @@ def parse():
     p.add_argument("--no-check", action="store_true")
     p.add_argument("--only", default=None, choices=["fp64", "mixed"],
                    help="time one precision form only (profiling runs)")
+    p.add_argument("--workload", default="config2", choices=["config2", "config4", "adjoint"],
+                   help="config2: the headline line; config4: uneven batch; adjoint: config 5")
+    p.add_argument("--no-adjoint", action="store_true",
+                   help="skip the adjoint/forward timing of the headline line")
     return p.parse_args()
 
 
@@ -170,6 +174,82 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- adjoint and uneven
+def time_adjoint(eng, W=10_000, reps=3):
+    """Forward and adjoint times of config 5 (10 000 x 60, N=16, thermal + solar,
+    per-layer HG moments): gradients of TOA F_up and BOA F_down with respect to
+    delta_tau, omega, the moments and the 61 level temperatures.  Returns
+    (forward ms, adjoint ms) on the device, median of `reps`."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    b = workloads.config5(W=W)
+    di = to_device(b)
+    do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+    n = b.W * (b.L + 1)
+    cot = {"flux_up": torch.zeros(n, dtype=torch.float64, device="cuda"),
+           "flux_down": torch.zeros(n, dtype=torch.float64, device="cuda")}
+    cot["flux_up"].view(b.W, -1)[:, 0] = 1.0
+    cot["flux_down"].view(b.W, -1)[:, b.L] = 1.0
+    gr = {k: torch.zeros_like(di[k])
+          for k in ("delta_tau", "single_scat_albedo", "phase_moments", "temperature")}
+    eng.solve_device(b.desc, di, do)
+    eng.adjoint(b.desc, di, cot, gr)
+    torch.cuda.synchronize()
+    fw, ad = [], []
+    for _ in range(reps):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        eng.solve_device(b.desc, di, do)
+        e1.record()
+        eng.adjoint(b.desc, di, cot, gr)
+        e2.record()
+        torch.cuda.synchronize()
+        fw.append(e0.elapsed_time(e1))
+        ad.append(e1.elapsed_time(e2))
+    return statistics.median(fw), statistics.median(ad)
+
+
+def run_config4(args, eng):
+    """Uneven batch (config 4 columns: L ~ U{20..150}, N in {4, 8, 16}, W log-uniform
+    256..8192, solar / thermal / both, mixed precision), the first columns up to
+    --wavenumbers wavenumber-columns: one launch of the persistent multi-order
+    kernel against one launch per column (the reference's pattern of a
+    solveBatch call per column)."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    cols = workloads.config4_columns(ncols=4096, seed=4, max_total=args.wavenumbers)
+    dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in cols]
+    total = sum(c.W for c in cols)
+    for _ in range(args.warmup):
+        eng.solve_uneven(dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        eng.solve_uneven(dev)
+    e1.record()
+    torch.cuda.synchronize()
+    one = e0.elapsed_time(e1) / args.steps
+    for d, di, do in dev:
+        eng.solve_device(d, di, do)
+    torch.cuda.synchronize()
+    e0.record()
+    for d, di, do in dev:
+        eng.solve_device(d, di, do)
+    e1.record()
+    torch.cuda.synchronize()
+    per_col = e0.elapsed_time(e1)
+    line = {"metric": "wavenumber-solves/s, uneven batch (config 4)", "value": total / (one * 1e-3),
+            "unit": "wavenumber-solves/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": one, "higher_is_better": True,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"config4: first {len(cols)} columns, {total} wavenumber-"
+                                   "columns, N in {4,8,16}, L 20..150, mixed precision"},
+            "one_launch_ms": one, "launch_per_column_ms": per_col,
+            "speedup_vs_launch_per_column": per_col / one, "status": eng.read_status()}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- engine arm
 def main():
     args = parse()
@@ -191,6 +271,15 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     eng = Engine(device=local)
+    if args.workload == "config4":
+        return run_config4(args, eng)
+    if args.workload == "adjoint":
+        fw, ad = time_adjoint(eng)
+        print(json.dumps({"metric": "adjoint time / forward time, config 5", "value": ad / fw,
+                          "unit": "ratio", "higher_is_better": False, "forward_ms": fw,
+                          "adjoint_ms": ad, "config": {"workload": "config5: W=10000 x L=60, "
+                                                       "N=16, thermal + solar, FP64"}}))
+        return
     results = {}
     precisions = [args.only] if args.only else ["fp64", "mixed"]
     for pname in precisions:
@@ -269,6 +358,10 @@ def main():
     h2d = int(sum(v.nbytes for v in hb.arrays.values()))
     d2h = int(sum(v.nbytes for v in hout.values()))
 
+    adj = {}
+    if not args.no_adjoint:
+        fw, ad = time_adjoint(eng)
+        adj = {"adjoint_over_forward": ad / fw, "adjoint_config5_ms": ad, "forward_config5_ms": fw}
     if rank == 0:
         from oracle import oracle
         fl = oracle.flops(b)  # algorithmic flops of the whole batch
@@ -276,9 +369,17 @@ def main():
         peaks = measured_peaks(_lib.load())
         pk = peaks["fp64_tflops"] if pname == "fp64" else peaks["fp32_tflops"]
         achieved = fl / (ms * 1e-3) / 1e12
+        traffic = None
+        try:
+            tj = json.load(open(os.path.join(ROOT, "profiles", "solve_kernel_traffic.json")))
+            traffic = tj[f"{pname}_bytes_per_wavenumber"] * args.wavenumbers
+        except Exception:
+            pass
         roof = {"bound": "fp64" if pname == "fp64" else "fp32", "achieved": achieved,
                 "peak": pk, "unit": "TFLOP/s", "frac": achieved / pk if pk else None,
-                "traffic": None, "peak_source": peaks["source"],
+                "traffic": traffic, "traffic_note": "ncu, scaled per wavenumber from a "
+                "4000-wavenumber capture (profiles/solve_kernel_traffic.json)",
+                "peak_source": peaks["source"] + " (of measured)",
                 "flops_per_launch": fl}
         line = {
             "metric": METRIC,
@@ -301,6 +402,7 @@ def main():
             "e2e": {"value": args.wavenumbers * world / e2e_s, "unit": "wavenumber-solves/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
+            **adj,
             "clocks": results[pname]["clocks"],
             "device_status": {p: results[p]["status"] for p in precisions},
         }

@@ -248,6 +248,7 @@ typedef struct adrt_gradients {
   double* phase_moments;
   double* temperature;
   double* planck_levels;
+  double* surface_emission; /* [W], overwritten; raw-source (non-thermal) batches only */
 } adrt_gradients;
 
 /* Reverse-mode adjoint of the batched solve: given the loss cotangents,

@@ -253,20 +253,21 @@ def test_bad_values_set_the_device_status_flag(eng):
 
 
 def test_uneven_batch_equals_separate_solves(eng):
+    """Columns of different W, L, N (4, 8, 16, 32) and precision in one call give
+    exactly the results of solving each column on its own."""
     import torch
     from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
-    cols = workloads.config4_columns(ncols=12, seed=4)
-    cols = [c for c in cols if c.N in (8, 16)][:6]
-    for c in cols:
-        c.desc.precision = _abi.PRECISION_FP64
-    groups = {}
-    for c in cols:
-        groups.setdefault(8 if c.N <= 8 else 16, []).append(c)
-    for np_, grp in groups.items():
-        dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in grp]
-        eng.solve_uneven(dev)
-        torch.cuda.synchronize()
-        for c, (_, _, do) in zip(grp, dev):
-            single = run_device(eng, c, _abi.INTERFACE_OUTPUTS)
-            for k in _abi.INTERFACE_OUTPUTS:
-                assert np.array_equal(do[k].cpu().numpy(), single[k]), k
+    cols = [c.subset(np.arange(min(c.W, 200))) for c in workloads.config4_columns(ncols=12, seed=4)]
+    extra = workloads.random_small(77, N=32, L=5, W=3, use_delta_m=0)
+    cols.append(extra)
+    for i, c in enumerate(cols):
+        c.desc.precision = _abi.PRECISION_FP64 if i % 2 else _abi.PRECISION_MIXED
+    assert {c.N for c in cols} >= {4, 8, 16, 32}
+    dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in cols]
+    eng.solve_uneven(dev)
+    torch.cuda.synchronize()
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_BAD_INPUT) == 0
+    for c, (_, _, do) in zip(cols, dev):
+        single = run_device(eng, c, _abi.INTERFACE_OUTPUTS)
+        for k in _abi.INTERFACE_OUTPUTS:
+            assert np.array_equal(do[k].cpu().numpy(), single[k]), (c.N, c.desc.precision, k)
