@@ -76,7 +76,8 @@ def test_solve_batch_forward_and_gradients():
         grad = t[k].grad.detach().cpu().numpy()
         for _ in range(4):
             idx = tuple(int(rng.integers(0, s)) for s in arr.shape)
-            h = 1e-5 * max(abs(arr[idx]), 1e-2)
+            # steps well above the scheme's own FP64 round-off (~1e-12 relative)
+            h = 1e-4 * max(abs(arr[idx]), 0.05)
             ap, am = arr.copy(), arr.copy()
             ap[idx] += h
             am[idx] -= h
@@ -84,4 +85,4 @@ def test_solve_batch_forward_and_gradients():
             args_m = [tau, ssa, mom, planck]
             args_p[k], args_m[k] = ap, am
             fdv = (L(*args_p) - L(*args_m)) / (2 * h)
-            assert abs(grad[idx] - fdv) <= 1e-5 * max(1.0, abs(fdv)), (k, idx, grad[idx], fdv)
+            assert abs(grad[idx] - fdv) <= 2e-6 * max(1.0, abs(fdv)), (k, idx, grad[idx], fdv)
