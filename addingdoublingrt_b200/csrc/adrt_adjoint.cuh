@@ -182,9 +182,17 @@ struct AdjSlot {
   }
 };
 
+// The adjoint holds 25 matrices per wavenumber, so few groups fit on an SM;
+// at NP = 16 a group is four warps (one 8x8 product tile each) so that the SM
+// still runs as many warps as the forward kernel.
+template <int NP>
+constexpr int adjoint_group() { return (NP == 16) ? 128 : default_group<NP>(); }
+template <int NP>
+using AdjGeo = Geo<NP, double, adjoint_group<NP>()>;
+
 template <int NP>
 struct AdjGroup {
-  using GD = Geo<NP, double>;
+  using GD = AdjGeo<NP>;
   static constexpr size_t bytes =
       align16(CommonLayout<NP>::bytes + TypedLayout<GD, kMatsAdj>::bytes);
 };
@@ -584,7 +592,7 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
 template <int NP>
 __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int bar, int w,
                                          char* slot, int lmax, unsigned* status, AdjDev AD) {
-  using Gm = Geo<NP, double>;
+  using Gm = AdjGeo<NP>;
   using Real = double;
   using SLay = SlotLayout<Gm>;
   using AS = AdjSlot<Gm>;
@@ -1047,7 +1055,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
 // ---------------------------------------------------------------- kernel
 template <int NP>
 struct AdjKern {
-  using GD = Geo<NP, double>;
+  using GD = AdjGeo<NP>;
   static constexpr size_t kMaxSmem = 227 * 1024;
   static constexpr int G = GD::G;
   static constexpr int kGroups =
@@ -1058,8 +1066,8 @@ struct AdjKern {
 };
 
 template <int NP>
-__global__ void __launch_bounds__(128) adjoint_kernel(SolveParams P, ColumnDev col0, AdjDev AD) {
-  using GD = Geo<NP, double>;
+__global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolveParams P, ColumnDev col0, AdjDev AD) {
+  using GD = AdjGeo<NP>;
   constexpr int G = GD::G;
   const int gib = threadIdx.x / G;
   const int t = threadIdx.x % G;
@@ -1088,7 +1096,7 @@ __global__ void __launch_bounds__(128) adjoint_kernel(SolveParams P, ColumnDev c
     if (task >= P.ntasks) break;
     const int w = (int)task;
     gsync<G>(bar);
-    wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, 0);
+    wav_prologue<NP, adjoint_group<NP>()>(goff, t, bar, w, sl, P.max_layers, P.status, 0);
     double* iv = reinterpret_cast<double*>(sl + AdjSlot<GD>::fwd(P.max_layers));
     wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status, iv);
     wav_adjoint<NP>(goff, tb, t, bar, w, sl, P.max_layers, P.status, AD);

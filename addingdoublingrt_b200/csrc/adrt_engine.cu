@@ -652,7 +652,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   } k{};
   auto make = [&](auto tag) {
     constexpr int NP = decltype(tag)::value;
-    using GD = Geo<NP, double>;
+    using GD = AdjGeo<NP>;
     k.groups = AdjKern<NP>::kGroups;
     k.threads = AdjKern<NP>::kThreads;
     k.smem = (size_t)k.groups * AdjGroup<NP>::bytes;

@@ -581,7 +581,7 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
                                               double F0, double mu0, const double* Ppp,
                                               const double* Ppm, int* singular,
                                               double* src64) {
-  using GmF = Geo<GmD::NP, float>;
+  using GmF = Geo<GmD::NP, float, GmD::G>;
   constexpr int TR = GmD::TR, TC = GmD::TC, NP = GmD::NP;
   static_assert(GmF::TR == TR && GmF::TC == TC && GmF::G == GmD::G, "tile maps must agree");
   const int tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0,
@@ -659,10 +659,10 @@ __device__ __forceinline__ void emit_interface(const Ctx<Gm>& X, const ColumnDev
 // (src/solver.cpp:385-514), cumulative scaled tau and the boundary sources;
 // with `mixed`, also the per-layer FP64 flags of the mixed form.  Returns
 // (group-uniform) whether any layer is flagged.
-template <int NP>
+template <int NP, int GS = default_group<NP>()>
 __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, char* slot,
                                          int lmax, unsigned* status, int mixed) {
-  using Gm = Geo<NP, double>;
+  using Gm = Geo<NP, double, GS>;
   constexpr int G = Gm::G;
   const Ctx<Gm> X(goff, goff, t_, bar);  // common prefix only
   const ColumnDev* C = X.col;
@@ -1090,7 +1090,7 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
 
 // ------------------------------------------------------------- persistent kernel
 template <int NP, int KIND>
-__global__ void __launch_bounds__(128) solve_kernel(SolveParams P, ColumnDev col0) {
+__global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev col0) {
   using GD = Geo<NP, double>;
   using GF = Geo<NP, float>;
   using GL = GroupLayout<NP, KIND>;

@@ -58,11 +58,16 @@ __device__ __forceinline__ unsigned soff(const void* p) {
 }
 
 // ============================================================== geometry
-template <int NP_, typename Real_>
+// Threads that solve one wavenumber: a warp up to NP = 16, four warps at 32.
+template <int NP>
+constexpr int default_group() { return (NP <= 16) ? 32 : 128; }
+
+template <int NP_, typename Real_, int G_ = default_group<NP_>()>
 struct Geo {
   static constexpr int NP = NP_;
   using Real = Real_;
-  static constexpr int G = (NP <= 16) ? 32 : 128;  // threads per wavenumber
+  static constexpr int G = G_;  // threads per wavenumber (32, 64 or 128)
+  static_assert(G == 32 || G == 64 || G == 128, "group of one, two or four warps");
   static constexpr int RB = (G == 32) ? 4 : 8;      // thread-grid rows
   static constexpr int CB = G / RB;                 // thread-grid cols
   static constexpr int TR = (NP + RB - 1) / RB;     // tile rows per thread
@@ -246,7 +251,8 @@ struct Tile {
 template <class Gm>
 struct UseMMA {
   static constexpr bool value =
-      ADRT_GEMM_MMA && sizeof(typename Gm::Real) == 8 && Gm::NP >= 8;
+      ADRT_GEMM_MMA && sizeof(typename Gm::Real) == 8 && Gm::NP >= 8 &&
+      (Gm::NP / 8) * (Gm::NP / 8) >= Gm::G / 32;  // at least one 8x8 tile per warp
 };
 
 __device__ __forceinline__ void mma_f64_m8n8k4(double& d0, double& d1, double a, double b) {
@@ -261,9 +267,10 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
                                          double* out_cm, int t) {
   constexpr int NP = Gm::NP, LD = Gm::LD;
   constexpr int NT = NP / 8;
-  constexpr int WR = (NT >= 2) ? 2 : 1, WC = WR;
+  constexpr int TPW = NT * NT / (Gm::G / 32);  // 8x8 output tiles per warp
+  constexpr int WR = (TPW >= 4) ? 2 : 1, WC = (TPW >= 2) ? 2 : 1;
   constexpr int WPC = NT / WC;  // warps per tile-row band
-  static_assert((NT / WR) * WPC == Gm::G / 32, "warp grid must cover the tiles");
+  static_assert(TPW >= 1 && (NT / WR) * WPC == Gm::G / 32, "warp grid must cover the tiles");
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
   const int r0 = (warp / WPC) * WR * 8, c0 = (warp % WPC) * WC * 8;
   double acc[WR][WC][2];
@@ -448,6 +455,160 @@ __device__ __noinline__ void op_gemm_lam(unsigned xt_off, unsigned y_off, unsign
   }
 }
 
+// FP64 right-solve X = B A^{-1} on the tensor cores, without pivoting.
+//
+// Every matrix the solver inverts is I - R R' with R, R' reflection matrices
+// (non-negative, row sums <= 1): I - R^2 in the doubling, I - R_b R in the
+// adding, (I - R R_b)^T at the interfaces and their transposes in the adjoint.
+// Such a matrix is diagonally dominant by rows (or, transposed, by columns),
+// so elimination without pivoting is backward stable, and partial pivoting
+// -- the reference's LU of A^T (src/matrix.hpp:120-124) -- would choose the
+// diagonal at every step.
+//
+// The stacked matrix M = [A; B] (2NP x NP) lives in m8n8k4 accumulator
+// fragments.  Columns are eliminated four at a time: for the panel of pivot
+// rows/columns 4j..4j+3 with 4x4 pivot block P, the panel columns become
+// M[:, panel] P^{-1} (each row's four entries times P^{-1}, computed from the
+// published pivot rows by every thread) and every other column c becomes
+// M[:, c] - (M[:, panel] P^{-1}) M[pivot rows, c], one k = 4 DMMA per 8x8
+// tile.  After NP/4 panels the A part is I and the B part is B A^{-1}.
+// lbuf (8 NP doubles) and rbuf (4 (NP + 4) doubles) are scratch.
+#ifndef ADRT_GJ_MMA
+#define ADRT_GJ_MMA 1
+#endif
+
+template <class Gm>
+struct UseGjMMA {
+  static constexpr int NP = Gm::NP, NW = Gm::G / 32;
+  static constexpr bool value = ADRT_GJ_MMA && sizeof(typename Gm::Real) == 8 && NP >= 8 &&
+                                2 * NP <= Gm::G &&  // one thread per row of [A; B]
+                                ((2 * NP / 8) * (NP / 8)) % NW == 0;
+};
+
+template <class Gm>
+__device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, const double* bvec,
+                                      double* out_cm, double* out_rm, double* lbuf, double* rbuf,
+                                      int t, int bar) {
+  constexpr int NP = Gm::NP, LD = Gm::LD, G = Gm::G, NW = G / 32;
+  constexpr int NTR = 2 * NP / 8, NTC = NP / 8, TPW = NTR * NTC / NW;
+  constexpr int RS = NP + 4;  // rbuf row stride (conflict-free B-fragment loads)
+  constexpr int NROW = 2 * NP;
+  const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+  double acc[TPW][2];
+#pragma unroll
+  for (int u = 0; u < TPW; ++u) {
+    const int tau = warp * TPW + u, i = tau / NTC, jt = tau % NTC;
+    const int r = 8 * i + g, c = 8 * jt + 2 * q;
+    double2 v;
+    if (r < NP) {
+      v = *reinterpret_cast<const double2*>(A_rm + r * LD + c);
+    } else if (B_rm) {
+      v = *reinterpret_cast<const double2*>(B_rm + (r - NP) * LD + c);
+    } else {
+      v = (r == NP) ? make_double2(bvec[c], bvec[c + 1]) : make_double2(0.0, 0.0);
+    }
+    acc[u][0] = v.x;
+    acc[u][1] = v.y;
+  }
+  int singular = 0;
+#pragma unroll
+  for (int j = 0; j < NP / 4; ++j) {
+    const int pt = j >> 1, half = j & 1;  // tile row/column holding the panel, and which half
+    // 1. publish the panel columns (lbuf, 2NP x 4) and the pivot rows (rbuf, 4 x NP)
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+      const int tau = warp * TPW + u, i = tau / NTC, jt = tau % NTC;
+      if (jt == pt && (q >> 1) == half)
+        *reinterpret_cast<double2*>(lbuf + (8 * i + g) * 4 + 2 * (q & 1)) =
+            make_double2(acc[u][0], acc[u][1]);
+      if (i == pt && (g >> 2) == half)
+        *reinterpret_cast<double2*>(rbuf + (g & 3) * RS + 8 * jt + 2 * q) =
+            make_double2(acc[u][0], acc[u][1]);
+    }
+    gsync<G>(bar);
+    // 2. row t of the panel times P^{-1} (every thread reduces P, so the
+    //    singular flag is group-uniform; rows < 2NP are stored)
+    {
+      double P[4][4], x[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const double2 p0 = *reinterpret_cast<const double2*>(rbuf + a * RS + 4 * j);
+        const double2 p1 = *reinterpret_cast<const double2*>(rbuf + a * RS + 4 * j + 2);
+        P[a][0] = p0.x;
+        P[a][1] = p0.y;
+        P[a][2] = p1.x;
+        P[a][3] = p1.y;
+      }
+      if (t < NROW) {
+        const double2 x0 = *reinterpret_cast<const double2*>(lbuf + t * 4);
+        const double2 x1 = *reinterpret_cast<const double2*>(lbuf + t * 4 + 2);
+        x[0] = x0.x;
+        x[1] = x0.y;
+        x[2] = x1.x;
+        x[3] = x1.y;
+      } else {
+        x[0] = x[1] = x[2] = x[3] = 0.0;
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+        const double piv = P[s][s];
+        singular |= (piv == 0.0);
+        const double inv = recip(piv);
+        const double fx = x[s] * inv;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c != s) x[c] = fma(-fx, P[s][c], x[c]);
+        x[s] = fx;
+#pragma unroll
+        for (int s2 = s + 1; s2 < 4; ++s2) {
+          const double f = P[s2][s] * inv;
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            if (c != s) P[s2][c] = fma(-f, P[s][c], P[s2][c]);
+          P[s2][s] = f;
+        }
+      }
+      const int pr = t - 4 * j;  // pivot rows take the exact unit rows
+      if (pr >= 0 && pr < 4) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) x[c] = (c == pr) ? 1.0 : 0.0;
+      }
+      if (t < NROW) {  // each thread reads and writes only its own row
+        *reinterpret_cast<double2*>(lbuf + t * 4) = make_double2(x[0], x[1]);
+        *reinterpret_cast<double2*>(lbuf + t * 4 + 2) = make_double2(x[2], x[3]);
+      }
+    }
+    gsync<G>(bar);
+    // 3. rank-4 update of every tile, then the panel columns take their new values
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+      const int tau = warp * TPW + u, i = tau / NTC, jt = tau % NTC;
+      const double a = -lbuf[(8 * i + g) * 4 + q];
+      const double b = rbuf[q * RS + 8 * jt + g];
+      mma_f64_m8n8k4(acc[u][0], acc[u][1], a, b);
+      if (jt == pt && (q >> 1) == half) {
+        const double2 l = *reinterpret_cast<const double2*>(lbuf + (8 * i + g) * 4 + 2 * (q & 1));
+        acc[u][0] = l.x;
+        acc[u][1] = l.y;
+      }
+    }
+    gsync<G>(bar);  // the next panel overwrites lbuf / rbuf
+  }
+#pragma unroll
+  for (int u = 0; u < TPW; ++u) {
+    const int tau = warp * TPW + u, i = tau / NTC, jt = tau % NTC;
+    const int r = 8 * i + g - NP, c = 8 * jt + 2 * q;
+    if (r >= 0) {
+      if (out_rm) *reinterpret_cast<double2*>(out_rm + r * LD + c) = make_double2(acc[u][0], acc[u][1]);
+      if (out_cm) {
+        out_cm[c * LD + r] = acc[u][0];
+        out_cm[(c + 1) * LD + r] = acc[u][1];
+      }
+    }
+  }
+  return singular;
+}
+
 // X = B A^{-1} by Gauss-Jordan column elimination, with column pivoting on
 // the largest |entry| of the pivot row -- the pivot rule of the LU with
 // partial pivoting of A^T that the reference's right-solve performs
@@ -467,6 +628,12 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
   unsigned* red = sp<unsigned>(red_off);
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP, DIM = Gm::DIM;
   constexpr int G = Gm::G;
+  if constexpr (UseGjMMA<Gm>::value) {
+    static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
+    Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+    Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
+    return gj_mma<Gm>(A_rm, B_rm, bvec, o_cm, out_rm, o_cm ? o_cm : out_rm, gjbuf, t, bar);
+  }
   const Tile<Gm> tl(t);
   const bool tv = tl.valid();
   Real A[TR][TC], B[TR][TC];

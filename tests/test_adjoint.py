@@ -118,7 +118,7 @@ def rel_err(ad, fd):
     return float(np.max(np.abs(ad[m] - fd[m])) / np.max(np.abs(fd[m])))
 
 
-@pytest.mark.parametrize("N", [4, 8, 16])
+@pytest.mark.parametrize("N", [4, 8, 16, 32])
 def test_adjoint_tau_and_omega_match_finite_differences(eng, N):
     b = small_batch(11 + N, N)
     rng = np.random.default_rng(N)
