@@ -147,6 +147,17 @@ enum AdjMat {
   J_bT1, J_bT1c, J_bTGR, J_bTGRc, J_bTG, J_W, J_C, J_Cc, J_T1, J_T2, J_VEC,
   kMatsAdj = J_VEC + 2  // J_VEC spans two buffers (18 vectors even at NP = 8)
 };
+// Doubling steps per layer budgeted for the forward's record of the chains.
+// nn = trunc(log2 tau) + 4 / 10 / 16, so 24 covers tau up to 256 for any omega;
+// the record is one pool per wavenumber, so thin layers leave room for thick
+// ones, and layers beyond it are recomputed in the adjoint.
+constexpr int kTapeStepsPerLayer = 24;
+
+// A recomputing (taping) doubling runs while the layer cotangents sit in
+// J_bR0..J_bT0c; its extra buffers are the adjoint step's scratch J_W, J_C, J_Cc.
+static_assert(kTapeBufTc0 == J_W && kTapeBufTc1 == J_C && kTapeBufAinv == J_Cc &&
+                  kTapeBufTc0 > J_bT0c,
+              "taping doubling buffers must not hold live cotangents");
 // Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 20 NP).
 enum AdjVec {
   A_BY = 0, A_BZ, A_BSU, A_BSD, A_H, A_RU, A_RD, A_BRU, A_BRD, A_BH, A_Y, A_Z, A_SU, A_SD,
@@ -155,8 +166,10 @@ enum AdjVec {
 };
 
 // Adjoint slot in HBM: the forward slot (levels, phase, records), the
-// interface intensities, the downward-pass vectors, the doubling record and
-// the layout-1 phase-cotangent accumulators.
+// interface intensities, the downward-pass vectors, one layer's doubling
+// record (for layers recomputed in the adjoint), the layout-1 phase-cotangent
+// accumulators, the per-layer tape offsets, then (bytes() onwards) the
+// forward's record of every layer's doubling, tape_cap doubles.
 template <class Gm>
 struct AdjSlot {
   using SL = SlotLayout<Gm>;
@@ -168,7 +181,10 @@ struct AdjSlot {
   }
   static __host__ __device__ size_t dvec(int lmax) { return ivec(lmax); }
   static __host__ __device__ size_t tape() {
-    return ((size_t)kMaxDoublings * Tp::STEP * sizeof(double) + 255) & ~size_t(255);
+    return ((size_t)Tp::layer(kMaxDoublings) * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t toff(int lmax) {
+    return ((size_t)lmax * sizeof(long long) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t pacc() {
     return ((size_t)2 * NP * NP * sizeof(double) + 2 * NP * sizeof(double) + 255) & ~size_t(255);
@@ -178,6 +194,10 @@ struct AdjSlot {
     return ((size_t)4 * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t bytes(int lmax) {
+    return toff_at(lmax) + toff(lmax);
+  }
+  // byte offset of the per-layer tape offsets (after the 256-byte scalar block)
+  static __host__ __device__ size_t toff_at(int lmax) {
     return fwd(lmax) + ivec(lmax) + dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256;
   }
 };
@@ -201,6 +221,7 @@ struct AdjGroup {
 struct AdjDev {
   const double *c_fu, *c_fd, *c_J, *c_fdir;  // [W*(L+1)] each, or null
   double *g_tau, *g_ssa, *g_mom, *g_temp, *g_planck, *g_semis;
+  long long tape_cap;  // doubles per slot for the forward's record of the doubling chains
 };
 
 // ---------------------------------------------------------------- doubling adjoint
@@ -215,7 +236,8 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
                                               double tau, double om, double Bt, double Bb,
                                               double tcum, int N, bool solar, double F0,
                                               double mu0, const double* Ppp, const double* Ppm,
-                                              double* tape, double* out, int* singular) {
+                                              double* tape, bool recompute, double* out,
+                                              int* singular) {
   using Real = typename Gm::Real;
   static_assert(sizeof(Real) == 8, "the adjoint runs in FP64");
   using Tp = TapeLayout<Gm>;
@@ -223,12 +245,12 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, G = Gm::G;
   const int t = X.t;
   double* red = reinterpret_cast<double*>(X.gjbuf) + 4;  // 4 doubles of reduction scratch
-  // 1. forward chain of this layer again, recorded (uses buffers 0..5 and V_*)
+  // 1. the record of this layer's chain: taped by the forward pass, or the
+  //    chain again now (buffers 0..5, the kTapeBuf* buffers and V_*)
   const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
-  const int tcur =
-      doubling<Gm>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
-                   singular, tape);
-  (void)tcur;
+  if (recompute)
+    doubling<Gm>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm, singular,
+                 tape);
   X.sync();
   const double* mu = X.DV(D_MU);
   const double* wt = X.DV(D_WT);
@@ -245,14 +267,12 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   (void)yF;
   double pBbar = 0.0, pBd = 0.0;
   {
-    // final y, z of the chain are the inputs of "step nn": rebuild them from the
-    // last record step (recompute one vector update is avoided by reading the
-    // forward's final vectors still in V_Y/V_Z of the FP64 view)
-    const int par = nn & 1;
+    // final y, z of the chain: the tape's tail
+    const double* tail = tape + (size_t)nn * Tp::STEP;
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
       const double bu = VA(A_BUP)[i], bd = VA(A_BDN)[i];
-      const double y = X.V(V_Y0 + par)[i], z = X.V(V_Z0 + par)[i];
+      const double y = tail[i], z = tail[NP + i];
       VA(A_BY)[i] = (bu + bd) * Bbar;
       VA(A_BZ)[i] = (bu - bd) * Bd;
       VA(A_BSU)[i] = bu;
@@ -270,24 +290,24 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   for (int k = nn - 1; k >= 0; --k) {
     const double* tk = tape + (size_t)k * Tp::STEP;
     const double g = ldexp(tau0, k - 1);
-    const double gam = tk[3 * Tp::TILE + 4 * NP];
+    const double gam = tk[Tp::OFF_VEC + 4 * NP];
     const unsigned bRr = X.mo(cs ? J_bR1 : J_bR0), bRc = X.mo(cs ? J_bR1c : J_bR0c);
     const unsigned bTr = X.mo(cs ? J_bT1 : J_bT0), bTc = X.mo(cs ? J_bT1c : J_bT0c);
     const unsigned nRr = X.mo(cs ? J_bR0 : J_bR1), nRc = X.mo(cs ? J_bR0c : J_bR1c);
     const unsigned nTr = X.mo(cs ? J_bT0 : J_bT1), nTc = X.mo(cs ? J_bT0c : J_bT1c);
     X.sync();
-    op_g2s<Gm>(tk, X.mo(J_R), X.mo(J_Rc), t);
-    op_g2s<Gm>(tk + Tp::TILE, kNoMat, X.mo(J_Tc), t);
-    op_g2s<Gm>(tk + 2 * Tp::TILE, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
+    op_g2s<Gm>(tk + Tp::OFF_R, X.mo(J_R), X.mo(J_Rc), t);
+    op_g2s<Gm>(tk + Tp::OFF_T, kNoMat, X.mo(J_Tc), t);
+    op_g2s<Gm>(tk + Tp::OFF_TG, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
+    op_g2s<Gm>(tk + Tp::OFF_AI, kNoMat, X.mo(J_Ac), t);       // (I - R R)^{-1} (cm)
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
-      VA(A_Y)[i] = tk[3 * Tp::TILE + i];
-      VA(A_Z)[i] = tk[3 * Tp::TILE + NP + i];
-      VA(A_SU)[i] = tk[3 * Tp::TILE + 2 * NP + i];
-      VA(A_SD)[i] = tk[3 * Tp::TILE + 3 * NP + i];
+      VA(A_Y)[i] = tk[Tp::OFF_VEC + i];
+      VA(A_Z)[i] = tk[Tp::OFF_VEC + NP + i];
+      VA(A_SU)[i] = tk[Tp::OFF_VEC + 2 * NP + i];
+      VA(A_SD)[i] = tk[Tp::OFF_VEC + 3 * NP + i];
     }
     X.sync();
-    op_gemm<Gm>(X.mo(J_Rc), X.mo(J_R), kNoMat, 1, kNoMat, X.mo(J_Ac), t);  // A = I - R R (cm)
     op_gemm<Gm>(X.mo(J_TGc), X.mo(J_R), kNoMat, 0, X.mo(J_TGR), kNoMat, t);  // TGR = TG R
     if (X.warp == 0) {  // h = z + g y, ru = R sd + gam su, rd = gam R su + sd
       const Real* vv[2] = {VA(A_SD), VA(A_SU)};
@@ -309,14 +329,14 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
                 kNoMat, kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
     X.sync();
     // dTG = dT T^T + dTGR R^T + bz h^T + by y^T + bsu ru^T + bsd rd^T
-    op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Rc), X.mo(J_T1), 0, X.mo(J_bTG), kNoMat, t);
+    //   (kept column-major in J_bTG)
+    op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Rc), X.mo(J_T1), 0, kNoMat, X.mo(J_bTG), t);
     X.sync();
-    op_rank<Gm>(X.mo(J_bTG), kNoMat, vo(A_BZ), vo(A_H), 1.0, vo(A_BY), vo(A_Y), 1.0, vo(A_BSU),
+    op_rank<Gm>(kNoMat, X.mo(J_bTG), vo(A_BZ), vo(A_H), 1.0, vo(A_BY), vo(A_Y), 1.0, vo(A_BSU),
                 vo(A_RU), 1.0, vo(A_BSD), vo(A_RD), 1.0, t);
     X.sync();
-    // W = dTG A^{-T}   (Gauss-Jordan on A^T = the column-major buffer of A)
-    *singular |= op_gj<Gm>(X.mo(J_Ac), X.mo(J_bTG), kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
-                           X.mo(J_W));
+    // W = dTG A^{-T} = dTG ((I - R R)^{-1})^T
+    op_gemm<Gm>(X.mo(J_bTG), X.mo(J_Ac), kNoMat, 0, X.mo(J_W), kNoMat, t);
     X.sync();
     // C = TG^T W  (= -dA);  dT' = TG^T dT + W + TGR^T dR
     op_gemm<Gm>(X.mo(J_TG), X.mo(J_W), kNoMat, 0, X.mo(J_C), X.mo(J_Cc), t);
@@ -620,6 +640,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   double* brb = reinterpret_cast<double*>(p += AS::pacc());       // carried d R_base (tiles)
   double* acc = reinterpret_cast<double*>(p += AS::brb());        // bB, btc, dtau, dom
   double* scal = reinterpret_cast<double*>(p += AS::acc(lmax));   // 32 doubles
+  const long long* toff = reinterpret_cast<const long long*>(slot + AS::toff_at(lmax));
+  double* tape_all = reinterpret_cast<double*>(slot + AS::bytes(lmax));
   double* bB = acc;
   double* btc = acc + (lmax + 1);
   double* gtau = acc + 2 * (lmax + 1);
@@ -915,8 +937,9 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       nuse_l1 = nuse;
       if (layout != 1)
         build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+      const long long to = toff[l];
       doubling_adjoint<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
-                           Ppp, Ppm, tape, scal, &singular);
+                           Ppp, Ppm, to >= 0 ? tape_all + to : tape, to < 0, scal, &singular);
       if (t == 0) {
         gtau[l] += scal[0];
         gom[l] += scal[1];
@@ -1098,7 +1121,10 @@ __global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolvePar
     gsync<G>(bar);
     wav_prologue<NP, adjoint_group<NP>()>(goff, t, bar, w, sl, P.max_layers, P.status, 0);
     double* iv = reinterpret_cast<double*>(sl + AdjSlot<GD>::fwd(P.max_layers));
-    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status, iv);
+    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status, iv,
+                            reinterpret_cast<double*>(sl + AdjSlot<GD>::bytes(P.max_layers)),
+                            AD.tape_cap,
+                            reinterpret_cast<long long*>(sl + AdjSlot<GD>::toff_at(P.max_layers)));
     wav_adjoint<NP>(goff, tb, t, bar, w, sl, P.max_layers, P.status, AD);
   }
 }

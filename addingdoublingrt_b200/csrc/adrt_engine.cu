@@ -646,7 +646,8 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   const int np = padded_order(d->num_quadrature);
   struct AK {
     int groups, threads;
-    size_t smem, slot;
+    size_t smem, slot, base;
+    long long tape_cap;
     const void* fn;
     void (*launch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
   } k{};
@@ -656,7 +657,9 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
     k.groups = AdjKern<NP>::kGroups;
     k.threads = AdjKern<NP>::kThreads;
     k.smem = (size_t)k.groups * AdjGroup<NP>::bytes;
-    k.slot = (AdjSlot<GD>::bytes(d->num_layers) + 255) & ~size_t(255);
+    k.base = (AdjSlot<GD>::bytes(d->num_layers) + 255) & ~size_t(255);
+    k.tape_cap = (long long)d->num_layers * TapeLayout<GD>::layer(kTapeStepsPerLayer);
+    k.slot = k.base + (((size_t)k.tape_cap * sizeof(double) + 255) & ~size_t(255));
     k.fn = reinterpret_cast<const void*>(adjoint_kernel<NP>);
     k.launch = [](const SolveParams& p, const ColumnDev& c, const AdjDev& a, int grid, size_t smem,
                   cudaStream_t st) {
@@ -678,8 +681,18 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   grid = std::min(grid, need_blocks);
   size_t need = (size_t)grid * k.groups * k.slot;
   if (e->max_ws && need > e->max_ws) {
-    grid = (int)(e->max_ws / ((size_t)k.groups * k.slot));
-    if (grid < 1) return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint slot (%zu B)", k.slot);
+    // a shorter tape first (layers beyond it are recomputed), then fewer groups
+    const size_t per = e->max_ws / ((size_t)grid * k.groups);
+    if (per >= k.base) {
+      k.tape_cap = (long long)((per - k.base) / sizeof(double)) & ~31ll;
+      k.slot = k.base + (size_t)k.tape_cap * sizeof(double);
+    } else {
+      k.tape_cap = 0;
+      k.slot = k.base;
+      grid = (int)(e->max_ws / ((size_t)k.groups * k.slot));
+      if (grid < 1)
+        return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint slot (%zu B)", k.slot);
+    }
     need = (size_t)grid * k.groups * k.slot;
   }
   if (need > e->adj_scratch_bytes) {
@@ -719,6 +732,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   a.g_temp = gr->temperature;
   a.g_planck = gr->planck_levels;
   a.g_semis = gr->surface_emission;
+  a.tape_cap = k.tape_cap;
   CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
   k.launch(p, c0, a, grid, k.smem, s);
   CUDA_TRY(cudaGetLastError());

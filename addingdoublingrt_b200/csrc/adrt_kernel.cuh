@@ -75,13 +75,22 @@ struct SlotLayout {
 
 // One step of the adjoint's doubling record (per layer, nn steps): R, T, TG
 // tiles (TG taken from its column-major buffer, i.e. TG^T in tile order),
-// then y, z, s_up, s_dn and gamma.
+// (I - R^2)^{-1}, then y, z, s_up, s_dn and gamma.  After the nn steps, a
+// tail holds the final y and z of the chain.
 template <class Gm>
 struct TapeLayout {
   static constexpr int NP = Gm::NP;
   static constexpr int TILE = Gm::G * Gm::TE;
-  static constexpr int STEP = (3 * TILE + 4 * NP + 1 + 1) / 2 * 2;
+  static constexpr int OFF_R = 0, OFF_T = TILE, OFF_TG = 2 * TILE, OFF_AI = 3 * TILE;
+  static constexpr int OFF_VEC = 4 * TILE;  // y, z, s_up, s_dn (NP each), gamma
+  static constexpr int STEP = (4 * TILE + 4 * NP + 1 + 1) / 2 * 2;
+  static constexpr int TAIL = 2 * NP;
+  static __host__ __device__ long long layer(int nn) { return (long long)nn * STEP + TAIL; }
 };
+// Matrix buffers a taping doubling uses besides 0..5: T column-major
+// (ping-pong) and (I - R^2)^{-1}.  They lie above the buffers that carry the
+// adjoint's layer cotangents into the doubling adjoint.
+constexpr int kTapeBufTc0 = 18, kTapeBufTc1 = 19, kTapeBufAinv = 20;
 
 // Shared-memory bytes of one group for a kernel kind: the common prefix and
 // one typed region (FP64), or for the mixed kind the larger of the FP32
@@ -256,7 +265,10 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
 // thin-layer start at tau0 = tau 2^-nn, then nn doublings of R, T and of the
 // thermal (y, z) and solar sources.  On return R is in m[0] (row-major) and
 // m[1] (column-major), T in m[return value] (row-major, 2 or 3), and the
-// combined thermal + solar sources in V_SUP / V_SDN.
+// combined thermal + solar sources in V_SUP / V_SDN.  With a tape, every
+// step is recorded for the adjoint (TapeLayout); the step then inverts
+// I - R^2 explicitly (kept on the tape) and forms TG = T (I - R^2)^{-1} as a
+// product, using the extra buffers kTapeBuf*.
 template <class Gm>
 __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
                                      double om, double Bt, double Bb, double tcum, int N,
@@ -276,6 +288,9 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
   const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oTG = X.mo(5);
   const unsigned oT[2] = {X.mo(2), X.mo(3)};
+  const bool taping = (tape != nullptr);
+  const unsigned oTcm[2] = {X.mo(kTapeBufTc0), X.mo(kTapeBufTc1)};
+  const unsigned oAi = X.mo(kTapeBufAinv);
   Real* Rrm = sp<Real>(oR);
   Real* Rcm = sp<Real>(oRc);
   Real* Am = sp<Real>(oA);  // I - R R, then TG R (column-major)
@@ -305,6 +320,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
       tl.store_rm(Rt, Rrm);
       tl.store_cm(Rt, Rcm);
       tl.store_rm(Tt, sp<Real>(oT[0]));
+      if (taping) tl.store_cm(Tt, sp<Real>(oTcm[0]));
     }
   }
   if (X.warp == 0 && X.lane < NP) {
@@ -345,26 +361,33 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     }
     op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
     X.sync();
-    *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
+    if (taping) {  // (I - R^2)^{-1}, then TG = T (I - R^2)^{-1}
+      *singular |= op_gj<Gm>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar, oAi);
+      X.sync();
+      op_gemm<Gm>(oTcm[cur], oAi, kNoMat, 0, kNoMat, oTG, t);
+    } else {
+      *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
+    }
     X.sync();
-    if (tape) {  // the adjoint's record of this step: R, T, TG (stored from column-major) + vectors
+    if (taping) {  // the adjoint's record of this step
       using Tp = TapeLayout<Gm>;
       Real* tk = tape + (size_t)k * Tp::STEP;
-      op_s2g<Gm>(oR, tk, t);
-      op_s2g<Gm>(oTc, tk + Tp::TILE, t);
-      op_s2g<Gm>(oTG, tk + 2 * Tp::TILE, t);
+      op_s2g<Gm>(oR, tk + Tp::OFF_R, t);
+      op_s2g<Gm>(oTc, tk + Tp::OFF_T, t);
+      op_s2g<Gm>(oTG, tk + Tp::OFF_TG, t);  // from column-major: TG^T
+      op_s2g<Gm>(oAi, tk + Tp::OFF_AI, t);
       if (X.warp == 0 && X.lane < NP) {
-        tk[3 * Tp::TILE + X.lane] = y[X.lane];
-        tk[3 * Tp::TILE + NP + X.lane] = z[X.lane];
-        tk[3 * Tp::TILE + 2 * NP + X.lane] = su[X.lane];
-        tk[3 * Tp::TILE + 3 * NP + X.lane] = sd[X.lane];
+        tk[Tp::OFF_VEC + X.lane] = y[X.lane];
+        tk[Tp::OFF_VEC + NP + X.lane] = z[X.lane];
+        tk[Tp::OFF_VEC + 2 * NP + X.lane] = su[X.lane];
+        tk[Tp::OFF_VEC + 3 * NP + X.lane] = sd[X.lane];
       }
-      if (t == 0) tk[3 * Tp::TILE + 4 * NP] = gam;
+      if (t == 0) tk[Tp::OFF_VEC + 4 * NP] = gam;
     }
     op_gemm<Gm>(oTG, oR, kNoMat, 0, kNoMat, oA, t);  // TGR = TG R (column-major)
     X.sync();
     op_gemm<Gm>(oA, oTc, oR, 0, oR, oRc, t);                 // R <- R + TGR T
-    op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], kNoMat, t);  // T <- TG T
+    op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], taping ? oTcm[cur ^ 1] : kNoMat, t);  // T <- TG T
     if (X.warp == 0) {
       Real* yn = X.V(V_Y0 + 1 - par);
       Real* zn = X.V(V_Z0 + 1 - par);
@@ -394,6 +417,11 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     cur ^= 1;
   }
   X.sync();
+  if (taping && X.warp == 0 && X.lane < NP) {  // tail: the chain's final y, z
+    Real* tl_ = tape + (size_t)nn * TapeLayout<Gm>::STEP;
+    tl_[X.lane] = X.V(V_Y0 + (nn & 1))[X.lane];
+    tl_[NP + X.lane] = X.V(V_Z0 + (nn & 1))[X.lane];
+  }
   if (X.warp == 0 && X.lane < NP) {
     const int i = X.lane, par = nn & 1;
     const double Bbar = (Bb + Bt) / 2.0;
@@ -765,7 +793,8 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
 template <class Gm, int MODE>
 __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, int t_, int bar,
                                       int w, char* slot, int lmax, unsigned* status,
-                                      double* ivec = nullptr) {
+                                      double* ivec = nullptr, double* tape_all = nullptr,
+                                      long long tape_cap = 0, long long* toff = nullptr) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   using SLay = SlotLayout<Gm>;
@@ -860,7 +889,11 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
   }
 
   // ---------------- upward: doubling + adding onto the composite below
+  // With tape_all (the adjoint's forward, FP64), the doubling chains of the
+  // layers are recorded back to back from the bottom while they fit in
+  // tape_cap doubles; toff[l] is the offset of layer l's record or -1.
   int singular = 0;
+  long long tape_used = 0;
   for (int l = nL - 1; l >= 0; --l) {
     const double tau = lv.tau[l], om = lv.om[l];
     const double Bt = lv.B[l], Bb = lv.B[l + 1];
@@ -911,8 +944,19 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
                     Ppm);
       }
       if constexpr (MODE == MODE_FP64) {
+        Real* tape_l = nullptr;
+        if (tape_all) {
+          const long long need = TapeLayout<Gm>::layer(num_doublings(tau, om > 1.0 ? 1.0 : om));
+          if (tape_used + need <= tape_cap) {
+            tape_l = tape_all + tape_used;
+            if (t == 0) toff[l] = tape_used;
+            tape_used += need;
+          } else if (t == 0) {
+            toff[l] = -1;
+          }
+        }
         tcur = doubling<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
-                            Ppp, Ppm, &singular);
+                            Ppp, Ppm, &singular, tape_l);
       } else if constexpr (MODE == MODE_MIX_S) {
         tcur = doubling_lam<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0,
                                 mu0, Ppp, Ppm, &singular, nullptr);

@@ -323,6 +323,8 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
 // alias out_rm (each thread reads its own tile before writing it).
 // Marks an absent optional operand (add / out_rm / out_cm / B / bvec).
 constexpr unsigned kNoMat = 0xffffffffu;
+// As op_gj's right-hand side: the identity (X = A^{-1}).
+constexpr unsigned kIdentity = 0xfffffffeu;
 
 template <class Gm>
 __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned add_off,
@@ -504,8 +506,10 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
       v = *reinterpret_cast<const double2*>(A_rm + r * LD + c);
     } else if (B_rm) {
       v = *reinterpret_cast<const double2*>(B_rm + (r - NP) * LD + c);
-    } else {
+    } else if (bvec) {
       v = (r == NP) ? make_double2(bvec[c], bvec[c + 1]) : make_double2(0.0, 0.0);
+    } else {  // identity right-hand side
+      v = make_double2((r - NP == c) ? 1.0 : 0.0, (r - NP == c + 1) ? 1.0 : 0.0);
     }
     acc[u][0] = v.x;
     acc[u][1] = v.y;
@@ -612,17 +616,19 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
 // X = B A^{-1} by Gauss-Jordan column elimination, with column pivoting on
 // the largest |entry| of the pivot row -- the pivot rule of the LU with
 // partial pivoting of A^T that the reference's right-solve performs
-// (src/matrix.hpp:120-124).  A and B are row-major in smem; when B is null
-// the right-hand side is the single row `bvec` (a vector solve).  The result
-// is written column-major to out_cm.  Returns nonzero if a pivot was exactly 0.
+// (src/matrix.hpp:120-124).  A and B are row-major in smem; when B is kNoMat
+// the right-hand side is the single row `bvec` (a vector solve), when it is
+// kIdentity the result is A^{-1}.  The result is written column-major to
+// out_cm and/or row-major to out_rm.  FP64 orders >= 8 take gj_mma (above).
+// Returns nonzero if a pivot was exactly 0.
 template <class Gm>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
                                   int bar, unsigned orm_off = 0xffffffffu) {
   using Real = typename Gm::Real;
   const Real* A_rm = sp<Real>(a_off);
-  const Real* B_rm = (b_off == kNoMat) ? nullptr : sp<Real>(b_off);
-  const Real* bvec = (bvec_off == kNoMat) ? nullptr : sp<Real>(bvec_off);
+  const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
+  const Real* bvec = (bvec_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(bvec_off);
   Real* out_cm = sp<Real>(ocm_off);
   Real* gjbuf = sp<Real>(gj_off);
   unsigned* red = sp<unsigned>(red_off);
@@ -641,11 +647,16 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
     tl.load_rm(A, A_rm);
     if (B_rm) {
       tl.load_rm(B, B_rm);
-    } else {
+    } else if (bvec) {
 #pragma unroll
       for (int a = 0; a < TR; ++a)
 #pragma unroll
         for (int b = 0; b < TC; ++b) B[a][b] = (tl.row(a) == 0) ? bvec[tl.col(b)] : Real(0);
+    } else {
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) B[a][b] = (tl.row(a) == tl.col(b)) ? Real(1) : Real(0);
     }
   } else {
 #pragma unroll
