@@ -500,6 +500,9 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   Real* qp = vb + A_H * NP;
   Real* qm = vb + A_RU * NP;
   // un-normalised Q
+  if constexpr (UsePhaseMMA<Gm>::value)
+    phase_products<Gm>(chi, nuse, -1.0, N, pl, Qpp, Qpm, LD, t);
+  else
   for (int e = t; e < NP * NP; e += G) {
     const int r = e / NP, c = e % NP;
     double spp = 0.0, spm = 0.0;
@@ -575,14 +578,51 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   }
   X.sync();
   // dchi_l = (2l+1)/(2 pi) [P_l^T (dQpp + s_l dQpm) P_l + p0_l P_l . (dqp + s_l dqm)]
+  bool forms_done = false;
+  if constexpr (UsePhaseMMA<Gm>::value) {
+    // the quadratic forms on the tensor cores: V = S B with S = dQpp + dQpm
+    // (even l) or dQpp - dQpm (odd l) and B[j][k] = P_l(k)(mu_j), l(k) = 2k or
+    // 2k + 1; the form of moment l(k) is column k of V dotted with P_l(k)(mu_.)
+    constexpr int NT = NP / 8, NW = G / 32;
+    const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+    const int kt = (((nuse + 1) >> 1) + 7) >> 3;  // 8-column tiles of moments per parity
+    for (int tau = warp; tau < 2 * NT * kt; tau += NW) {
+      const int par = tau / (NT * kt), i = (tau % (NT * kt)) / kt, jt = tau % kt;
+      const double sg = par ? -1.0 : 1.0;
+      const int r = 8 * i + g, lb = 2 * (8 * jt + g) + par;
+      double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < NP / 4; ++ks) {
+        const int j = 4 * ks + q;
+        const double a = dPpp[r * LD + j] + sg * dPpm[r * LD + j];
+        const double b = (j < N && lb < nuse) ? pl[lb * N + j] : 0.0;
+        mma_f64_m8n8k4(v0, v1, a, b);
+      }
+      const int l0 = 2 * (8 * jt + 2 * q) + par, l1 = l0 + 2;  // columns 2q, 2q + 1
+      double s0 = (r < N && l0 < nuse) ? v0 * pl[l0 * N + r] : 0.0;
+      double s1 = (r < N && l1 < nuse) ? v1 * pl[l1 * N + r] : 0.0;
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      }
+      if (g == 0) {
+        if (l0 < nuse) atomicAdd(&dchi[l0], (2 * l0 + 1) * s0 / (2.0 * kPi));
+        if (l1 < nuse) atomicAdd(&dchi[l1], (2 * l1 + 1) * s1 / (2.0 * kPi));
+      }
+    }
+    forms_done = true;
+  }
   for (int l = t; l < nuse; l += G) {
     const double sg = (l & 1) ? -1.0 : 1.0;
     double acc = 0.0;
-    for (int i = 0; i < N; ++i) {
-      double ri = 0.0;
-      for (int j = 0; j < N; ++j)
-        ri += (dPpp[i * LD + j] + sg * dPpm[i * LD + j]) * pl[l * N + j];
-      acc += pl[l * N + i] * ri;
+    if (!forms_done) {
+      for (int i = 0; i < N; ++i) {
+        double ri = 0.0;
+        for (int j = 0; j < N; ++j)
+          ri += (dPpp[i * LD + j] + sg * dPpm[i * LD + j]) * pl[l * N + j];
+        acc += pl[l * N + i] * ri;
+      }
     }
     if (solar) {
       double p0 = 1.0, p1 = mu0, plm = 1.0;
@@ -601,7 +641,7 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
       for (int i = 0; i < N; ++i) sv += pl[l * N + i] * (qp[i] + sg * qm[i]);
       acc += plm * sv;
     }
-    atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
+    if (!forms_done || solar) atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
   }
   X.sync();
 }

@@ -173,6 +173,57 @@ struct Levels {
 // and, with a solar beam, the phase vectors at mu0 (src/phase_matrix.hpp:
 // 131-181) into D_PP / D_PM.  chi_l = (chi[l] - f) / (1 - f) when delta-M
 // truncation applies (f >= 0), chi[l] otherwise.
+//
+// On the FP64 tensor cores (NP >= 8) the double sum is two products over the
+// even and the odd moments, E = A_e B_e and O = A_o B_o with
+// A[r][k] = d_l P_l(mu_r), B[k][c] = P_l(mu_c), d_l = (2l+1) chi_l, so that
+// P++ = (E + O) / 2pi and P+- = (E - O) / 2pi; rows and columns >= N are zero.
+template <class Gm>
+struct UsePhaseMMA {
+  static constexpr int NT = Gm::NP / 8, NW = Gm::G / 32;
+  static constexpr bool value = Gm::NP >= 8 && (NT * NT) % NW == 0;
+};
+
+// Un-normalised Q+- (as above) into qpp / qpm with row stride ldq.
+template <class Gm>
+__device__ __forceinline__ void phase_products(const double* chi, int nuse, double f, int N,
+                                               const double* pl, double* qpp, double* qpm,
+                                               int ldq, int t) {
+  constexpr int NT = UsePhaseMMA<Gm>::NT, NW = UsePhaseMMA<Gm>::NW, TPW = NT * NT / NW;
+  const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+  const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
+  const int kh = (nuse + 1) >> 1;  // even moments (odd ones: nuse / 2)
+  double ev[TPW][2], od[TPW][2];
+#pragma unroll
+  for (int u = 0; u < TPW; ++u) ev[u][0] = ev[u][1] = od[u][0] = od[u][1] = 0.0;
+  for (int k0 = 0; k0 < kh; k0 += 4) {
+    const int le = 2 * (k0 + q), lo = le + 1;
+    double de = 0.0, dd = 0.0;
+    if (le < nuse) de = (2 * le + 1) * ((f >= 0.0) ? (chi[le] - f) * inv_1mf : chi[le]);
+    if (lo < nuse) dd = (2 * lo + 1) * ((f >= 0.0) ? (chi[lo] - f) * inv_1mf : chi[lo]);
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+      const int tau = warp * TPW + u, r = 8 * (tau / NT) + g, c = 8 * (tau % NT) + g;
+      const double ae = (r < N && le < nuse) ? de * pl[le * N + r] : 0.0;
+      const double be = (c < N && le < nuse) ? pl[le * N + c] : 0.0;
+      const double ao = (r < N && lo < nuse) ? dd * pl[lo * N + r] : 0.0;
+      const double bo = (c < N && lo < nuse) ? pl[lo * N + c] : 0.0;
+      mma_f64_m8n8k4(ev[u][0], ev[u][1], ae, be);
+      mma_f64_m8n8k4(od[u][0], od[u][1], ao, bo);
+    }
+  }
+  const double s = 1.0 / (2.0 * kPi);
+#pragma unroll
+  for (int u = 0; u < TPW; ++u) {
+    const int tau = warp * TPW + u, r = 8 * (tau / NT) + g, c = 8 * (tau % NT) + 2 * q;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      qpp[r * ldq + c + e] = (ev[u][e] + od[u][e]) * s;
+      qpm[r * ldq + c + e] = (ev[u][e] - od[u][e]) * s;
+    }
+  }
+}
+
 template <class Gm>
 __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
                                          const double* chi, int nuse, double f, int N,
@@ -183,6 +234,9 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
+  if constexpr (UsePhaseMMA<Gm>::value)
+    phase_products<Gm>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t);
+  else
   for (int e = t; e < NP * NP; e += G) {
     const int r = e / NP, c = e % NP;
     double spp = 0.0, spm = 0.0;
