@@ -147,17 +147,15 @@ enum AdjMat {
   J_bT1, J_bT1c, J_bTGR, J_bTGRc, J_bTG, J_W, J_C, J_Cc, J_T1, J_T2, J_VEC,
   kMatsAdj = J_VEC + 2  // J_VEC spans two buffers (18 vectors even at NP = 8)
 };
-// Doubling steps per layer budgeted for the forward's record of the chains.
-// nn = trunc(log2 tau) + 4 / 10 / 16, so 24 covers tau up to 256 for any omega;
-// the record is one pool per wavenumber, so thin layers leave room for thick
-// ones, and layers beyond it are recomputed in the adjoint.
-constexpr int kTapeStepsPerLayer = 24;
+// The record pool of a chunk holds kTapeStepsPerLayer doubling steps per
+// layer and wavenumber on average (nn = trunc(log2 tau) + 4 / 10 / 16, so
+// 12 covers tau up to 2^-4 .. 2^8 depending on omega; the pool is shared, so
+// thin layers leave room for thick ones).  A wavenumber whose chains do not
+// fit is recomputed in the reverse.  kAdjointMemory bounds the adjoint's
+// work memory when the engine has no workspace limit.
+constexpr int kTapeStepsPerLayer = 12;
+constexpr size_t kAdjointMemory = size_t(16) << 30;
 
-// A recomputing (taping) doubling runs while the layer cotangents sit in
-// J_bR0..J_bT0c; its extra buffers are the adjoint step's scratch J_W, J_C, J_Cc.
-static_assert(kTapeBufTc0 == J_W && kTapeBufTc1 == J_C && kTapeBufAinv == J_Cc &&
-                  kTapeBufTc0 > J_bT0c,
-              "taping doubling buffers must not hold live cotangents");
 // Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 20 NP).
 enum AdjVec {
   A_BY = 0, A_BZ, A_BSU, A_BSD, A_H, A_RU, A_RD, A_BRU, A_BRD, A_BH, A_Y, A_Z, A_SU, A_SD,
@@ -165,26 +163,39 @@ enum AdjVec {
   A_CUB  // the adding adjoint's carried d U_base (not touched by the layer adjoints)
 };
 
-// Adjoint slot in HBM: the forward slot (levels, phase, records), the
-// interface intensities, the downward-pass vectors, one layer's doubling
-// record (for layers recomputed in the adjoint), the layout-1 phase-cotangent
-// accumulators, the per-layer tape offsets, then (bytes() onwards) the
-// forward's record of every layer's doubling, tape_cap doubles.
+// Per-wavenumber state that the taping forward (tape_kernel, the forward
+// kernel's geometry GC) leaves for the reverse (adjoint_kernel): the forward
+// slot (levels, phase, records in GC's tile order), the interface
+// intensities, and the offsets of the layers' doubling records (toff[l],
+// relative to the wavenumber's block of the record pool, or -1; toff[L] is
+// that block's offset in the pool, or -1).
+template <class GC>
+struct WavState {
+  static __host__ __device__ size_t fwd(int lmax) {
+    return (SlotLayout<GC>::bytes(lmax) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t ivec(int lmax) {
+    return ((size_t)(lmax + 1) * 2 * GC::NP * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t toff_at(int lmax) { return fwd(lmax) + ivec(lmax); }
+  static __host__ __device__ size_t bytes(int lmax) {
+    return toff_at(lmax) + (((size_t)(lmax + 1) * sizeof(long long) + 255) & ~size_t(255));
+  }
+};
+
+// Per-group scratch of the reverse: the downward-pass vectors, one layer's
+// doubling record (layers without a record are recomputed into it), the
+// layout-1 phase-cotangent accumulators, the carried d R_base (own tile
+// order), the level accumulators and 32 scalars.
 template <class Gm>
-struct AdjSlot {
-  using SL = SlotLayout<Gm>;
+struct AdjScratch {
   using Tp = TapeLayout<Gm>;
   static constexpr int NP = Gm::NP;
-  static __host__ __device__ size_t fwd(int lmax) { return (SL::bytes(lmax) + 255) & ~size_t(255); }
-  static __host__ __device__ size_t ivec(int lmax) {
+  static __host__ __device__ size_t dvec(int lmax) {
     return ((size_t)(lmax + 1) * 2 * NP * sizeof(double) + 255) & ~size_t(255);
   }
-  static __host__ __device__ size_t dvec(int lmax) { return ivec(lmax); }
   static __host__ __device__ size_t tape() {
     return ((size_t)Tp::layer(kMaxDoublings) * sizeof(double) + 255) & ~size_t(255);
-  }
-  static __host__ __device__ size_t toff(int lmax) {
-    return ((size_t)lmax * sizeof(long long) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t pacc() {
     return ((size_t)2 * NP * NP * sizeof(double) + 2 * NP * sizeof(double) + 255) & ~size_t(255);
@@ -194,11 +205,7 @@ struct AdjSlot {
     return ((size_t)4 * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t bytes(int lmax) {
-    return toff_at(lmax) + toff(lmax);
-  }
-  // byte offset of the per-layer tape offsets (after the 256-byte scalar block)
-  static __host__ __device__ size_t toff_at(int lmax) {
-    return fwd(lmax) + ivec(lmax) + dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256;
+    return dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256;
   }
 };
 
@@ -221,7 +228,14 @@ struct AdjGroup {
 struct AdjDev {
   const double *c_fu, *c_fd, *c_J, *c_fdir;  // [W*(L+1)] each, or null
   double *g_tau, *g_ssa, *g_mom, *g_temp, *g_planck, *g_semis;
-  long long tape_cap;  // doubles per slot for the forward's record of the doubling chains
+  // one chunk of wavenumbers [w0, w0 + P.ntasks): per-wavenumber states
+  // (WavState, state_bytes apart) and the pool of doubling records
+  long long w0;
+  char* state;
+  size_t state_bytes;
+  double* pool;
+  long long pool_cap;               // doubles
+  unsigned long long* pool_used;    // zeroed before each chunk
 };
 
 // ---------------------------------------------------------------- doubling adjoint
@@ -241,12 +255,13 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   using Real = typename Gm::Real;
   static_assert(sizeof(Real) == 8, "the adjoint runs in FP64");
   using Tp = TapeLayout<Gm>;
+  using GC = Geo<Gm::NP, double>;  // record order
   const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, G = Gm::G;
   const int t = X.t;
   double* red = reinterpret_cast<double*>(X.gjbuf) + 4;  // 4 doubles of reduction scratch
   // 1. the record of this layer's chain: taped by the forward pass, or the
-  //    chain again now (buffers 0..5, the kTapeBuf* buffers and V_*)
+  //    chain again now (buffers 0..5 and V_*)
   const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
   if (recompute)
     doubling<Gm>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm, singular,
@@ -296,10 +311,10 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     const unsigned nRr = X.mo(cs ? J_bR0 : J_bR1), nRc = X.mo(cs ? J_bR0c : J_bR1c);
     const unsigned nTr = X.mo(cs ? J_bT0 : J_bT1), nTc = X.mo(cs ? J_bT0c : J_bT1c);
     X.sync();
-    op_g2s<Gm>(tk + Tp::OFF_R, X.mo(J_R), X.mo(J_Rc), t);
-    op_g2s<Gm>(tk + Tp::OFF_T, kNoMat, X.mo(J_Tc), t);
-    op_g2s<Gm>(tk + Tp::OFF_TG, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
-    op_g2s<Gm>(tk + Tp::OFF_AI, kNoMat, X.mo(J_Ac), t);       // (I - R R)^{-1} (cm)
+    op_g2s<Gm, GC>(tk + Tp::OFF_R, X.mo(J_R), X.mo(J_Rc), t);
+    op_g2s<Gm, GC>(tk + Tp::OFF_T, kNoMat, X.mo(J_Tc), t);
+    op_g2s<Gm, GC>(tk + Tp::OFF_TG, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
+    op_g2s<Gm, GC>(tk + Tp::OFF_AI, kNoMat, X.mo(J_Ac), t);       // (I - R R)^{-1} (cm)
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
       VA(A_Y)[i] = tk[Tp::OFF_VEC + i];
@@ -648,14 +663,19 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
 
 
 // ---------------------------------------------------------------- one wavenumber
-// Runs after wav_body (FP64, with the interface intensities kept in `iv`).
+// Runs on the state a taping forward left for wavenumber w (WavState: the
+// slot with levels, phase matrices and records in GC's tile order, the
+// interface intensities, the record offsets), with the group's scratch.
 template <int NP>
 __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int bar, int w,
-                                         char* slot, int lmax, unsigned* status, AdjDev AD) {
+                                         char* slot, char* scr, int lmax, unsigned* status,
+                                         AdjDev AD) {
   using Gm = AdjGeo<NP>;
+  using GC = Geo<NP, double>;  // the taping forward's geometry: record order
   using Real = double;
   using SLay = SlotLayout<Gm>;
-  using AS = AdjSlot<Gm>;
+  using WS = WavState<GC>;
+  using AS = AdjScratch<Gm>;
   constexpr int TILE = SLay::TILE, REC = SLay::REC, G = Gm::G, TR = Gm::TR, TC = Gm::TC;
   constexpr int LD = Gm::LD;
   const Ctx<Gm> X(goff, tb, t_, bar);
@@ -672,16 +692,17 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   double* Ppp = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
   double* Ppm = Ppp + NP * NP;
   double* recs = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
-  char* p = slot + AS::fwd(lmax);
-  double* iv = reinterpret_cast<double*>(p);                      // [L+1][Id, Iu]
-  double* dv = reinterpret_cast<double*>(p += AS::ivec(lmax));    // [L+1][brhs, u]
+  double* iv = reinterpret_cast<double*>(slot + WS::fwd(lmax));   // [L+1][Id, Iu]
+  const long long* toff = reinterpret_cast<const long long*>(slot + WS::toff_at(lmax));
+  char* p = scr;
+  double* dv = reinterpret_cast<double*>(p);                      // [L+1][brhs, u]
   double* tape = reinterpret_cast<double*>(p += AS::dvec(lmax));
   double* pacc = reinterpret_cast<double*>(p += AS::tape());      // dPpp, dPpm, dpp, dpm
   double* brb = reinterpret_cast<double*>(p += AS::pacc());       // carried d R_base (tiles)
   double* acc = reinterpret_cast<double*>(p += AS::brb());        // bB, btc, dtau, dom
   double* scal = reinterpret_cast<double*>(p += AS::acc(lmax));   // 32 doubles
-  const long long* toff = reinterpret_cast<const long long*>(slot + AS::toff_at(lmax));
-  double* tape_all = reinterpret_cast<double*>(slot + AS::bytes(lmax));
+  const long long tbase = toff[nL];                               // this wavenumber's records
+  double* tape_all = (tbase >= 0) ? AD.pool + tbase : nullptr;
   double* bB = acc;
   double* btc = acc + (lmax + 1);
   double* gtau = acc + 2 * (lmax + 1);
@@ -719,9 +740,9 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     const int scat = rl[3 * TILE + 2 * NP] != 0.0;
     const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
     X.sync();
-    op_g2s<Gm>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);  // R_base(l+1)
-    op_g2s<Gm>(rl, X.mo(J_R), X.mo(J_Rc), t);               // R_l
-    op_g2s<Gm>(rl + TILE, X.mo(J_TG), kNoMat, t);           // T_l (rm)
+    op_g2s<Gm, GC>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);  // R_base(l+1)
+    op_g2s<Gm, GC>(rl, X.mo(J_R), X.mo(J_Rc), t);               // R_l
+    op_g2s<Gm, GC>(rl + TILE, X.mo(J_TG), kNoMat, t);           // T_l (rm)
     X.sync();
     if (X.warp == 0) {  // bIu(l+1), bx = Rb^T bIu + bId
       if (X.lane < NP) {
@@ -763,7 +784,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   }
   X.sync();
   // interface 0: Iu0 = Rb0 Id0 + Ub0, Id0 = Btop
-  op_g2s<Gm>(recs + 2 * TILE, X.mo(J_TGR), kNoMat, t);
+  op_g2s<Gm, GC>(recs + 2 * TILE, X.mo(J_TGR), kNoMat, t);
   X.sync();
   double pBtop = 0.0;
   if (X.warp == 0) {
@@ -813,9 +834,9 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
     const double tau = lv.tau[l], om = lv.om[l];
     X.sync();
-    op_g2s<Gm>(rl, X.mo(J_R), X.mo(J_Rc), t);
-    op_g2s<Gm>(rl + TILE, X.mo(J_TG), X.mo(J_Tc), t);
-    op_g2s<Gm>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);
+    op_g2s<Gm, GC>(rl, X.mo(J_R), X.mo(J_Rc), t);
+    op_g2s<Gm, GC>(rl + TILE, X.mo(J_TG), X.mo(J_Tc), t);
+    op_g2s<Gm, GC>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);
     op_g2s<Gm>(brb, X.mo(J_bTGR), X.mo(J_bTGRc), t);
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
@@ -977,7 +998,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       nuse_l1 = nuse;
       if (layout != 1)
         build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
-      const long long to = toff[l];
+      const long long to = tape_all ? toff[l] : -1;
       doubling_adjoint<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
                            Ppp, Ppm, to >= 0 ? tape_all + to : tape, to < 0, scal, &singular);
       if (t == 0) {
@@ -1128,6 +1149,73 @@ struct AdjKern {
   static constexpr int kThreads = kGroups * G;
 };
 
+// Taping forward of one chunk, in the forward kernel's geometry and shared
+// memory (one-warp groups at NP <= 16): prologue, a claim on the record pool
+// for all of the wavenumber's doubling chains (none when the pool is full:
+// the reverse then recomputes them), and the forward solve recording the
+// chains, the records and the interface intensities into the wavenumber's
+// WavState.
+template <int NP>
+__global__ void __launch_bounds__(128, 3) tape_kernel(SolveParams P, ColumnDev col0, AdjDev AD) {
+  using GD = Geo<NP, double>;
+  using GL = GroupLayout<NP, KIND_FP64>;
+  using WS = WavState<GD>;
+  constexpr int G = GD::G;
+  const int gib = threadIdx.x / G;
+  const int t = threadIdx.x % G;
+  const int bar = 1 + gib;
+  const unsigned goff = (unsigned)(gib * GL::bytes);
+  const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
+  for (unsigned i = (unsigned)t * 4u; i < (unsigned)GL::bytes; i += (unsigned)G * 4u)
+    *sp<unsigned>(goff + i) = 0u;
+  gsync<G>(bar);
+  if (t == 0) *sp<ColumnDev>(goff + CommonLayout<NP>::col) = col0;
+  long long* task_s = sp<long long>(goff + CommonLayout<NP>::misc + 32);
+  double* red = sp<double>(goff + CommonLayout<NP>::misc + 64);
+  const int lmax = P.max_layers, nL = col0.L;
+  for (;;) {
+    long long task;
+    if constexpr (G == 32) {
+      unsigned long long v = 0;
+      if (t == 0) v = atomicAdd(P.counter, 1ull);
+      task = (long long)__shfl_sync(0xffffffffu, v, 0);
+    } else {
+      gsync<G>(bar);
+      if (t == 0) *task_s = (long long)atomicAdd(P.counter, 1ull);
+      gsync<G>(bar);
+      task = *task_s;
+    }
+    if (task >= P.ntasks) break;
+    const int w = (int)(AD.w0 + task);
+    char* st = AD.state + (size_t)task * AD.state_bytes;
+    long long* toff = reinterpret_cast<long long*>(st + WS::toff_at(lmax));
+    gsync<G>(bar);
+    wav_prologue<NP>(goff, t, bar, w, st, lmax, P.status, 0);
+    const Levels lv(st, lmax);
+    double need = 0.0;  // doubles of this wavenumber's records (exact in FP64)
+    for (int l = t; l < nL; l += G) {
+      const double tau = lv.tau[l], om = lv.om[l];
+      if (tau > 0.0 && om > 0.0)
+        need += (double)TapeLayout<GD>::layer(num_doublings(tau, om > 1.0 ? 1.0 : om));
+    }
+    need = gsum<G>(need, red, bar);
+    if (t == 0) {
+      const unsigned long long n = (unsigned long long)need;
+      const unsigned long long base = atomicAdd(AD.pool_used, n);
+      toff[nL] = (base + n <= (unsigned long long)AD.pool_cap) ? (long long)base : -1ll;
+    }
+    gsync<G>(bar);
+    const long long base = toff[nL];
+    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, st, lmax, P.status,
+                            reinterpret_cast<double*>(st + WS::fwd(lmax)),
+                            base >= 0 ? AD.pool + base : nullptr, base >= 0 ? (long long)need : 0,
+                            toff);
+  }
+}
+
+// Reverse of one chunk (after its tape_kernel): per wavenumber, the prologue
+// again for the group's shared constants, then wav_adjoint on the state the
+// forward left.
 template <int NP>
 __global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolveParams P, ColumnDev col0, AdjDev AD) {
   using GD = AdjGeo<NP>;
@@ -1138,7 +1226,7 @@ __global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolvePar
   const unsigned goff = (unsigned)(gib * AdjGroup<NP>::bytes);
   const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
   const int slot = blockIdx.x * (blockDim.x / G) + gib;
-  char* sl = P.scratch + (size_t)slot * P.slot_bytes;
+  char* scr = P.scratch + (size_t)slot * P.slot_bytes;
   for (unsigned i = (unsigned)t * 4u; i < (unsigned)AdjGroup<NP>::bytes; i += (unsigned)G * 4u)
     *sp<unsigned>(goff + i) = 0u;
   gsync<G>(bar);
@@ -1157,15 +1245,11 @@ __global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolvePar
       task = *task_s;
     }
     if (task >= P.ntasks) break;
-    const int w = (int)task;
+    const int w = (int)(AD.w0 + task);
+    char* st = AD.state + (size_t)task * AD.state_bytes;
     gsync<G>(bar);
-    wav_prologue<NP, adjoint_group<NP>()>(goff, t, bar, w, sl, P.max_layers, P.status, 0);
-    double* iv = reinterpret_cast<double*>(sl + AdjSlot<GD>::fwd(P.max_layers));
-    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status, iv,
-                            reinterpret_cast<double*>(sl + AdjSlot<GD>::bytes(P.max_layers)),
-                            AD.tape_cap,
-                            reinterpret_cast<long long*>(sl + AdjSlot<GD>::toff_at(P.max_layers)));
-    wav_adjoint<NP>(goff, tb, t, bar, w, sl, P.max_layers, P.status, AD);
+    wav_prologue<NP, adjoint_group<NP>()>(goff, t, bar, w, st, P.max_layers, P.status, 0);
+    wav_adjoint<NP>(goff, tb, t, bar, w, st, scr, P.max_layers, P.status, AD);
   }
 }
 

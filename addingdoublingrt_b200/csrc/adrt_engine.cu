@@ -644,26 +644,40 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   e->last_stream = s;
   if ((rc = ensure_quad(e, d->num_quadrature, d->num_moments))) return rc;
   const int np = padded_order(d->num_quadrature);
+  // Per chunk of wavenumbers: tape_kernel (the forward kernel's geometry)
+  // leaves each wavenumber's state and doubling records in HBM, then
+  // adjoint_kernel runs the reverse on them.
   struct AK {
-    int groups, threads;
-    size_t smem, slot, base;
-    long long tape_cap;
-    const void* fn;
+    int groups, threads, fgroups, fthreads;
+    size_t smem, fsmem, scr, state;
+    long long step;  // doubles per recorded doubling step
+    const void *fn, *ffn;
     void (*launch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
+    void (*flaunch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
   } k{};
+  const int L = d->num_layers;
   auto make = [&](auto tag) {
     constexpr int NP = decltype(tag)::value;
     using GD = AdjGeo<NP>;
+    using GC = Geo<NP, double>;
     k.groups = AdjKern<NP>::kGroups;
     k.threads = AdjKern<NP>::kThreads;
     k.smem = (size_t)k.groups * AdjGroup<NP>::bytes;
-    k.base = (AdjSlot<GD>::bytes(d->num_layers) + 255) & ~size_t(255);
-    k.tape_cap = (long long)d->num_layers * TapeLayout<GD>::layer(kTapeStepsPerLayer);
-    k.slot = k.base + (((size_t)k.tape_cap * sizeof(double) + 255) & ~size_t(255));
+    k.scr = align256(AdjScratch<GD>::bytes(L));
+    k.state = align256(WavState<GC>::bytes(L));
+    k.step = TapeLayout<GC>::STEP;
+    k.fthreads = Kern<NP, KIND_FP64>::kThreads;
+    k.fgroups = Kern<NP, KIND_FP64>::kGroups;
+    k.fsmem = Kern<NP, KIND_FP64>::smem();
     k.fn = reinterpret_cast<const void*>(adjoint_kernel<NP>);
+    k.ffn = reinterpret_cast<const void*>(tape_kernel<NP>);
     k.launch = [](const SolveParams& p, const ColumnDev& c, const AdjDev& a, int grid, size_t smem,
                   cudaStream_t st) {
       adjoint_kernel<NP><<<grid, AdjKern<NP>::kThreads, smem, st>>>(p, c, a);
+    };
+    k.flaunch = [](const SolveParams& p, const ColumnDev& c, const AdjDev& a, int grid,
+                   size_t smem, cudaStream_t st) {
+      tape_kernel<NP><<<grid, Kern<NP, KIND_FP64>::kThreads, smem, st>>>(p, c, a);
     };
   };
   switch (np) {
@@ -673,28 +687,25 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
     default: make(std::integral_constant<int, 32>{}); break;
   }
   CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
-  int bps = 0;
+  CUDA_TRY(cudaFuncSetAttribute(k.ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.fsmem));
+  int bps = 0, fbps = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, k.threads, k.smem));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fbps, k.ffn, k.fthreads, k.fsmem));
   if (bps < 1) bps = 1;
-  int grid = bps * e->num_sms;
-  const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
-  grid = std::min(grid, need_blocks);
-  size_t need = (size_t)grid * k.groups * k.slot;
-  if (e->max_ws && need > e->max_ws) {
-    // a shorter tape first (layers beyond it are recomputed), then fewer groups
-    const size_t per = e->max_ws / ((size_t)grid * k.groups);
-    if (per >= k.base) {
-      k.tape_cap = (long long)((per - k.base) / sizeof(double)) & ~31ll;
-      k.slot = k.base + (size_t)k.tape_cap * sizeof(double);
-    } else {
-      k.tape_cap = 0;
-      k.slot = k.base;
-      grid = (int)(e->max_ws / ((size_t)k.groups * k.slot));
-      if (grid < 1)
-        return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint slot (%zu B)", k.slot);
-    }
-    need = (size_t)grid * k.groups * k.slot;
-  }
+  if (fbps < 1) fbps = 1;
+  const long long W = d->num_wavenumbers;
+  // chunk: one wavenumber per resident forward group, within the memory budget
+  const long long rgroups = (long long)bps * e->num_sms * k.groups;
+  const size_t rev_bytes = (size_t)rgroups * k.scr;
+  const size_t per_w = k.state + (size_t)L * kTapeStepsPerLayer * k.step * sizeof(double);
+  const size_t budget = e->max_ws ? e->max_ws : kAdjointMemory;
+  if (budget < rev_bytes + per_w)
+    return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint chunk (%zu B)",
+                rev_bytes + per_w);
+  long long wc = std::min<long long>(W, (long long)fbps * e->num_sms * k.fgroups);
+  wc = std::max<long long>(1, std::min<long long>(wc, (long long)((budget - rev_bytes) / per_w)));
+  const long long pool_cap = wc * L * kTapeStepsPerLayer * k.step;
+  const size_t need = rev_bytes + (size_t)wc * k.state + (size_t)pool_cap * sizeof(double) + 256;
   if (need > e->adj_scratch_bytes) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cap);
@@ -714,13 +725,11 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   SolveParams p{};
   p.cols = nullptr;
   p.ncols = 1;
-  p.ntasks = d->num_wavenumbers;
   p.counter = e->counter;
   p.status = e->status;
   p.scratch = e->adj_scratch;
-  p.slot_bytes = k.slot;
-  p.nslots = grid * k.groups;
-  p.max_layers = d->num_layers;
+  p.slot_bytes = k.scr;
+  p.max_layers = L;
   AdjDev a{};
   a.c_fu = cot->flux_up;
   a.c_fd = cot->flux_down;
@@ -732,10 +741,28 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   a.g_temp = gr->temperature;
   a.g_planck = gr->planck_levels;
   a.g_semis = gr->surface_emission;
-  a.tape_cap = k.tape_cap;
-  CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
-  k.launch(p, c0, a, grid, k.smem, s);
-  CUDA_TRY(cudaGetLastError());
+  a.state = e->adj_scratch + rev_bytes;
+  a.state_bytes = k.state;
+  a.pool = reinterpret_cast<double*>(a.state + (size_t)wc * k.state);
+  a.pool_cap = pool_cap;
+  a.pool_used = reinterpret_cast<unsigned long long*>(a.pool + pool_cap);
+  for (long long w0 = 0; w0 < W; w0 += wc) {
+    const long long nw = std::min(wc, W - w0);
+    a.w0 = w0;
+    p.ntasks = nw;
+    const int fgrid = (int)std::min<long long>((long long)fbps * e->num_sms,
+                                               (nw + k.fgroups - 1) / k.fgroups);
+    const int rgrid = (int)std::min<long long>((long long)bps * e->num_sms,
+                                               (nw + k.groups - 1) / k.groups);
+    p.nslots = rgrid * k.groups;
+    CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(a.pool_used, 0, sizeof(unsigned long long), s));
+    k.flaunch(p, c0, a, fgrid, k.fsmem, s);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+    k.launch(p, c0, a, rgrid, k.smem, s);
+    CUDA_TRY(cudaGetLastError());
+  }
   return ADRT_OK;
 }
 

@@ -87,10 +87,7 @@ struct TapeLayout {
   static constexpr int TAIL = 2 * NP;
   static __host__ __device__ long long layer(int nn) { return (long long)nn * STEP + TAIL; }
 };
-// Matrix buffers a taping doubling uses besides 0..5: T column-major
-// (ping-pong) and (I - R^2)^{-1}.  They lie above the buffers that carry the
-// adjoint's layer cotangents into the doubling adjoint.
-constexpr int kTapeBufTc0 = 18, kTapeBufTc1 = 19, kTapeBufAinv = 20;
+
 
 // Shared-memory bytes of one group for a kernel kind: the common prefix and
 // one typed region (FP64), or for the mixed kind the larger of the FP32
@@ -320,9 +317,10 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
 // thermal (y, z) and solar sources.  On return R is in m[0] (row-major) and
 // m[1] (column-major), T in m[return value] (row-major, 2 or 3), and the
 // combined thermal + solar sources in V_SUP / V_SDN.  With a tape, every
-// step is recorded for the adjoint (TapeLayout); the step then inverts
-// I - R^2 explicitly (kept on the tape) and forms TG = T (I - R^2)^{-1} as a
-// product, using the extra buffers kTapeBuf*.
+// step is recorded for the adjoint (TapeLayout, matrices in the tile order of
+// the forward kernel's geometry whatever the group size): R, T, TG, and
+// (I - R^2)^{-1} from a second right-solve against the identity that writes
+// straight to the tape.
 template <class Gm>
 __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
                                      double om, double Bt, double Bb, double tcum, int N,
@@ -343,8 +341,8 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oTG = X.mo(5);
   const unsigned oT[2] = {X.mo(2), X.mo(3)};
   const bool taping = (tape != nullptr);
-  const unsigned oTcm[2] = {X.mo(kTapeBufTc0), X.mo(kTapeBufTc1)};
-  const unsigned oAi = X.mo(kTapeBufAinv);
+  using GC = Geo<NP, Real>;  // record order
+  using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);
   Real* Rcm = sp<Real>(oRc);
   Real* Am = sp<Real>(oA);  // I - R R, then TG R (column-major)
@@ -374,7 +372,6 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
       tl.store_rm(Rt, Rrm);
       tl.store_cm(Rt, Rcm);
       tl.store_rm(Tt, sp<Real>(oT[0]));
-      if (taping) tl.store_cm(Tt, sp<Real>(oTcm[0]));
     }
   }
   if (X.warp == 0 && X.lane < NP) {
@@ -415,21 +412,17 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     }
     op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
     X.sync();
-    if (taping) {  // (I - R^2)^{-1}, then TG = T (I - R^2)^{-1}
-      *singular |= op_gj<Gm>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar, oAi);
-      X.sync();
-      op_gemm<Gm>(oTcm[cur], oAi, kNoMat, 0, kNoMat, oTG, t);
-    } else {
-      *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
-    }
+    *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
     X.sync();
     if (taping) {  // the adjoint's record of this step
-      using Tp = TapeLayout<Gm>;
       Real* tk = tape + (size_t)k * Tp::STEP;
-      op_s2g<Gm>(oR, tk + Tp::OFF_R, t);
-      op_s2g<Gm>(oTc, tk + Tp::OFF_T, t);
-      op_s2g<Gm>(oTG, tk + Tp::OFF_TG, t);  // from column-major: TG^T
-      op_s2g<Gm>(oAi, tk + Tp::OFF_AI, t);
+      // (I - R^2)^{-1} straight to the record; the free T buffer is the scratch
+      *singular |= op_gj<Gm, GC>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
+                                 oT[cur ^ 1], tk + Tp::OFF_AI);
+      op_s2g<Gm, GC>(oR, tk + Tp::OFF_R, t);
+      op_s2g<Gm, GC>(oTc, tk + Tp::OFF_T, t);
+      op_s2g<Gm, GC>(oTG, tk + Tp::OFF_TG, t);  // from column-major: TG^T
+      X.sync();
       if (X.warp == 0 && X.lane < NP) {
         tk[Tp::OFF_VEC + X.lane] = y[X.lane];
         tk[Tp::OFF_VEC + NP + X.lane] = z[X.lane];
@@ -441,7 +434,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     op_gemm<Gm>(oTG, oR, kNoMat, 0, kNoMat, oA, t);  // TGR = TG R (column-major)
     X.sync();
     op_gemm<Gm>(oA, oTc, oR, 0, oR, oRc, t);                 // R <- R + TGR T
-    op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], taping ? oTcm[cur ^ 1] : kNoMat, t);  // T <- TG T
+    op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], kNoMat, t);  // T <- TG T
     if (X.warp == 0) {
       Real* yn = X.V(V_Y0 + 1 - par);
       Real* zn = X.V(V_Z0 + 1 - par);
@@ -472,7 +465,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   }
   X.sync();
   if (taping && X.warp == 0 && X.lane < NP) {  // tail: the chain's final y, z
-    Real* tl_ = tape + (size_t)nn * TapeLayout<Gm>::STEP;
+    Real* tl_ = tape + (size_t)nn * Tp::STEP;
     tl_[X.lane] = X.V(V_Y0 + (nn & 1))[X.lane];
     tl_[NP + X.lane] = X.V(V_Z0 + (nn & 1))[X.lane];
   }
@@ -943,9 +936,9 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
   }
 
   // ---------------- upward: doubling + adding onto the composite below
-  // With tape_all (the adjoint's forward, FP64), the doubling chains of the
-  // layers are recorded back to back from the bottom while they fit in
-  // tape_cap doubles; toff[l] is the offset of layer l's record or -1.
+  // With toff (the adjoint's forward, FP64), the doubling chains of the
+  // layers are recorded back to back from the bottom into tape_all while they
+  // fit in tape_cap doubles; toff[l] is the offset of layer l's record or -1.
   int singular = 0;
   long long tape_used = 0;
   for (int l = nL - 1; l >= 0; --l) {
@@ -999,9 +992,9 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
       }
       if constexpr (MODE == MODE_FP64) {
         Real* tape_l = nullptr;
-        if (tape_all) {
+        if (toff) {
           const long long need = TapeLayout<Gm>::layer(num_doublings(tau, om > 1.0 ? 1.0 : om));
-          if (tape_used + need <= tape_cap) {
+          if (tape_all && tape_used + need <= tape_cap) {
             tape_l = tape_all + tape_used;
             if (t == 0) toff[l] = tape_used;
             tape_used += need;

@@ -244,6 +244,13 @@ struct Tile {
   }
 };
 
+// Offset of element (r, c) of an NP x NP matrix stored in the tile order of
+// geometry GO (thread t of GO owns TE contiguous Reals).
+template <class GO>
+__host__ __device__ __forceinline__ int tile_index(int r, int c) {
+  return ((r / GO::TR) * GO::CB + c / GO::TC) * GO::TE + (r % GO::TR) * GO::TC + c % GO::TC;
+}
+
 // FP64 products on the tensor cores: mma.sync m8n8k4 f64 (the FP64 tensor
 // path of sm_100a; tcgen05 has no f64 kind).  Each warp owns WR x WC output
 // tiles of 8x8; lane (g = lane/4, q = lane%4) holds rows g, columns 2q, 2q+1
@@ -487,10 +494,10 @@ struct UseGjMMA {
                                 ((2 * NP / 8) * (NP / 8)) % NW == 0;
 };
 
-template <class Gm>
+template <class Gm, class GO = Gm>
 __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, const double* bvec,
                                       double* out_cm, double* out_rm, double* lbuf, double* rbuf,
-                                      int t, int bar) {
+                                      int t, int bar, double* out_g = nullptr) {
   constexpr int NP = Gm::NP, LD = Gm::LD, G = Gm::G, NW = G / 32;
   constexpr int NTR = 2 * NP / 8, NTC = NP / 8, TPW = NTR * NTC / NW;
   constexpr int RS = NP + 4;  // rbuf row stride (conflict-free B-fragment loads)
@@ -608,6 +615,10 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
         out_cm[c * LD + r] = acc[u][0];
         out_cm[(c + 1) * LD + r] = acc[u][1];
       }
+      if (out_g) {  // HBM, in the tile order of GO
+        out_g[tile_index<GO>(r, c)] = acc[u][0];
+        out_g[tile_index<GO>(r, c + 1)] = acc[u][1];
+      }
     }
   }
   return singular;
@@ -621,10 +632,12 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
 // kIdentity the result is A^{-1}.  The result is written column-major to
 // out_cm and/or row-major to out_rm.  FP64 orders >= 8 take gj_mma (above).
 // Returns nonzero if a pivot was exactly 0.
-template <class Gm>
+// out_g (optional): the result also into HBM, in the tile order of GO.
+template <class Gm, class GO = Gm>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
-                                  int bar, unsigned orm_off = 0xffffffffu) {
+                                  int bar, unsigned orm_off = 0xffffffffu,
+                                  typename Gm::Real* out_g = nullptr) {
   using Real = typename Gm::Real;
   const Real* A_rm = sp<Real>(a_off);
   const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
@@ -638,7 +651,9 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
     static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
     Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
     Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
-    return gj_mma<Gm>(A_rm, B_rm, bvec, o_cm, out_rm, o_cm ? o_cm : out_rm, gjbuf, t, bar);
+    // scratch: the output buffer, or the one matrix buffer the call names
+    Real* lbuf = o_cm ? o_cm : out_rm;
+    return gj_mma<Gm, GO>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
   }
   const Tile<Gm> tl(t);
   const bool tv = tl.valid();
@@ -765,14 +780,19 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
 #pragma unroll
         for (int a = 0; a < TR; ++a) out_rm[tl.row(a) * LD + q[b]] = colv[a];
       }
+      if (out_g) {
+#pragma unroll
+        for (int a = 0; a < TR; ++a) out_g[tile_index<GO>(tl.row(a), q[b])] = colv[a];
+      }
     }
   }
   return singular;
 }
 
-// Tile copies between the HBM scratch (tile order: thread t owns TE
-// contiguous Reals) and smem.
-template <class Gm>
+// Tile copies between the HBM scratch and smem.  The HBM side is in the tile
+// order of GO: the group's own (thread t owns TE contiguous Reals) or, for
+// records written by a kernel of another group size, that kernel's order.
+template <class Gm, class GO = Gm>
 __device__ __noinline__ void op_g2s(const typename Gm::Real* g, unsigned orm_off,
                                     unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
@@ -782,16 +802,23 @@ __device__ __noinline__ void op_g2s(const typename Gm::Real* g, unsigned orm_off
   const Tile<Gm> tl(t);
   if (!tl.valid()) return;
   Real X[TR][TC];
-  const Real* p = g + t * Gm::TE;
+  if constexpr (GO::G == Gm::G) {
+    const Real* p = g + t * Gm::TE;
 #pragma unroll
-  for (int a = 0; a < TR; ++a)
+    for (int a = 0; a < TR; ++a)
 #pragma unroll
-    for (int b = 0; b < TC; ++b) X[a][b] = p[a * TC + b];
+      for (int b = 0; b < TC; ++b) X[a][b] = p[a * TC + b];
+  } else {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) X[a][b] = g[tile_index<GO>(tl.row(a), tl.col(b))];
+  }
   if (out_rm) tl.store_rm(X, out_rm);
   if (out_cm) tl.store_cm(X, out_cm);
 }
 
-template <class Gm>
+template <class Gm, class GO = Gm>
 __device__ __noinline__ void op_s2g(unsigned in_off, typename Gm::Real* g, int t) {
   using Real = typename Gm::Real;
   const Real* in_rm = sp<Real>(in_off);
@@ -800,11 +827,18 @@ __device__ __noinline__ void op_s2g(unsigned in_off, typename Gm::Real* g, int t
   if (!tl.valid()) return;
   Real X[TR][TC];
   tl.load_rm(X, in_rm);
-  Real* p = g + t * Gm::TE;
+  if constexpr (GO::G == Gm::G) {
+    Real* p = g + t * Gm::TE;
 #pragma unroll
-  for (int a = 0; a < TR; ++a)
+    for (int a = 0; a < TR; ++a)
 #pragma unroll
-    for (int b = 0; b < TC; ++b) p[a * TC + b] = X[a][b];
+      for (int b = 0; b < TC; ++b) p[a * TC + b] = X[a][b];
+  } else {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) g[tile_index<GO>(tl.row(a), tl.col(b))] = X[a][b];
+  }
 }
 
 // ============================================================== matvec (warp 0)
