@@ -122,6 +122,143 @@ __device__ __noinline__ void op_rank(unsigned orm, unsigned ocm, unsigned u0, un
   }
 }
 
+// out = sum_s X_s Y_s [+ add] [+ sum_p a_p u_p v_p^T]: up to three products
+// (X_s column-major, Y_s row-major, K = NP each), an added row-major matrix
+// and up to four rank-one terms (vectors in smem) in one pass, so that a
+// step of the doubling adjoint needs one barrier per dependent product.
+struct GemmX {
+  unsigned x[3], y[3];
+  int nseg;
+  unsigned add, orm, ocm;
+  unsigned u[4], v[4];
+  double a[4];
+  int nrank;
+};
+
+template <class Gm, int NSEG, int NRANK>
+__device__ __noinline__ void op_gemm_x(const GemmX g, int t) {
+  using Real = typename Gm::Real;
+  constexpr int NP = Gm::NP, LD = Gm::LD;
+  const Real* add = (g.add == kNoMat) ? nullptr : sp<Real>(g.add);
+  Real* out_rm = (g.orm == kNoMat) ? nullptr : sp<Real>(g.orm);
+  Real* out_cm = (g.ocm == kNoMat) ? nullptr : sp<Real>(g.ocm);
+  const Real* ru[NRANK > 0 ? NRANK : 1];
+  const Real* rv[NRANK > 0 ? NRANK : 1];
+#pragma unroll
+  for (int p = 0; p < NRANK; ++p) {
+    ru[p] = sp<Real>(g.u[p]);
+    rv[p] = sp<Real>(g.v[p]);
+  }
+  auto rank = [&](int r, int c) {
+    Real v = Real(0);
+#pragma unroll
+    for (int p = 0; p < NRANK; ++p) v += static_cast<Real>(g.a[p]) * ru[p][r] * rv[p][c];
+    return v;
+  };
+  if constexpr (UseMMA<Gm>::value) {
+    constexpr int NT = NP / 8;
+    constexpr int TPW = NT * NT / (Gm::G / 32);
+    constexpr int WR = (TPW >= 4) ? 2 : 1, WC = (TPW >= 2) ? 2 : 1;
+    constexpr int WPC = NT / WC;
+    // a warp with one output tile keeps two partial sums (even / odd k-steps)
+    // so that consecutive DMMAs do not wait on each other
+    constexpr int NA = (WR * WC == 1) ? 2 : 1;
+    const int warp = t >> 5, lane = t & 31, gg = lane >> 2, q = lane & 3;
+    const int r0 = (warp / WPC) * WR * 8, c0 = (warp % WPC) * WC * 8;
+    double acc[NA][WR][WC][2];
+#pragma unroll
+    for (int h = 0; h < NA; ++h)
+#pragma unroll
+      for (int i = 0; i < WR; ++i)
+#pragma unroll
+        for (int j = 0; j < WC; ++j) acc[h][i][j][0] = acc[h][i][j][1] = 0.0;
+#pragma unroll
+    for (int sg = 0; sg < NSEG; ++sg) {
+      const double* XT = sp<double>(g.x[sg]);
+      const double* Y = sp<double>(g.y[sg]);
+#pragma unroll
+      for (int ks = 0; ks < NP / 4; ++ks) {
+        const int k = ks * 4 + q;
+        const int h = (sg * (NP / 4) + ks) % NA;
+        double a[WR], b[WC];
+#pragma unroll
+        for (int i = 0; i < WR; ++i) a[i] = XT[k * LD + r0 + i * 8 + gg];
+#pragma unroll
+        for (int j = 0; j < WC; ++j) b[j] = Y[k * LD + c0 + j * 8 + gg];
+#pragma unroll
+        for (int i = 0; i < WR; ++i)
+#pragma unroll
+          for (int j = 0; j < WC; ++j)
+            mma_f64_m8n8k4(acc[h][i][j][0], acc[h][i][j][1], a[i], b[j]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < WR; ++i)
+#pragma unroll
+      for (int j = 0; j < WC; ++j) {
+        const int r = r0 + i * 8 + gg, c = c0 + j * 8 + 2 * q;
+        double v0 = acc[0][i][j][0], v1 = acc[0][i][j][1];
+        if constexpr (NA == 2) {
+          v0 += acc[1][i][j][0];
+          v1 += acc[1][i][j][1];
+        }
+        if (add) {
+          const double2 ad = *reinterpret_cast<const double2*>(add + r * LD + c);
+          v0 = ad.x + v0;
+          v1 = ad.y + v1;
+        }
+        if constexpr (NRANK > 0) {
+          v0 += rank(r, c);
+          v1 += rank(r, c + 1);
+        }
+        if (out_rm) *reinterpret_cast<double2*>(out_rm + r * LD + c) = make_double2(v0, v1);
+        if (out_cm) {
+          out_cm[c * LD + r] = v0;
+          out_cm[(c + 1) * LD + r] = v1;
+        }
+      }
+  } else {
+    constexpr int TR = Gm::TR, TC = Gm::TC;
+    const Tile<Gm> tl(t);
+    if (!tl.valid()) return;
+    Real acc[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) acc[a][b] = Real(0);
+#pragma unroll
+    for (int sg = 0; sg < NSEG; ++sg) {
+      const Real* xp = sp<Real>(g.x[sg]) + tl.rb * TR;
+      const Real* yp = sp<Real>(g.y[sg]) + tl.cb * TC;
+      for (int k = 0; k < NP; ++k) {
+        Real xa[TR], yb[TC];
+        lds_vec<Real, TR>(xa, xp + k * LD);
+        lds_vec<Real, TC>(yb, yp + k * LD);
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+          for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+      }
+    }
+    if (add) {
+      Real ad[TR][TC];
+      tl.load_rm(ad, add);
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) acc[a][b] = ad[a][b] + acc[a][b];
+    }
+    if constexpr (NRANK > 0) {
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) acc[a][b] += rank(tl.row(a), tl.col(b));
+    }
+    if (out_rm) tl.store_rm(acc, out_rm);
+    if (out_cm) tl.store_cm(acc, out_cm);
+  }
+}
+
 // Copy a row-major matrix into row-major and/or column-major buffers, scaled.
 template <class Gm>
 __device__ __noinline__ void op_copy(unsigned in_rm, unsigned orm, unsigned ocm, double scale,
@@ -310,6 +447,19 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     const unsigned bTr = X.mo(cs ? J_bT1 : J_bT0), bTc = X.mo(cs ? J_bT1c : J_bT0c);
     const unsigned nRr = X.mo(cs ? J_bR0 : J_bR1), nRc = X.mo(cs ? J_bR0c : J_bR1c);
     const unsigned nTr = X.mo(cs ? J_bT0 : J_bT1), nTc = X.mo(cs ? J_bT0c : J_bT1c);
+    auto gx = [&](unsigned x0, unsigned y0, unsigned x1, unsigned y1, unsigned x2, unsigned y2,
+                  unsigned add, unsigned orm, unsigned ocm) {
+      GemmX a{};
+      a.x[0] = x0; a.y[0] = y0; a.x[1] = x1; a.y[1] = y1; a.x[2] = x2; a.y[2] = y2;
+      a.nseg = (x1 == kNoMat) ? 1 : (x2 == kNoMat) ? 2 : 3;
+      a.add = add; a.orm = orm; a.ocm = ocm;
+      a.nrank = 0;
+      return a;
+    };
+    auto rk = [&](GemmX& a, int s_u, int s_v, double al) {
+      a.u[a.nrank] = vo(s_u); a.v[a.nrank] = vo(s_v); a.a[a.nrank] = al; ++a.nrank;
+    };
+    // 1. this step's record; h = z + g y
     X.sync();
     op_g2s<Gm, GC>(tk + Tp::OFF_R, X.mo(J_R), X.mo(J_Rc), t);
     op_g2s<Gm, GC>(tk + Tp::OFF_T, kNoMat, X.mo(J_Tc), t);
@@ -317,46 +467,56 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     op_g2s<Gm, GC>(tk + Tp::OFF_AI, kNoMat, X.mo(J_Ac), t);       // (I - R R)^{-1} (cm)
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
-      VA(A_Y)[i] = tk[Tp::OFF_VEC + i];
-      VA(A_Z)[i] = tk[Tp::OFF_VEC + NP + i];
+      const double y = tk[Tp::OFF_VEC + i], z = tk[Tp::OFF_VEC + NP + i];
+      VA(A_Y)[i] = y;
+      VA(A_Z)[i] = z;
+      VA(A_H)[i] = z + g * y;
       VA(A_SU)[i] = tk[Tp::OFF_VEC + 2 * NP + i];
       VA(A_SD)[i] = tk[Tp::OFF_VEC + 3 * NP + i];
     }
     X.sync();
-    op_gemm<Gm>(X.mo(J_TGc), X.mo(J_R), kNoMat, 0, X.mo(J_TGR), kNoMat, t);  // TGR = TG R
-    if (X.warp == 0) {  // h = z + g y, ru = R sd + gam su, rd = gam R su + sd
+    // 2. TGR = TG R;  dTGR = dR T^T - bz h^T + by y^T;  ru = R sd + gam su, rd = gam R su + sd
+    op_gemm_x<Gm, 1, 0>(gx(X.mo(J_TGc), X.mo(J_R), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat,
+                           X.mo(J_TGR), kNoMat), t);
+    {
+      GemmX a = gx(bRc, X.mo(J_Tc), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat, X.mo(J_bTGR),
+                   X.mo(J_bTGRc));
+      rk(a, A_BZ, A_H, -1.0);
+      rk(a, A_BY, A_Y, 1.0);
+      op_gemm_x<Gm, 1, 2>(a, t);
+    }
+    if (X.warp == 0) {
       const Real* vv[2] = {VA(A_SD), VA(A_SU)};
       Real yv[2];
       matvec<Gm, true, 2>(X.m(J_Rc), vv, yv, X.lane);
       if (X.lane < NP) {
         const int i = X.lane;
-        VA(A_H)[i] = VA(A_Z)[i] + g * VA(A_Y)[i];
         VA(A_RU)[i] = yv[0] + gam * VA(A_SU)[i];
         VA(A_RD)[i] = gam * yv[1] + VA(A_SD)[i];
       }
     }
-    // dTGR = dR T^T - bz h^T + by y^T
-    op_gemm<Gm>(bRc, X.mo(J_Tc), kNoMat, 0, X.mo(J_bTGR), X.mo(J_bTGRc), t);
-    // dTG (partial) = dT T^T
-    op_gemm<Gm>(bTc, X.mo(J_Tc), kNoMat, 0, X.mo(J_T1), kNoMat, t);
     X.sync();
-    op_rank<Gm>(X.mo(J_bTGR), X.mo(J_bTGRc), vo(A_BZ), vo(A_H), -1.0, vo(A_BY), vo(A_Y), 1.0,
-                kNoMat, kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
+    // 3. dTG = dTGR R^T + dT T^T + bz h^T + by y^T + bsu ru^T + bsd rd^T (column-major)
+    {
+      GemmX a = gx(X.mo(J_bTGRc), X.mo(J_Rc), bTc, X.mo(J_Tc), kNoMat, kNoMat, kNoMat, kNoMat,
+                   X.mo(J_bTG));
+      rk(a, A_BZ, A_H, 1.0);
+      rk(a, A_BY, A_Y, 1.0);
+      rk(a, A_BSU, A_RU, 1.0);
+      rk(a, A_BSD, A_RD, 1.0);
+      op_gemm_x<Gm, 2, 4>(a, t);
+    }
     X.sync();
-    // dTG = dT T^T + dTGR R^T + bz h^T + by y^T + bsu ru^T + bsd rd^T
-    //   (kept column-major in J_bTG)
-    op_gemm<Gm>(X.mo(J_bTGRc), X.mo(J_Rc), X.mo(J_T1), 0, kNoMat, X.mo(J_bTG), t);
+    // 4. W = dTG A^{-T} = dTG ((I - R R)^{-1})^T
+    op_gemm_x<Gm, 1, 0>(gx(X.mo(J_bTG), X.mo(J_Ac), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat,
+                           X.mo(J_W), kNoMat), t);
     X.sync();
-    op_rank<Gm>(kNoMat, X.mo(J_bTG), vo(A_BZ), vo(A_H), 1.0, vo(A_BY), vo(A_Y), 1.0, vo(A_BSU),
-                vo(A_RU), 1.0, vo(A_BSD), vo(A_RD), 1.0, t);
-    X.sync();
-    // W = dTG A^{-T} = dTG ((I - R R)^{-1})^T
-    op_gemm<Gm>(X.mo(J_bTG), X.mo(J_Ac), kNoMat, 0, X.mo(J_W), kNoMat, t);
-    X.sync();
-    // C = TG^T W  (= -dA);  dT' = TG^T dT + W + TGR^T dR
-    op_gemm<Gm>(X.mo(J_TG), X.mo(J_W), kNoMat, 0, X.mo(J_C), X.mo(J_Cc), t);
-    op_gemm<Gm>(X.mo(J_TG), bTr, X.mo(J_W), 0, X.mo(J_T1), kNoMat, t);
-    if (X.warp == 0) {  // vector cotangents of this step
+    // 5. C = TG^T W (= -dA);  dT' = TG^T dT + TGR^T dR + W;  the vector cotangents
+    op_gemm_x<Gm, 1, 0>(gx(X.mo(J_TG), X.mo(J_W), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat,
+                           X.mo(J_C), X.mo(J_Cc)), t);
+    op_gemm_x<Gm, 2, 0>(gx(X.mo(J_TG), bTr, X.mo(J_TGR), bRr, kNoMat, kNoMat, X.mo(J_W), nTr,
+                           nTc), t);
+    if (X.warp == 0) {
       const Real* v1[2] = {VA(A_BSU), VA(A_BSD)};
       Real tgs[2];
       matvec<Gm, true, 2>(X.m(J_TG), v1, tgs, X.lane);  // TG^T bsu, TG^T bsd
@@ -402,16 +562,14 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       }
     }
     X.sync();
-    op_gemm<Gm>(X.mo(J_TGR), bRr, X.mo(J_T1), 0, nTr, nTc, t);  // dT' = ... + TGR^T dR
-    // dR' = dR + TG^T dTGR + C R^T + R^T C + bru sd^T + gam brd su^T
-    op_gemm<Gm>(X.mo(J_TG), X.mo(J_bTGR), bRr, 0, X.mo(J_T2), kNoMat, t);
-    X.sync();
-    op_gemm<Gm>(X.mo(J_Cc), X.mo(J_Rc), X.mo(J_T2), 0, X.mo(J_T1), kNoMat, t);
-    X.sync();
-    op_gemm<Gm>(X.mo(J_R), X.mo(J_C), X.mo(J_T1), 0, nRr, nRc, t);
-    X.sync();
-    op_rank<Gm>(nRr, nRc, vo(A_BRU), vo(A_SD), 1.0, vo(A_BRD), vo(A_SU), gam, kNoMat, kNoMat, 0.0,
-                kNoMat, kNoMat, 0.0, t);
+    // 6. dR' = TG^T dTGR + C R^T + R^T C + dR + bru sd^T + gam brd su^T
+    {
+      GemmX a = gx(X.mo(J_TG), X.mo(J_bTGR), X.mo(J_Cc), X.mo(J_Rc), X.mo(J_R), X.mo(J_C), bRr,
+                   nRr, nRc);
+      rk(a, A_BRU, A_SD, 1.0);
+      rk(a, A_BRD, A_SU, gam);
+      op_gemm_x<Gm, 3, 2>(a, t);
+    }
     const double pg = red[0], pgam = red[1];
     bgam = pgam + 2.0 * gam * bgam;
     bg = pg + 2.0 * bg;

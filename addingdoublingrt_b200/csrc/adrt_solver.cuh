@@ -280,11 +280,15 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
   static_assert(TPW >= 1 && (NT / WR) * WPC == Gm::G / 32, "warp grid must cover the tiles");
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
   const int r0 = (warp / WPC) * WR * 8, c0 = (warp % WPC) * WC * 8;
-  double acc[WR][WC][2];
+  // a warp with one output tile keeps two partial sums (even / odd k-steps)
+  constexpr int NA = (WR * WC == 1 && NP >= 16) ? 2 : 1;
+  double acc[NA][WR][WC][2];
 #pragma unroll
-  for (int i = 0; i < WR; ++i)
+  for (int h = 0; h < NA; ++h)
 #pragma unroll
-    for (int j = 0; j < WC; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int i = 0; i < WR; ++i)
+#pragma unroll
+      for (int j = 0; j < WC; ++j) acc[h][i][j][0] = acc[h][i][j][1] = 0.0;
 #pragma unroll
   for (int ks = 0; ks < NP / 4; ++ks) {
     const int k = ks * 4 + q;
@@ -296,14 +300,19 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
 #pragma unroll
     for (int i = 0; i < WR; ++i)
 #pragma unroll
-      for (int j = 0; j < WC; ++j) mma_f64_m8n8k4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      for (int j = 0; j < WC; ++j)
+        mma_f64_m8n8k4(acc[ks % NA][i][j][0], acc[ks % NA][i][j][1], a[i], b[j]);
   }
 #pragma unroll
   for (int i = 0; i < WR; ++i)
 #pragma unroll
     for (int j = 0; j < WC; ++j) {
       const int r = r0 + i * 8 + g, c = c0 + j * 8 + 2 * q;
-      double v0 = acc[i][j][0], v1 = acc[i][j][1];
+      double v0 = acc[0][i][j][0], v1 = acc[0][i][j][1];
+      if constexpr (NA == 2) {
+        v0 += acc[1][i][j][0];
+        v1 += acc[1][i][j][1];
+      }
       if (id_minus == 1) {
         v0 = ((r == c) ? 1.0 : 0.0) - v0;
         v1 = ((r == c + 1) ? 1.0 : 0.0) - v1;
