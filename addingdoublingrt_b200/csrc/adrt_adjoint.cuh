@@ -162,7 +162,7 @@ __device__ __noinline__ void op_gemm_x(const GemmX g, int t) {
     constexpr int WPC = NT / WC;
     // a warp with one output tile keeps two partial sums (even / odd k-steps)
     // so that consecutive DMMAs do not wait on each other
-    constexpr int NA = (WR * WC == 1) ? 2 : 1;
+    constexpr int NA = (WR * WC == 1) ? ((NSEG > 1) ? 4 : 2) : 1;
     const int warp = t >> 5, lane = t & 31, gg = lane >> 2, q = lane & 3;
     const int r0 = (warp / WPC) * WR * 8, c0 = (warp % WPC) * WC * 8;
     double acc[NA][WR][WC][2];
@@ -198,9 +198,10 @@ __device__ __noinline__ void op_gemm_x(const GemmX g, int t) {
       for (int j = 0; j < WC; ++j) {
         const int r = r0 + i * 8 + gg, c = c0 + j * 8 + 2 * q;
         double v0 = acc[0][i][j][0], v1 = acc[0][i][j][1];
-        if constexpr (NA == 2) {
-          v0 += acc[1][i][j][0];
-          v1 += acc[1][i][j][1];
+#pragma unroll
+        for (int h = 1; h < NA; ++h) {
+          v0 += acc[h][i][j][0];
+          v1 += acc[h][i][j][1];
         }
         if (add) {
           const double2 ad = *reinterpret_cast<const double2*>(add + r * LD + c);
@@ -299,6 +300,9 @@ enum AdjVec {
   A_BUP, A_BDN, A_T0, A_T1,
   A_CUB  // the adding adjoint's carried d U_base (not touched by the layer adjoints)
 };
+// Partial products of one doubling-adjoint step, in slots that are scratch
+// inside the step loop (z is only needed for h; T0 / T1 are written after it).
+constexpr int A_X0 = A_BH, A_X1 = A_T0, A_X2 = A_T1, A_X3 = A_Z;
 
 // Per-wavenumber state that the taping forward (tape_kernel, the forward
 // kernel's geometry GC) leaves for the reverse (adjoint_kernel): the forward
@@ -395,6 +399,7 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   using GC = Geo<Gm::NP, double>;  // record order
   const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, G = Gm::G;
+  constexpr int NWG = G / 32;  // warps of the group (vector work is spread over them)
   const int t = X.t;
   double* red = reinterpret_cast<double*>(X.gjbuf) + 4;  // 4 doubles of reduction scratch
   // 1. the record of this layer's chain: taped by the forward pass, or the
@@ -485,7 +490,7 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       rk(a, A_BY, A_Y, 1.0);
       op_gemm_x<Gm, 1, 2>(a, t);
     }
-    if (X.warp == 0) {
+    if (X.warp == 3 % NWG) {
       const Real* vv[2] = {VA(A_SD), VA(A_SU)};
       Real yv[2];
       matvec<Gm, true, 2>(X.m(J_Rc), vv, yv, X.lane);
@@ -516,21 +521,45 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
                            X.mo(J_C), X.mo(J_Cc)), t);
     op_gemm_x<Gm, 2, 0>(gx(X.mo(J_TG), bTr, X.mo(J_TGR), bRr, kNoMat, kNoMat, X.mo(J_W), nTr,
                            nTc), t);
-    if (X.warp == 0) {
+    // the vector cotangents' products, one warp each
+    if (X.warp == 1 % NWG) {
       const Real* v1[2] = {VA(A_BSU), VA(A_BSD)};
       Real tgs[2];
       matvec<Gm, true, 2>(X.m(J_TG), v1, tgs, X.lane);  // TG^T bsu, TG^T bsd
-      const Real* v2[2] = {VA(A_BZ), VA(A_BY)};
-      Real tgz[2], trz[2];
-      matvec<Gm, true, 2>(X.m(J_TG), v2, tgz, X.lane);   // TG^T bz, TG^T by
-      matvec<Gm, true, 2>(X.m(J_TGR), v2, trz, X.lane);  // TGR^T bz, TGR^T by
       if (X.lane < NP) {
         VA(A_BRU)[X.lane] = tgs[0];
         VA(A_BRD)[X.lane] = tgs[1];
-        VA(A_BH)[X.lane] = tgz[0] - trz[0];
-        VA(A_T0)[X.lane] = tgz[1] + trz[1];  // (TG + TGR)^T by
       }
-      __syncwarp();
+    }
+    if (X.warp == 2 % NWG) {
+      const Real* v2[2] = {VA(A_BZ), VA(A_BY)};
+      Real tgz[2];
+      matvec<Gm, true, 2>(X.m(J_TG), v2, tgz, X.lane);  // TG^T bz, TG^T by
+      if (X.lane < NP) {
+        VA(A_X0)[X.lane] = tgz[0];
+        VA(A_X1)[X.lane] = tgz[1];
+      }
+    }
+    if (X.warp == 3 % NWG) {
+      const Real* v2[2] = {VA(A_BZ), VA(A_BY)};
+      Real trz[2];
+      matvec<Gm, true, 2>(X.m(J_TGR), v2, trz, X.lane);  // TGR^T bz, TGR^T by
+      if (X.lane < NP) {
+        VA(A_X2)[X.lane] = trz[0];
+        VA(A_X3)[X.lane] = trz[1];
+      }
+    }
+    X.sync();
+    // 6. dR' = TG^T dTGR + C R^T + R^T C + dR + bru sd^T + gam brd su^T; the
+    //    vector cotangents of the step before (reductions read after the next barrier)
+    {
+      GemmX a = gx(X.mo(J_TG), X.mo(J_bTGR), X.mo(J_Cc), X.mo(J_Rc), X.mo(J_R), X.mo(J_C), bRr,
+                   nRr, nRc);
+      rk(a, A_BRU, A_SD, 1.0);
+      rk(a, A_BRD, A_SU, gam);
+      op_gemm_x<Gm, 3, 2>(a, t);
+    }
+    if (X.warp == 1 % NWG) {
       const Real* v3[2] = {VA(A_BRD), VA(A_BRU)};
       Real rt[2];
       matvec<Gm, true, 2>(X.m(J_R), v3, rt, X.lane);  // R^T brd, R^T bru
@@ -540,14 +569,16 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       double pg = 0.0, pgam = 0.0;
       if (X.lane < NP) {
         const int i = X.lane;
-        const double bz = VA(A_BZ)[i], by = VA(A_BY)[i], bh = VA(A_BH)[i];
+        const double bz = VA(A_BZ)[i], by = VA(A_BY)[i];
+        const double bh = VA(A_X0)[i] - VA(A_X2)[i];    // (TG - TGR)^T bz
+        const double bt0 = VA(A_X1)[i] + VA(A_X3)[i];   // (TG + TGR)^T by
         const double bsu = VA(A_BSU)[i], bsd = VA(A_BSD)[i];
         const double y = VA(A_Y)[i], su = VA(A_SU)[i], sd = VA(A_SD)[i];
         const double bru = VA(A_BRU)[i], brd = VA(A_BRD)[i];
         pg = -y * bz + y * bh;
         pgam = sd * bsd + su * bru + rsu[0] * brd;
         VA(A_BZ)[i] = bz + bh;
-        VA(A_BY)[i] = -g * bz + VA(A_T0)[i] + by + g * bh;
+        VA(A_BY)[i] = -g * bz + bt0 + by + g * bh;
         VA(A_BSU)[i] = bsu + gam * bru + gam * rt[0];
         VA(A_BSD)[i] = gam * bsd + rt[1] + brd;
       }
@@ -562,14 +593,6 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       }
     }
     X.sync();
-    // 6. dR' = TG^T dTGR + C R^T + R^T C + dR + bru sd^T + gam brd su^T
-    {
-      GemmX a = gx(X.mo(J_TG), X.mo(J_bTGR), X.mo(J_Cc), X.mo(J_Rc), X.mo(J_R), X.mo(J_C), bRr,
-                   nRr, nRc);
-      rk(a, A_BRU, A_SD, 1.0);
-      rk(a, A_BRD, A_SU, gam);
-      op_gemm_x<Gm, 3, 2>(a, t);
-    }
     const double pg = red[0], pgam = red[1];
     bgam = pgam + 2.0 * gam * bgam;
     bg = pg + 2.0 * bg;
@@ -722,7 +745,7 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
           } else if (l == 1) {
             plm = mu0;
           } else {
-            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) / l;
+            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);  // off the chain
             p0 = p1;
             p1 = plm;
           }
@@ -805,7 +828,7 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
         } else if (m == 1) {
           plm = mu0;
         } else {
-          plm = ((2 * m - 1) * mu0 * p1 - (m - 1) * p0) / m;
+          plm = ((2 * m - 1) * mu0 * p1 - (m - 1) * p0) * recip((double)m);  // off the chain
           p0 = p1;
           p1 = plm;
         }

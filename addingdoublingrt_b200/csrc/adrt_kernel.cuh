@@ -181,11 +181,15 @@ struct UsePhaseMMA {
   static constexpr bool value = Gm::NP >= 8 && (NT * NT) % NW == 0;
 };
 
-// Un-normalised Q+- (as above) into qpp / qpm with row stride ldq.
-template <class Gm>
+// Q+- (as above) into qpp / qpm with row stride ldq; with NORM, already
+// Hansen-normalised: column c scaled by 1 / (2 pi s_c), s_c = sum_r (Q++ +
+// Q+-)[r][c] w_r = sum_r E[r][c] w_r / pi, reduced from the fragments (wt:
+// the quadrature weights, red: NW x NP doubles of scratch).
+template <class Gm, bool NORM = false>
 __device__ __forceinline__ void phase_products(const double* chi, int nuse, double f, int N,
                                                const double* pl, double* qpp, double* qpm,
-                                               int ldq, int t) {
+                                               int ldq, int t, const double* wt = nullptr,
+                                               double* red = nullptr, int bar = 0) {
   constexpr int NT = UsePhaseMMA<Gm>::NT, NW = UsePhaseMMA<Gm>::NW, TPW = NT * NT / NW;
   const int warp = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
@@ -210,13 +214,65 @@ __device__ __forceinline__ void phase_products(const double* chi, int nuse, doub
     }
   }
   const double s = 1.0 / (2.0 * kPi);
+  double corr[NT][2];
+#pragma unroll
+  for (int j = 0; j < NT; ++j) corr[j][0] = corr[j][1] = 1.0;
+  if constexpr (NORM) {
+    double cp[NT][2];  // this warp's part of the column sums of E w
+#pragma unroll
+    for (int j = 0; j < NT; ++j) cp[j][0] = cp[j][1] = 0.0;
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+      const int tau = warp * TPW + u, r = 8 * (tau / NT) + g, j = tau % NT;
+      const double wr = (r < N) ? wt[r] : 0.0;
+      cp[j][0] += ev[u][0] * wr;
+      cp[j][1] += ev[u][1] * wr;
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        cp[j][0] += __shfl_xor_sync(0xffffffffu, cp[j][0], o);
+        cp[j][1] += __shfl_xor_sync(0xffffffffu, cp[j][1], o);
+      }
+    if constexpr (NW > 1) {
+      constexpr int NP = Gm::NP;
+      if (g == 0) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) {
+          red[warp * NP + 8 * j + 2 * q] = cp[j][0];
+          red[warp * NP + 8 * j + 2 * q + 1] = cp[j][1];
+        }
+      }
+      gsync<Gm::G>(bar);
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        double a = 0.0, b = 0.0;
+#pragma unroll
+        for (int w2 = 0; w2 < NW; ++w2) {
+          a += red[w2 * NP + 8 * j + 2 * q];
+          b += red[w2 * NP + 8 * j + 2 * q + 1];
+        }
+        cp[j][0] = a;
+        cp[j][1] = b;
+      }
+      gsync<Gm::G>(bar);
+    }
+#pragma unroll
+    for (int j = 0; j < NT; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const double sc = cp[j][e] / kPi;
+        corr[j][e] = (sc > 0.0) ? 1.0 / (2.0 * kPi * sc) : 1.0;
+      }
+  }
 #pragma unroll
   for (int u = 0; u < TPW; ++u) {
-    const int tau = warp * TPW + u, r = 8 * (tau / NT) + g, c = 8 * (tau % NT) + 2 * q;
+    const int tau = warp * TPW + u, r = 8 * (tau / NT) + g, j = tau % NT, c = 8 * j + 2 * q;
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-      qpp[r * ldq + c + e] = (ev[u][e] + od[u][e]) * s;
-      qpm[r * ldq + c + e] = (ev[u][e] - od[u][e]) * s;
+      qpp[r * ldq + c + e] = (ev[u][e] + od[u][e]) * s * corr[j][e];
+      qpm[r * ldq + c + e] = (ev[u][e] - od[u][e]) * s * corr[j][e];
     }
   }
 }
@@ -232,7 +288,8 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
   if constexpr (UsePhaseMMA<Gm>::value)
-    phase_products<Gm>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t);
+    // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
+    phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
   else
   for (int e = t; e < NP * NP; e += G) {
     const int r = e / NP, c = e % NP;
@@ -253,7 +310,7 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
     Ppm[e] = spm;
   }
   X.sync();
-  if (t < N) {
+  if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
     const int c = t;
     double sum = 0.0;
     for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
@@ -279,7 +336,7 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
           } else if (l == 1) {
             plm = mu0;
           } else {
-            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) / l;
+            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);  // off the chain
             p0 = p1;
             p1 = plm;
           }
