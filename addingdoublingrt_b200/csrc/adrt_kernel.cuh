@@ -469,13 +469,19 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     }
     op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
     X.sync();
-    *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
+    if (taping) {
+      // (I - R^2)^{-1} into the free T buffer and the record, then TG = T (I - R^2)^{-1}
+      Real* tk = tape + (size_t)k * Tp::STEP;
+      *singular |= op_gj<Gm, GC>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
+                                 oT[cur ^ 1], tk + Tp::OFF_AI);
+      X.sync();
+      op_gemm<Gm>(oTc | kXRowMajor, oT[cur ^ 1], kNoMat, 0, kNoMat, oTG, t);
+    } else {
+      *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
+    }
     X.sync();
     if (taping) {  // the adjoint's record of this step
       Real* tk = tape + (size_t)k * Tp::STEP;
-      // (I - R^2)^{-1} straight to the record; the free T buffer is the scratch
-      *singular |= op_gj<Gm, GC>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
-                                 oT[cur ^ 1], tk + Tp::OFF_AI);
       op_s2g<Gm, GC>(oR, tk + Tp::OFF_R, t);
       op_s2g<Gm, GC>(oTc, tk + Tp::OFF_T, t);
       op_s2g<Gm, GC>(oTG, tk + Tp::OFF_TG, t);  // from column-major: TG^T

@@ -268,7 +268,7 @@ __device__ __forceinline__ void mma_f64_m8n8k4(double& d0, double& d1, double a,
                : "d"(a), "d"(b));
 }
 
-template <class Gm>
+template <class Gm, bool XRM = false>
 __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const double* __restrict__ Y,
                                          const double* add, int id_minus, double* out_rm,
                                          double* out_cm, int t) {
@@ -289,12 +289,13 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
     for (int i = 0; i < WR; ++i)
 #pragma unroll
       for (int j = 0; j < WC; ++j) acc[h][i][j][0] = acc[h][i][j][1] = 0.0;
+  constexpr int sk = XRM ? 1 : LD, sr = XRM ? LD : 1;  // X element (r, k) at XT[k sk + r sr]
 #pragma unroll
   for (int ks = 0; ks < NP / 4; ++ks) {
     const int k = ks * 4 + q;
     double a[WR], b[WC];
 #pragma unroll
-    for (int i = 0; i < WR; ++i) a[i] = XT[k * LD + r0 + i * 8 + g];
+    for (int i = 0; i < WR; ++i) a[i] = XT[k * sk + (r0 + i * 8 + g) * sr];
 #pragma unroll
     for (int j = 0; j < WC; ++j) b[j] = Y[k * LD + c0 + j * 8 + g];
 #pragma unroll
@@ -334,26 +335,32 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
 }
 
 // out = [I -] X Y [+ add] (id_minus = 1), or -X Y [+ add] (id_minus = 2):
-// X column-major (XT[k*LD + r] = X[r][k]), Y and add
-// row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
+// X column-major (XT[k*LD + r] = X[r][k]; row-major when xt_off carries
+// kXRowMajor), Y and add row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
 // alias out_rm (each thread reads its own tile before writing it).
 // Marks an absent optional operand (add / out_rm / out_cm / B / bvec).
 constexpr unsigned kNoMat = 0xffffffffu;
 // As op_gj's right-hand side: the identity (X = A^{-1}).
 constexpr unsigned kIdentity = 0xfffffffeu;
+// Flag on op_gemm's first operand: X given row-major instead of column-major.
+constexpr unsigned kXRowMajor = 1u << 30;
 
 template <class Gm>
 __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned add_off,
                                      int id_minus, unsigned orm_off, unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
-  const Real* __restrict__ XT = sp<Real>(xt_off);
+  const bool xrm = (xt_off & kXRowMajor) != 0;
+  const Real* __restrict__ XT = sp<Real>(xt_off & ~kXRowMajor);
   const Real* __restrict__ Y = sp<Real>(y_off);
   const Real* add = (add_off == kNoMat) ? nullptr : sp<Real>(add_off);
   Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
   Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
   if constexpr (UseMMA<Gm>::value) {
-    gemm_mma<Gm>(XT, Y, add, id_minus, out_rm, out_cm, t);
+    if (xrm)
+      gemm_mma<Gm, true>(XT, Y, add, id_minus, out_rm, out_cm, t);
+    else
+      gemm_mma<Gm, false>(XT, Y, add, id_minus, out_rm, out_cm, t);
     return;
   }
   const Tile<Gm> tl(t);
@@ -368,7 +375,12 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
 #pragma unroll 8
   for (int k = 0; k < NP; ++k) {
     Real xa[TR], yb[TC];
-    lds_vec<Real, TR>(xa, xp + k * LD);
+    if (xrm) {
+#pragma unroll
+      for (int a = 0; a < TR; ++a) xa[a] = XT[tl.row(a) * LD + k];
+    } else {
+      lds_vec<Real, TR>(xa, xp + k * LD);
+    }
     lds_vec<Real, TC>(yb, yp + k * LD);
 #pragma unroll
     for (int a = 0; a < TR; ++a)
