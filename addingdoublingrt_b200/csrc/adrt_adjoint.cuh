@@ -406,8 +406,8 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   //    chain again now (buffers 0..5 and V_*)
   const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
   if (recompute)
-    doubling<Gm>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm, singular,
-                 tape);
+    doubling<Gm, true>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
+                       singular, tape);
   X.sync();
   const double* mu = X.DV(D_MU);
   const double* wt = X.DV(D_WT);

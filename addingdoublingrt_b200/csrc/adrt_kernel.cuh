@@ -378,7 +378,7 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
 // the forward kernel's geometry whatever the group size): R, T, TG, and
 // (I - R^2)^{-1} from a second right-solve against the identity that writes
 // straight to the tape.
-template <class Gm>
+template <class Gm, bool TAPE = false>
 __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
                                      double om, double Bt, double Bb, double tcum, int N,
                                      bool solar, double F0, double mu0, const double* Ppp,
@@ -397,7 +397,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
   const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oTG = X.mo(5);
   const unsigned oT[2] = {X.mo(2), X.mo(3)};
-  const bool taping = (tape != nullptr);
+  constexpr bool taping = TAPE;
   using GC = Geo<NP, Real>;  // record order
   using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);
@@ -469,18 +469,18 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     }
     op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
     X.sync();
-    if (taping) {
+    if constexpr (taping) {
       // (I - R^2)^{-1} into the free T buffer and the record, then TG = T (I - R^2)^{-1}
       Real* tk = tape + (size_t)k * Tp::STEP;
-      *singular |= op_gj<Gm, GC>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t, X.bar,
-                                 oT[cur ^ 1], tk + Tp::OFF_AI);
+      *singular |= op_gj<Gm, GC, true>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t,
+                                       X.bar, oT[cur ^ 1], tk + Tp::OFF_AI);
       X.sync();
-      op_gemm<Gm>(oTc | kXRowMajor, oT[cur ^ 1], kNoMat, 0, kNoMat, oTG, t);
+      op_gemm_xrm<Gm>(oTc, oT[cur ^ 1], kNoMat, oTG, t);
     } else {
       *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
     }
     X.sync();
-    if (taping) {  // the adjoint's record of this step
+    if constexpr (taping) {  // the adjoint's record of this step
       Real* tk = tape + (size_t)k * Tp::STEP;
       op_s2g<Gm, GC>(oR, tk + Tp::OFF_R, t);
       op_s2g<Gm, GC>(oTc, tk + Tp::OFF_T, t);
@@ -527,10 +527,12 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     cur ^= 1;
   }
   X.sync();
-  if (taping && X.warp == 0 && X.lane < NP) {  // tail: the chain's final y, z
-    Real* tl_ = tape + (size_t)nn * Tp::STEP;
-    tl_[X.lane] = X.V(V_Y0 + (nn & 1))[X.lane];
-    tl_[NP + X.lane] = X.V(V_Z0 + (nn & 1))[X.lane];
+  if constexpr (taping) {  // tail: the chain's final y, z
+    if (X.warp == 0 && X.lane < NP) {
+      Real* tl_ = tape + (size_t)nn * Tp::STEP;
+      tl_[X.lane] = X.V(V_Y0 + (nn & 1))[X.lane];
+      tl_[NP + X.lane] = X.V(V_Z0 + (nn & 1))[X.lane];
+    }
   }
   if (X.warp == 0 && X.lane < NP) {
     const int i = X.lane, par = nn & 1;
@@ -1065,8 +1067,12 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
             toff[l] = -1;
           }
         }
-        tcur = doubling<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
-                            Ppp, Ppm, &singular, tape_l);
+        if (tape_l)
+          tcur = doubling<Gm, true>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar,
+                                    F0, mu0, Ppp, Ppm, &singular, tape_l);
+        else
+          tcur = doubling<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0,
+                              mu0, Ppp, Ppm, &singular);
       } else if constexpr (MODE == MODE_MIX_S) {
         tcur = doubling_lam<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0,
                                 mu0, Ppp, Ppm, &singular, nullptr);

@@ -335,32 +335,26 @@ __device__ __forceinline__ void gemm_mma(const double* __restrict__ XT, const do
 }
 
 // out = [I -] X Y [+ add] (id_minus = 1), or -X Y [+ add] (id_minus = 2):
-// X column-major (XT[k*LD + r] = X[r][k]; row-major when xt_off carries
-// kXRowMajor), Y and add row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
+// X column-major (XT[k*LD + r] = X[r][k]), Y and add row-major.  Writes out_rm and/or out_cm (either may be null).  `add` may
 // alias out_rm (each thread reads its own tile before writing it).
 // Marks an absent optional operand (add / out_rm / out_cm / B / bvec).
 constexpr unsigned kNoMat = 0xffffffffu;
 // As op_gj's right-hand side: the identity (X = A^{-1}).
 constexpr unsigned kIdentity = 0xfffffffeu;
-// Flag on op_gemm's first operand: X given row-major instead of column-major.
-constexpr unsigned kXRowMajor = 1u << 30;
+
 
 template <class Gm>
 __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned add_off,
                                      int id_minus, unsigned orm_off, unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
-  const bool xrm = (xt_off & kXRowMajor) != 0;
-  const Real* __restrict__ XT = sp<Real>(xt_off & ~kXRowMajor);
+  const Real* __restrict__ XT = sp<Real>(xt_off);
   const Real* __restrict__ Y = sp<Real>(y_off);
   const Real* add = (add_off == kNoMat) ? nullptr : sp<Real>(add_off);
   Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
   Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
   if constexpr (UseMMA<Gm>::value) {
-    if (xrm)
-      gemm_mma<Gm, true>(XT, Y, add, id_minus, out_rm, out_cm, t);
-    else
-      gemm_mma<Gm, false>(XT, Y, add, id_minus, out_rm, out_cm, t);
+    gemm_mma<Gm, false>(XT, Y, add, id_minus, out_rm, out_cm, t);
     return;
   }
   const Tile<Gm> tl(t);
@@ -375,12 +369,7 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
 #pragma unroll 8
   for (int k = 0; k < NP; ++k) {
     Real xa[TR], yb[TC];
-    if (xrm) {
-#pragma unroll
-      for (int a = 0; a < TR; ++a) xa[a] = XT[tl.row(a) * LD + k];
-    } else {
-      lds_vec<Real, TR>(xa, xp + k * LD);
-    }
+    lds_vec<Real, TR>(xa, xp + k * LD);
     lds_vec<Real, TC>(yb, yp + k * LD);
 #pragma unroll
     for (int a = 0; a < TR; ++a)
@@ -402,6 +391,42 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
     for (int a = 0; a < TR; ++a)
 #pragma unroll
       for (int b = 0; b < TC; ++b) acc[a][b] = ad[a][b] + acc[a][b];
+  }
+  if (out_rm) tl.store_rm(acc, out_rm);
+  if (out_cm) tl.store_cm(acc, out_cm);
+}
+
+// out = X Y with X row-major (the taping doubling's T (I - R^2)^{-1}); kept
+// apart from op_gemm so that the forward's product stays one body.
+template <class Gm>
+__device__ __noinline__ void op_gemm_xrm(unsigned x_off, unsigned y_off, unsigned orm_off,
+                                         unsigned ocm_off, int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
+  const Real* __restrict__ Xr = sp<Real>(x_off);
+  const Real* __restrict__ Y = sp<Real>(y_off);
+  Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+  Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
+  if constexpr (UseMMA<Gm>::value) {
+    gemm_mma<Gm, true>(Xr, Y, nullptr, 0, out_rm, out_cm, t);
+    return;
+  }
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real acc[TR][TC];
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b) acc[a][b] = Real(0);
+  for (int k = 0; k < NP; ++k) {
+    Real yb[TC];
+    lds_vec<Real, TC>(yb, Y + k * LD + tl.cb * TC);
+#pragma unroll
+    for (int a = 0; a < TR; ++a) {
+      const Real xa = Xr[tl.row(a) * LD + k];
+#pragma unroll
+      for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa, yb[b], acc[a][b]);
+    }
   }
   if (out_rm) tl.store_rm(acc, out_rm);
   if (out_cm) tl.store_cm(acc, out_cm);
@@ -515,7 +540,7 @@ struct UseGjMMA {
                                 ((2 * NP / 8) * (NP / 8)) % NW == 0;
 };
 
-template <class Gm, class GO = Gm>
+template <class Gm, class GO = Gm, bool OUTG = false>
 __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, const double* bvec,
                                       double* out_cm, double* out_rm, double* lbuf, double* rbuf,
                                       int t, int bar, double* out_g = nullptr) {
@@ -636,7 +661,7 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
         out_cm[c * LD + r] = acc[u][0];
         out_cm[(c + 1) * LD + r] = acc[u][1];
       }
-      if (out_g) {  // HBM, in the tile order of GO
+      if constexpr (OUTG) {  // HBM, in the tile order of GO
         out_g[tile_index<GO>(r, c)] = acc[u][0];
         out_g[tile_index<GO>(r, c + 1)] = acc[u][1];
       }
@@ -653,8 +678,8 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
 // kIdentity the result is A^{-1}.  The result is written column-major to
 // out_cm and/or row-major to out_rm.  FP64 orders >= 8 take gj_mma (above).
 // Returns nonzero if a pivot was exactly 0.
-// out_g (optional): the result also into HBM, in the tile order of GO.
-template <class Gm, class GO = Gm>
+// OUTG: the result also into HBM (out_g), in the tile order of GO.
+template <class Gm, class GO = Gm, bool OUTG = false>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
                                   int bar, unsigned orm_off = 0xffffffffu,
@@ -674,7 +699,7 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
     Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
     // scratch: the output buffer, or the one matrix buffer the call names
     Real* lbuf = o_cm ? o_cm : out_rm;
-    return gj_mma<Gm, GO>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
+    return gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
   }
   const Tile<Gm> tl(t);
   const bool tv = tl.valid();
@@ -801,7 +826,7 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
 #pragma unroll
         for (int a = 0; a < TR; ++a) out_rm[tl.row(a) * LD + q[b]] = colv[a];
       }
-      if (out_g) {
+      if constexpr (OUTG) {
 #pragma unroll
         for (int a = 0; a < TR; ++a) out_g[tile_index<GO>(tl.row(a), q[b])] = colv[a];
       }
