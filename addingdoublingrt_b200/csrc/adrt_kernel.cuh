@@ -371,13 +371,14 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
 // ------------------------------------------------------------- doubling (reference order)
 // One homogeneous scattering layer (src/doubling.hpp:79-229): first-order
 // thin-layer start at tau0 = tau 2^-nn, then nn doublings of R, T and of the
-// thermal (y, z) and solar sources.  On return R is in m[0] (row-major) and
-// m[1] (column-major), T in m[return value] (row-major, 2 or 3), and the
-// combined thermal + solar sources in V_SUP / V_SDN.  With a tape, every
-// step is recorded for the adjoint (TapeLayout, matrices in the tile order of
-// the forward kernel's geometry whatever the group size): R, T, TG, and
-// (I - R^2)^{-1} from a second right-solve against the identity that writes
-// straight to the tape.
+// thermal (y, z) and solar sources.  Buffers: m0 R (row-major), m1 / m2 T
+// (row-major, ping-pong), m3 I - R^2 then TG R (column-major), m4 TG
+// (column-major).  On return T is in m[return value] (1 or 2) and the
+// combined thermal + solar sources in V_SUP / V_SDN.  With a tape, every step
+// is recorded for the adjoint (TapeLayout, matrices in the tile order of the
+// forward kernel's geometry whatever the group size): R, T, TG, and
+// (I - R^2)^{-1}, which the taping step solves for (straight to the record)
+// and multiplies into TG.
 template <class Gm, bool TAPE = false>
 __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar, double tau,
                                      double om, double Bt, double Bb, double tcum, int N,
@@ -395,13 +396,12 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   const int nn = num_doublings(tau, om);
   const double tau0 = ldexp(tau, -nn);
   const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
-  const unsigned oR = X.mo(0), oRc = X.mo(1), oA = X.mo(4), oTG = X.mo(5);
-  const unsigned oT[2] = {X.mo(2), X.mo(3)};
+  const unsigned oR = X.mo(0), oA = X.mo(3), oTG = X.mo(4);
+  const unsigned oT[2] = {X.mo(1), X.mo(2)};
   constexpr bool taping = TAPE;
   using GC = Geo<NP, Real>;  // record order
   using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);
-  Real* Rcm = sp<Real>(oRc);
   Real* Am = sp<Real>(oA);  // I - R R, then TG R (column-major)
   Real* TGcm = sp<Real>(oTG);
   // thin-layer start (FP64): T = I - tau0 Gpp, R = tau0 Gpm
@@ -427,7 +427,6 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
           Rt[a][b] = static_cast<Real>(rv);
         }
       tl.store_rm(Rt, Rrm);
-      tl.store_cm(Rt, Rcm);
       tl.store_rm(Tt, sp<Real>(oT[0]));
     }
   }
@@ -461,13 +460,13 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     if (solar && X.warp == 0) {  // ru = R sd + gam su, rd = gam R su + sd (old R)
       const Real* vv[2] = {sd, su};
       Real yv[2];
-      matvec<Gm, true, 2>(Rcm, vv, yv, X.lane);
+      matvec<Gm, false, 2>(Rrm, vv, yv, X.lane);
       if (X.lane < NP) {
         X.V(V_RU)[X.lane] = yv[0] + gam * su[X.lane];
         X.V(V_RD)[X.lane] = gam * yv[1] + sd[X.lane];
       }
     }
-    op_gemm<Gm>(oRc, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2
+    op_gemm<Gm, true>(oR, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2 (X = R row-major)
     X.sync();
     if constexpr (taping) {
       // (I - R^2)^{-1} into the free T buffer and the record, then TG = T (I - R^2)^{-1}
@@ -475,7 +474,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
       *singular |= op_gj<Gm, GC, true>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t,
                                        X.bar, oT[cur ^ 1], tk + Tp::OFF_AI);
       X.sync();
-      op_gemm_xrm<Gm>(oTc, oT[cur ^ 1], kNoMat, oTG, t);
+      op_gemm<Gm, true>(oTc, oT[cur ^ 1], kNoMat, 0, kNoMat, oTG, t);
     } else {
       *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
     }
@@ -496,7 +495,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     }
     op_gemm<Gm>(oTG, oR, kNoMat, 0, kNoMat, oA, t);  // TGR = TG R (column-major)
     X.sync();
-    op_gemm<Gm>(oA, oTc, oR, 0, oR, oRc, t);                 // R <- R + TGR T
+    op_gemm<Gm>(oA, oTc, oR, 0, oR, kNoMat, t);              // R <- R + TGR T
     op_gemm<Gm>(oTG, oTc, kNoMat, 0, oT[cur ^ 1], kNoMat, t);  // T <- TG T
     if (X.warp == 0) {
       Real* yn = X.V(V_Y0 + 1 - par);
@@ -548,7 +547,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
     X.V(V_SUP)[i] = static_cast<Real>(up);
     X.V(V_SDN)[i] = static_cast<Real>(dn);
   }
-  return 2 + cur;
+  return 1 + cur;
 }
 
 // ------------------------------------------------------------- doubling (Lambda-split, FP32)
@@ -747,13 +746,13 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
         Td[a][b] = Tf[a][b];
       }
     td.store_rm(Rd, XD.m(0));
-    td.store_rm(Td, XD.m(2));
+    td.store_rm(Td, XD.m(1));
   }
   if (XD.warp == 0 && XD.lane < NP) {
     XD.V(V_SUP)[XD.lane] = src64[XD.lane];
     XD.V(V_SDN)[XD.lane] = src64[NP + XD.lane];
   }
-  return 2;
+  return 1;
 }
 
 // ------------------------------------------------------------- interface output
@@ -1096,19 +1095,25 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
     }
     if (t == 0) rp[3 * TILE + 2 * NP] = Real(scat);
 
-    // adding: top = this layer, bottom = composite (src/adding.hpp:478-490)
-    const unsigned oTl = X.mo(tcur);       // layer T (row-major)
-    const unsigned oSp = X.mo(tcur ^ 1);   // spare matrix
+    // adding: top = this layer, bottom = composite (src/adding.hpp:478-490).
+    // The layer's T is one of the doubling's two T buffers (1 / 2 for the
+    // FP64 forms, 2 / 3 for the FP32 Lambda-split form); the other is spare,
+    // and the two buffers after them take R_b and D1.
+    constexpr int tb0 = (MODE == MODE_MIX_S) ? 2 : 1;
+    if (!scat) tcur = tb0;
+    const unsigned oTl = X.mo(tcur);                 // layer T (row-major)
+    const unsigned oSp = X.mo(2 * tb0 + 1 - tcur);   // spare matrix
+    const unsigned oRb = X.mo(tb0 + 2), oD1 = X.mo(tb0 + 3);
     Real* Rtm = sp<Real>(oTl);
     if (!scat) {
       // non-scattering top (src/adding.hpp:349-406):
       // R_b <- t R_b t, U_b <- s_up + t (U_b + R_b s_dn)
-      op_g2s<Gm>(rb_below, kNoMat, X.mo(4), t);
+      op_g2s<Gm>(rb_below, oRb, kNoMat, t);
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_SDN)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m(4), vv, yv, X.lane);
+        matvec<Gm, false, 1>(sp<Real>(oRb), vv, yv, X.lane);
         if (X.lane < NP) {
           const int i = X.lane;
           X.V(V_UB)[i] = X.V(V_SUP)[i] + X.V(V_T)[i] * (X.V(V_UB)[i] + yv[0]);
@@ -1138,31 +1143,31 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
     } else {
       // general (src/adding.hpp:301-342): A1 = I - R_b R, D1 = T A1^{-1},
       // U_b <- s_up + D1 (U_b + R_b s_dn), R_b <- R + (D1 R_b) T
-      op_g2s<Gm>(rb_below, X.mo(5), X.mo(4), t);  // R_b row-major (m5), column-major (m4)
+      op_g2s<Gm>(rb_below, oRb, kNoMat, t);  // R_b (row-major)
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_SDN)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m(4), vv, yv, X.lane);
+        matvec<Gm, false, 1>(sp<Real>(oRb), vv, yv, X.lane);
         if (X.lane < NP) X.V(V_TMP)[X.lane] = X.V(V_UB)[X.lane] + yv[0];
       }
-      op_gemm<Gm>(X.mo(4), X.mo(0), kNoMat, 1, oSp, kNoMat, t);  // A1
+      op_gemm<Gm, true>(oRb, X.mo(0), kNoMat, 1, oSp, kNoMat, t);  // A1 = I - R_b R
       X.sync();
-      singular |= op_gj<Gm>(oSp, oTl, kNoMat, X.mo(1), X.gjo(), X.redo(), t, X.bar);  // D1 (cm)
+      singular |= op_gj<Gm>(oSp, oTl, kNoMat, oD1, X.gjo(), X.redo(), t, X.bar);  // D1 (cm)
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_TMP)};
         Real yv[1];
-        matvec<Gm, true, 1>(X.m(1), vv, yv, X.lane);
+        matvec<Gm, true, 1>(sp<Real>(oD1), vv, yv, X.lane);
         if (X.lane < NP) X.V(V_UB)[X.lane] = X.V(V_SUP)[X.lane] + yv[0];
       }
-      op_gemm<Gm>(X.mo(1), X.mo(5), kNoMat, 0, kNoMat, oSp, t);  // D1 R_b (cm)
+      op_gemm<Gm>(oD1, oRb, kNoMat, 0, kNoMat, oSp, t);  // D1 R_b (cm)
       X.sync();
-      op_gemm<Gm>(oSp, oTl, X.mo(0), 0, X.mo(4), kNoMat, t);  // R + (D1 R_b) T
+      op_gemm<Gm>(oSp, oTl, X.mo(0), 0, oRb, kNoMat, t);  // R + (D1 R_b) T
       // the tensor-core product writes in fragment order, the copy reads in
       // tile order: other threads' elements must be complete
       X.sync();
-      op_s2g<Gm>(X.mo(4), rp + 2 * TILE, t);
+      op_s2g<Gm>(oRb, rp + 2 * TILE, t);
     }
     if (X.warp == 0) {
       __syncwarp();

@@ -21,13 +21,14 @@
 //
 // Matrices are NP x NP (NP = N rounded up to 4, 8, 16 or 32; padded with the
 // identity/zero blocks, which the algebra keeps exact).  Each thread of the
-// group owns a TR x TC register tile of every matrix; products C = A B are
-// formed tile by tile from operands staged in shared memory (A column-major,
-// B row-major, so every operand load is one contiguous vector).  The
-// (I - R R)^{-1} right-solves are Gauss-Jordan eliminations on the register
-// tiles with column pivoting on the largest |entry| of the pivot row -- the
-// pivot rule of the reference's LU of the transpose (src/matrix.hpp:120-124)
-// -- selected with one warp-wide max-reduction per step.
+// group owns a TR x TC register tile of every matrix.  FP64 products C = A B
+// run on the FP64 tensor cores (mma.sync m8n8k4) from operands staged in
+// shared memory; FP32 products are register-tile FFMA loops.  The
+// (I - R R')^{-1} right-solves are, in FP64, a blocked Gauss-Jordan without
+// pivoting on the tensor cores (gj_mma; the matrices are diagonally dominant),
+// and in FP32 a register-tile Gauss-Jordan with the reference's pivot rule
+// (column pivoting on the largest |entry| of the pivot row, the LU of the
+// transpose of src/matrix.hpp:120-124).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -37,9 +38,6 @@
 
 namespace adrt_dev {
 
-#ifndef ADRT_DPAD
-#define ADRT_DPAD 2
-#endif
 #ifndef ADRT_GEMM_MMA
 #define ADRT_GEMM_MMA 1
 #endif
@@ -74,9 +72,11 @@ struct Geo {
   static constexpr int TC = (NP + CB - 1) / CB;     // tile cols per thread
   static constexpr int TE = TR * TC;
   static constexpr int DIM = (RB * TR > CB * TC) ? RB * TR : CB * TC;
-  // Row padding keeps rows 16-byte aligned and spreads the rows of a column
-  // over the shared-memory banks.
-  static constexpr int PAD = (sizeof(Real) == 8) ? ADRT_DPAD : 4;
+  // Row padding keeps rows 16-byte aligned and spreads rows over the shared-
+  // memory banks: an FP64 pitch of DIM + 4 puts the four k-rows of an m8n8k4
+  // operand load 8 banks apart (row- or column-major), so those loads are
+  // conflict-free.  NP = 32 keeps DIM + 2 so the adjoint's 25 matrices fit.
+  static constexpr int PAD = (sizeof(Real) == 8) ? ((NP_ <= 16) ? 4 : 2) : 4;
   static constexpr int LD = DIM + PAD;
   static constexpr int MAT = DIM * LD;                // Reals per smem matrix
   static constexpr int NW = G / 32;                   // warps per group
@@ -118,7 +118,7 @@ struct TypedLayout {
 
 // Matrix buffers of the reference-order (T-form) doubling and the adding,
 // and of the FP32 Lambda-split doubling.
-constexpr int kMatsTForm = 6;
+constexpr int kMatsTForm = 5;
 constexpr int kMatsLam = 9;
 
 // Vector slots (Real) inside TypedLayout::vecs.
@@ -343,7 +343,9 @@ constexpr unsigned kNoMat = 0xffffffffu;
 constexpr unsigned kIdentity = 0xfffffffeu;
 
 
-template <class Gm>
+// XRM: X given row-major (a separate instantiation; the common product keeps
+// one body).
+template <class Gm, bool XRM = false>
 __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned add_off,
                                      int id_minus, unsigned orm_off, unsigned ocm_off, int t) {
   using Real = typename Gm::Real;
@@ -354,7 +356,7 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
   Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
   Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
   if constexpr (UseMMA<Gm>::value) {
-    gemm_mma<Gm, false>(XT, Y, add, id_minus, out_rm, out_cm, t);
+    gemm_mma<Gm, XRM>(XT, Y, add, id_minus, out_rm, out_cm, t);
     return;
   }
   const Tile<Gm> tl(t);
@@ -369,7 +371,12 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
 #pragma unroll 8
   for (int k = 0; k < NP; ++k) {
     Real xa[TR], yb[TC];
-    lds_vec<Real, TR>(xa, xp + k * LD);
+    if constexpr (XRM) {
+#pragma unroll
+      for (int a = 0; a < TR; ++a) xa[a] = XT[tl.row(a) * LD + k];
+    } else {
+      lds_vec<Real, TR>(xa, xp + k * LD);
+    }
     lds_vec<Real, TC>(yb, yp + k * LD);
 #pragma unroll
     for (int a = 0; a < TR; ++a)
@@ -391,42 +398,6 @@ __device__ __noinline__ void op_gemm(unsigned xt_off, unsigned y_off, unsigned a
     for (int a = 0; a < TR; ++a)
 #pragma unroll
       for (int b = 0; b < TC; ++b) acc[a][b] = ad[a][b] + acc[a][b];
-  }
-  if (out_rm) tl.store_rm(acc, out_rm);
-  if (out_cm) tl.store_cm(acc, out_cm);
-}
-
-// out = X Y with X row-major (the taping doubling's T (I - R^2)^{-1}); kept
-// apart from op_gemm so that the forward's product stays one body.
-template <class Gm>
-__device__ __noinline__ void op_gemm_xrm(unsigned x_off, unsigned y_off, unsigned orm_off,
-                                         unsigned ocm_off, int t) {
-  using Real = typename Gm::Real;
-  constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP;
-  const Real* __restrict__ Xr = sp<Real>(x_off);
-  const Real* __restrict__ Y = sp<Real>(y_off);
-  Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
-  Real* out_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
-  if constexpr (UseMMA<Gm>::value) {
-    gemm_mma<Gm, true>(Xr, Y, nullptr, 0, out_rm, out_cm, t);
-    return;
-  }
-  const Tile<Gm> tl(t);
-  if (!tl.valid()) return;
-  Real acc[TR][TC];
-#pragma unroll
-  for (int a = 0; a < TR; ++a)
-#pragma unroll
-    for (int b = 0; b < TC; ++b) acc[a][b] = Real(0);
-  for (int k = 0; k < NP; ++k) {
-    Real yb[TC];
-    lds_vec<Real, TC>(yb, Y + k * LD + tl.cb * TC);
-#pragma unroll
-    for (int a = 0; a < TR; ++a) {
-      const Real xa = Xr[tl.row(a) * LD + k];
-#pragma unroll
-      for (int b = 0; b < TC; ++b) acc[a][b] = fma(xa, yb[b], acc[a][b]);
-    }
   }
   if (out_rm) tl.store_rm(acc, out_rm);
   if (out_cm) tl.store_cm(acc, out_cm);
