@@ -92,6 +92,22 @@ class Outputs(C.Structure):
     _fields_ = [(f, C.c_void_p) for f in OUTPUT_FIELDS]
 
 
+OUTPUT_F32_FIELDS = OUTPUT_FIELDS  # same order, float pointers
+
+
+class OutputsF32(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f in OUTPUT_F32_FIELDS]
+
+
+RAW_INPUT_FIELDS = ("absorption_coeff", "scattering_coeff", "altitude", "temperature",
+                    "wavenumber", "cloud_optical_depth", "phase_moments")
+
+
+class RawInputs(C.Structure):
+    """adrt_raw_inputs: FP32 coefficient arrays (level 0 = bottom), FP64 wavenumbers."""
+    _fields_ = [(f, C.c_void_p) for f in RAW_INPUT_FIELDS]
+
+
 COTANGENT_FIELDS = ("flux_up", "flux_down", "mean_intensity", "flux_direct")
 GRADIENT_FIELDS = ("delta_tau", "single_scat_albedo", "phase_moments", "temperature",
                    "planck_levels", "surface_emission")

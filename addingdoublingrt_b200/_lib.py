@@ -34,6 +34,7 @@ EXPORTS = (
     "adrt_planck_band",
     "adrt_solve_batch_noalloc",
     "adrt_adjoint",
+    "adrt_solve_batch_raw",
 )
 
 
@@ -75,6 +76,8 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                              C.c_void_p, C.c_void_p]
         lib.adrt_solve_batch_noalloc.argtypes = [P(_abi.BatchDesc), P(_abi.Inputs),
                                                  P(_abi.Outputs), C.c_void_p]
+        lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),
+                                             P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
         lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),
                                      C.c_void_p, P(_abi.Cotangents), P(_abi.Gradients),
                                      C.c_void_p]

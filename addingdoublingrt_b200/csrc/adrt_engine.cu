@@ -391,7 +391,7 @@ int cast_grid(size_t n, int num_sms) {
 
 // adrt_solve_batch after argument checks, with e->mu held.
 int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
-                 const adrt_outputs* out, cudaStream_t s) {
+                 const adrt_outputs* out, cudaStream_t s, const adrt_raw_inputs* raw = nullptr) {
   int rc;
   if ((rc = set_device(e))) return rc;
   e->last_stream = s;
@@ -401,6 +401,14 @@ int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   size_t sb;
   if ((rc = ensure_scratch(e, k, d->num_layers, &grid, &sb))) return rc;
   ColumnDev c0 = make_column(e, d, in, out);
+  if (raw) {
+    c0.raw_abs = raw->absorption_coeff;
+    c0.raw_scat = raw->scattering_coeff;
+    c0.raw_alt = raw->altitude;
+    c0.raw_temp = raw->temperature;
+    c0.raw_cloud = raw->cloud_optical_depth;
+    c0.raw_wn = raw->wavenumber;
+  }
   SolveParams p{};
   p.cols = nullptr;
   p.ncols = 1;
@@ -603,6 +611,78 @@ int adrt_solve_batch_f32(adrt_engine* e, const adrt_batch_desc* d, const adrt_in
   CUDA_TRY(cudaGetLastError());
   if ((rc = check_inputs(d, &din))) return rc;
   if ((rc = solve_locked(e, d, &din, &dout, s))) return rc;
+  for (int i = 0; i < 8; ++i) {
+    if (!fout[i]) continue;
+    narrow_kernel<<<cast_grid(nout[i], e->num_sms), 256, 0, s>>>(doutp[i], fout[i], nout[i]);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return ADRT_OK;
+}
+
+int adrt_solve_batch_raw(adrt_engine* e, const adrt_batch_desc* d0, const adrt_raw_inputs* in,
+                         const adrt_outputs_f32* out, void* stream_ptr) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  if (!d0 || !in || !out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null description, inputs or outputs");
+  if (!in->absorption_coeff || !in->scattering_coeff || !in->altitude || !in->temperature ||
+      !in->wavenumber || !in->phase_moments)
+    return fail(ADRT_ERR_INVALID_ARGUMENT,
+                "raw inputs need absorption and scattering coefficients, altitude, temperature, "
+                "wavenumber and phase moments");
+  // the coefficients carry the sources (single-wavenumber Planck levels) and
+  // their own bottom-first ordering; the moments are ordered from the top
+  adrt_batch_desc d = *d0;
+  d.use_thermal_emission = 0;
+  d.index_from_bottom = 0;
+  d.temperature_per_wavenumber = 0;
+  int rc;
+  {
+    // the skin and top temperatures set single-wavenumber Planck emissions
+    // here; the rest of the description follows the usual rules
+    adrt_batch_desc v = d;
+    v.surface_temperature = -1.0;
+    v.top_temperature = -1.0;
+    if ((rc = check_desc(&v))) return rc;
+  }
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = set_device(e))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  size_t nin[11], nout[8];
+  input_counts(&d, nin);
+  output_counts(&d, nout);
+  const size_t nmom = nin[2];  // phase moments of this layout
+  float* const* fout = &out->flux_up;
+  size_t need = align256(nmom * sizeof(double));
+  for (int i = 0; i < 8; ++i)
+    if (fout[i]) need += align256(nout[i] * sizeof(double));
+  if (need > e->stage_bytes) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE, "FP32 staging buffer too small during stream capture");
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->stage);
+    e->stage = nullptr;
+    e->stage_bytes = 0;
+    if (cudaMalloc(&e->stage, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "FP32 staging allocation of %zu B failed", need);
+    }
+    e->stage_bytes = need;
+  }
+  adrt_inputs din{};
+  adrt_outputs dout{};
+  double* mom = reinterpret_cast<double*>(e->stage);
+  size_t off = align256(nmom * sizeof(double));
+  widen_kernel<<<cast_grid(nmom, e->num_sms), 256, 0, s>>>(in->phase_moments, mom, nmom);
+  din.phase_moments = mom;
+  double** doutp = &dout.flux_up;
+  for (int i = 0; i < 8; ++i) {
+    if (!fout[i]) continue;
+    doutp[i] = reinterpret_cast<double*>(e->stage + off);
+    off += align256(nout[i] * sizeof(double));
+  }
+  CUDA_TRY(cudaGetLastError());
+  if ((rc = solve_locked(e, &d, &din, &dout, s, in))) return rc;
   for (int i = 0; i < 8; ++i) {
     if (!fout[i]) continue;
     narrow_kernel<<<cast_grid(nout[i], e->num_sms), 256, 0, s>>>(doutp[i], fout[i], nout[i]);

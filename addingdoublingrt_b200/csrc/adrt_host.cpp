@@ -284,6 +284,42 @@ void solveBatch(const BatchConfig& config, const DeviceData& data, cudaStream_t 
   check(adrt_solve_batch_f32(thread_engine(), &d, &in, &out, stream));
 }
 
+void solveBatchFromCoefficients(const BatchConfig& config, const RawDeviceData& data,
+                                cudaStream_t stream) {
+  const adrt_batch_desc d = to_desc(config, data.phase_moments_shared);
+  adrt_raw_inputs in{};
+  in.absorption_coeff = data.absorption_coeff;
+  in.scattering_coeff = data.scattering_coeff;
+  in.altitude = data.altitude;
+  in.temperature = data.temperature;
+  in.wavenumber = data.wavenumber;
+  in.cloud_optical_depth = data.cloud_optical_depth;
+  in.phase_moments = data.phase_moments;
+  adrt_outputs_f32 out{};
+  out.toa_flux_up = data.flux_up;
+  out.toa_flux_down = data.flux_down;
+  out.boa_flux_direct = data.flux_direct;
+  check(adrt_solve_batch_raw(thread_engine(), &d, &in, &out, stream));
+}
+
+void solveBatchFromCoefficients(const BatchConfig& config, const RawDeviceData& data,
+                                SolverWorkspaceGPU& workspace, cudaStream_t stream) {
+  workspace.allocate(config.num_wavenumbers, config.num_layers);
+  solveBatchFromCoefficients(config, data, stream);
+}
+
+// The engine forms the intermediate quantities inside its solve, so the
+// workspace only records the dimensions it was sized for.
+void SolverWorkspaceGPU::allocate(int nwav, int nlay) {
+  allocated_nwav = nwav;
+  allocated_nlay = nlay;
+}
+
+void SolverWorkspaceGPU::free() {
+  allocated_nwav = 0;
+  allocated_nlay = 0;
+}
+
 HostResult solveBatchHost(const BatchConfig& config, const std::vector<float>& delta_tau,
                           const std::vector<float>& single_scat_albedo,
                           const std::vector<float>& phase_moments, bool phase_moments_shared,

@@ -811,6 +811,10 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
   const double wlo = C->wlo_w ? C->wlo_w[w] : C->wn_lo;
   const double whi = C->whi_w ? C->whi_w[w] : C->wn_hi;
   const Levels lv(slot, lmax);
+  // raw coefficients (src_cuda/cuda_solver.cu:175-221, 1131-1186): levels and
+  // layers counted from the bottom, single-wavenumber Planck levels
+  const bool raw = (C->raw_abs != nullptr);
+  const double nu = raw ? C->raw_wn[w] : 0.0;
 
   if (t < NP) {
     double mu = 1.0, wt = 0.0;
@@ -827,7 +831,11 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
   for (int l = t; l <= nL; l += G) {
     const int ul = from_bottom ? nL - l : l;
     double Bv = 0.0;
-    if (C->thermal) {
+    if (raw) {
+      const double Tv = C->raw_temp[nL - l];
+      if (!(Tv >= 0.0)) bad = 1;
+      Bv = planck_single(Tv, nu);
+    } else if (C->thermal) {
       const double Tv = C->temperature[(C->temp_per_wav ? (size_t)w * (nL + 1) : 0) + ul];
       if (!(Tv >= 0.0)) bad = 1;
       Bv = planck_band(wlo, whi, Tv);
@@ -840,8 +848,23 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
   unsigned flagged = 0;
   for (int l = t; l < nL; l += G) {
     const int u = from_bottom ? nL - 1 - l : l;
-    double tau = C->dtau[(size_t)w * nL + u];
-    double om = C->ssa[(size_t)w * nL + u];
+    double tau, om;
+    if (raw) {
+      // trapezoid over the layer's two levels, plus the cloud's optical depth
+      const int b = nL - 1 - l;
+      const size_t W = C->W;
+      const double dz = (double)C->raw_alt[b + 1] - (double)C->raw_alt[b];
+      const double ab = C->raw_abs[b * W + w], at = C->raw_abs[(b + 1) * W + w];
+      const double sb = C->raw_scat[b * W + w], st = C->raw_scat[(b + 1) * W + w];
+      tau = dz * ((at + st) + (ab + sb)) * 0.5;
+      const double sdep = dz * (st + sb) * 0.5;
+      if (C->raw_cloud) tau += C->raw_cloud[b * W + w];
+      if (tau < 0.0) tau = 0.0;
+      om = (tau > 0.0) ? sdep / tau : 0.0;
+    } else {
+      tau = C->dtau[(size_t)w * nL + u];
+      om = C->ssa[(size_t)w * nL + u];
+    }
     if (!(tau >= 0.0 && tau < 1e300) || !(om >= 0.0 && om <= 1.0)) bad = 1;
     lv.omu[l] = om;
     if (om > 0.0 && tau > 0.0 && C->delta_m && M > 2 * N) {
@@ -881,7 +904,10 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
       lv.tc[l + 1] = tc;
     }
     double Bs, Btop;
-    if (C->thermal) {
+    if (raw) {
+      Bs = (C->surface_temperature >= 0.0) ? planck_single(C->surface_temperature, nu) : lv.B[nL];
+      Btop = (C->top_temperature >= 0.0) ? planck_single(C->top_temperature, nu) : lv.B[0];
+    } else if (C->thermal) {
       Bs = (C->surface_temperature >= 0.0) ? planck_band(wlo, whi, C->surface_temperature)
                                            : lv.B[nL];
       Btop = (C->top_temperature >= 0.0) ? planck_band(wlo, whi, C->top_temperature) : lv.B[0];

@@ -955,6 +955,16 @@ __host__ __device__ inline double planck_band(double wnumlo, double wnumhi, doub
   return (ans == 0.0) ? 0.0 : ans;
 }
 
+// Single-wavenumber Planck function of the raw-coefficient entry point,
+// B(T, nu) = c1 nu^3 / (exp(c2 nu / T) - 1) with c1 = 2 h c^2 = 1.19105e-8
+// W m^-2 cm (CGS with the 1e-3 unit factor) and c2 = h c / k = 1.43879 cm K,
+// zero below 1e-5 K (src_cuda/cuda_planck_single.cuh:19-35; evaluated in FP64).
+__host__ __device__ inline double planck_single(double temp, double nu) {
+  const double c1 = 1.19105e-08, c2 = 1.43879;
+  if (temp < 1e-5) return 0.0;
+  return c1 * nu * nu * nu / (exp(c2 * nu / temp) - 1.0);
+}
+
 // Extra doublings from omega (src/doubling.hpp:20-26).
 __device__ __forceinline__ int ipow0(double omega) {
   return omega < 0.01 ? 4 : (omega < 0.1 ? 10 : 16);

@@ -31,6 +31,12 @@ struct ColumnDev {
   const double *dtau, *ssa, *moments, *temperature, *planck;
   const double *albedo_w, *mu0_w, *wlo_w, *whi_w, *semis_w, *temis_w;
   double *fu, *fd, *fdir, *J, *divF, *toa_fu, *toa_fd, *boa_fdir;
+  // raw retrieval inputs (all null unless the batch is given as coefficients):
+  // level-major [(L+1) x W] absorption / scattering coefficients, altitude
+  // and temperature [L+1], cloud optical depth [L x W] (or null), level and
+  // layer 0 at the bottom; wavenumber [W]
+  const float *raw_abs, *raw_scat, *raw_alt, *raw_temp, *raw_cloud;
+  const double* raw_wn;
   QuadDev quad;
   long long task_begin;  // first flattened task index of this column
 };

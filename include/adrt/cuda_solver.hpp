@@ -91,5 +91,58 @@ HostResult solveBatchHost(const BatchConfig& config, const std::vector<float>& d
                           const std::vector<float>& planck_levels,
                           const std::vector<float>& temperature = {});
 
+// ---------------------------------------------------------------- raw inputs
+/// Raw retrieval inputs (caller-owned device memory), as the reference's
+/// RawDeviceData (src_cuda/cuda_solver.cuh:104-133): coefficient arrays are
+/// level-major, array[level * nwav + wav], with the bottom of the atmosphere
+/// at level 0; the phase moments keep the solver's top-first layer order.
+struct RawDeviceData {
+  const float* absorption_coeff;     ///< [nlev * nwav] absorption coefficient (cm^-1)
+  const float* scattering_coeff;     ///< [nlev * nwav] scattering coefficient (cm^-1)
+  const float* altitude;             ///< [nlev] altitude (cm), bottom first
+  const float* temperature;          ///< [nlev] temperature (K), bottom first
+  const double* wavenumber;          ///< [nwav] wavenumber (cm^-1)
+
+  const float* phase_moments;        ///< [nlay * nmom] or [nwav * nlay * nmom]
+  bool phase_moments_shared = false;
+
+  const float* cloud_optical_depth = nullptr;  ///< [nlay * nwav] or nullptr
+
+  float* flux_up = nullptr;      ///< [nwav] TOA upward flux (x spectrum_scaling)
+  float* flux_down = nullptr;    ///< [nwav] TOA downward flux
+  float* flux_direct = nullptr;  ///< [nwav] direct solar flux at the surface, or nullptr
+};
+
+/// Workspace of the reference's preprocessing path
+/// (src_cuda/cuda_solver.cuh:137-156), kept for source compatibility.  The
+/// engine forms optical depths, albedos and Planck levels inside its solve and
+/// needs no intermediate arrays: allocate() only records the dimensions, and
+/// the pointers stay null.
+struct SolverWorkspaceGPU {
+  float* delta_tau = nullptr;           ///< [nwav * nlay]
+  float* single_scat_albedo = nullptr;  ///< [nwav * nlay]
+  float* planck_levels = nullptr;       ///< [nwav * nlev]
+  float* surface_emission = nullptr;    ///< [nwav]
+  float* top_emission = nullptr;        ///< [nwav]
+  int allocated_nwav = 0;
+  int allocated_nlay = 0;
+
+  void allocate(int nwav, int nlay);
+  void free();
+  ~SolverWorkspaceGPU() { free(); }
+};
+
+/// Solve from raw coefficients (src_cuda/cuda_solver.cuh:166-169): optical
+/// depths by the trapezoid rule over altitude plus the cloud optical depth,
+/// single-scattering albedos and single-wavenumber Planck levels are formed in
+/// the solve.  Any N (the reference's overload without a workspace takes N <= 8).
+void solveBatchFromCoefficients(const BatchConfig& config, const RawDeviceData& data,
+                                cudaStream_t stream = 0);
+
+/// The reference's workspace overload (src_cuda/cuda_solver.cuh:175-179): same
+/// results as the overload without a workspace.
+void solveBatchFromCoefficients(const BatchConfig& config, const RawDeviceData& data,
+                                SolverWorkspaceGPU& workspace, cudaStream_t stream = 0);
+
 }  // namespace cuda
 }  // namespace adrt

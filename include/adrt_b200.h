@@ -205,6 +205,36 @@ int adrt_solve_batch_f32(adrt_engine* engine, const adrt_batch_desc* desc,
                          const adrt_inputs_f32* in, const adrt_outputs_f32* out,
                          void* cuda_stream);
 
+/* Raw retrieval inputs (device, FP32 as the reference's RawDeviceData,
+ * src_cuda/cuda_solver.cuh:104-133).  Levels and layers of the coefficient
+ * arrays are counted from the bottom of the atmosphere (level 0 = BOA); the
+ * phase moments keep the solver's top-first layer order. */
+typedef struct adrt_raw_inputs {
+  const float* absorption_coeff;     /* [(L+1) * W] level-major, cm^-1 */
+  const float* scattering_coeff;     /* [(L+1) * W] level-major, cm^-1 */
+  const float* altitude;             /* [L+1] cm */
+  const float* temperature;          /* [L+1] K */
+  const double* wavenumber;          /* [W] cm^-1 */
+  const float* cloud_optical_depth;  /* [L * W] layer-major, or NULL */
+  const float* phase_moments;        /* per desc->moment_layout; layer 0 = top */
+} adrt_raw_inputs;
+
+/* Batched solve from raw absorption / scattering coefficients: replaces
+ * adrt::cuda::solveBatchFromCoefficients (src_cuda/cuda_solver.cuh:166-179,
+ * src_cuda/cuda_solver.cu:1193-1353).  Layer optical depths by the trapezoid
+ * rule over altitude (plus the cloud optical depth), single-scattering albedo
+ * = scattering depth / optical depth, and single-wavenumber Planck levels are
+ * formed inside the solve's prologue (no intermediate arrays); the surface
+ * emits B(T_BOA) (or B(surface_temperature) when >= 0) and the top sees
+ * B(T_TOA) (or B(top_temperature) when >= 0).  desc's use_thermal_emission,
+ * index_from_bottom and temperature_per_wavenumber are ignored.  Outputs as
+ * adrt_solve_batch_f32 (the reference writes toa_flux_up, toa_flux_down and
+ * boa_flux_direct).  Any N (the reference's workspace-free overload takes
+ * N <= 8). */
+int adrt_solve_batch_raw(adrt_engine* engine, const adrt_batch_desc* desc,
+                         const adrt_raw_inputs* in, const adrt_outputs_f32* out,
+                         void* cuda_stream);
+
 /* Validate a batch description and (host) inputs with the rules of
  * ADConfig::validate() (src/adding_doubling.hpp:123-174) applied to every
  * wavenumber.  Returns ADRT_ERR_INVALID_ARGUMENT with a detail message. */

@@ -151,3 +151,45 @@ def norm_error(x: np.ndarray, ref: np.ndarray, per: int) -> float:
     scale = np.max(np.abs(ref), axis=1, keepdims=True)
     scale[scale == 0.0] = 1.0
     return float(np.max(np.abs(x - ref) / scale))
+
+
+def planck_single(temp, nu):
+    """Single-wavenumber Planck function of the raw entry point,
+    c1 nu^3 / (exp(c2 nu / T) - 1), c1 = 1.19105e-8, c2 = 1.43879, zero below
+    1e-5 K (src_cuda/cuda_planck_single.cuh:19-35), in FP64."""
+    temp = np.asarray(temp, dtype=np.float64)
+    nu = np.asarray(nu, dtype=np.float64)
+    with np.errstate(over="ignore", divide="ignore"):
+        b = 1.19105e-08 * nu ** 3 / np.expm1(1.43879 * nu / np.where(temp < 1e-5, 1.0, temp))
+    return np.where(temp < 1e-5, 0.0, b)
+
+
+def raw_preprocess(absorption, scattering, altitude, temperature, wavenumber, cloud=None,
+                   surface_temperature=-1.0, top_temperature=-1.0) -> dict:
+    """FP64 restatement of the reference's raw-coefficient preprocessing
+    (src_cuda/cuda_solver.cu:1131-1186, and the inline path :175-249, :428-440):
+    coefficient arrays [(L+1), W] with level 0 at the bottom, altitude and
+    temperature [L+1] bottom first, cloud optical depth [L, W] bottom first.
+    Returns the solver's top-first arrays: delta_tau and single_scat_albedo
+    [W, L], planck_levels [W, L+1], surface_emission and top_emission [W]."""
+    ab = np.asarray(absorption, dtype=np.float64)
+    sc = np.asarray(scattering, dtype=np.float64)
+    alt = np.asarray(altitude, dtype=np.float64)
+    tmp = np.asarray(temperature, dtype=np.float64)
+    nu = np.asarray(wavenumber, dtype=np.float64)
+    L = alt.size - 1
+    dz = (alt[1:] - alt[:-1])[:, None]                      # [L, 1] bottom first
+    ext = ab + sc
+    tau = dz * (ext[1:] + ext[:-1]) * 0.5                    # [L, W]
+    sdep = dz * (sc[1:] + sc[:-1]) * 0.5
+    if cloud is not None:
+        tau = tau + np.asarray(cloud, dtype=np.float64)
+    tau = np.maximum(tau, 0.0)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ssa = np.where(tau > 0.0, sdep / np.where(tau > 0.0, tau, 1.0), 0.0)
+    B = planck_single(tmp[::-1][None, :], nu[:, None])      # [W, L+1] top first
+    surf = planck_single(surface_temperature, nu) if surface_temperature >= 0.0 else B[:, L]
+    top = planck_single(top_temperature, nu) if top_temperature >= 0.0 else B[:, 0]
+    return {"delta_tau": tau[::-1].T.copy(), "single_scat_albedo": ssa[::-1].T.copy(),
+            "planck_levels": B, "surface_emission": np.asarray(surf, dtype=np.float64),
+            "top_emission": np.asarray(top, dtype=np.float64)}
