@@ -147,6 +147,11 @@ KernInfo pick(int n, int precision) {
 
 }  // namespace
 
+// The host entry splits batches of at least 2 x kHostChunkMin wavenumbers into
+// up to four chunks so that the copies overlap the solves; a chunk then keeps
+// every resident thread group busy for several wavenumbers.
+constexpr size_t kHostChunkMin = 8192;
+
 struct adrt_engine {
   int device = 0;
   int num_sms = 0;
@@ -170,8 +175,13 @@ struct adrt_engine {
   // FP64 staging of the FP32 entry point (grows outside stream capture only)
   char* stage = nullptr;
   size_t stage_bytes = 0;
-  // host-entry staging buffers
-  std::vector<void*> host_stage;
+  // host entry: device staging (grows only), copy-in / solve / copy-out
+  // streams and the events of two chunk buffers
+  char* hstage = nullptr;
+  size_t hstage_bytes = 0;
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t hev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  std::mutex hmu;  // one host-entry call at a time per engine
   std::mutex mu;
 };
 
@@ -474,7 +484,11 @@ int adrt_engine_destroy(adrt_engine* e) {
   if (e->h_cols) cudaFreeHost(e->h_cols);
   if (e->cols_copied) cudaEventDestroy(e->cols_copied);
   for (auto& q : e->quad) cudaFree(q.buf);
-  for (void* p : e->host_stage) cudaFree(p);
+  cudaFree(e->hstage);
+  for (auto& st : e->hs)
+    if (st) cudaStreamDestroy(st);
+  for (auto& ev : e->hev)
+    if (ev) cudaEventDestroy(ev);
   cudaFree(e->stage);
   cudaFree(e->adj_scratch);
   delete e;
@@ -988,69 +1002,133 @@ int adrt_solve_batch_host(adrt_engine* e, const adrt_batch_desc* d, const adrt_i
   if (rc) return rc;
   if ((rc = check_inputs(d, hin))) return rc;
   if (!hout) return fail(ADRT_ERR_INVALID_ARGUMENT, "null outputs");
+  std::lock_guard<std::mutex> hl(e->hmu);
   {
     std::lock_guard<std::mutex> lk(e->mu);
     if ((rc = set_device(e))) return rc;
   }
+  // Arrays split by wavenumber into chunks (per-wavenumber arrays) or copied
+  // once (shared moments, a common temperature profile).  Chunk i is copied
+  // in on hs[0], solved on hs[1] and copied out on hs[2], into one of two
+  // buffer sets, so the copies of one chunk overlap the solves of its
+  // neighbours; hev[b] / hev[2+b] / hev[4+b] mark buffer set b's copy-in,
+  // solve and copy-out.
   const size_t W = d->num_wavenumbers, L = d->num_layers, M = d->num_moments;
-  size_t nmom = d->moment_layout == ADRT_MOMENTS_SHARED ? L * M
-                : d->moment_layout == ADRT_MOMENTS_PER_WAVENUMBER ? W * M : W * L * M;
+  const bool mom_w = d->moment_layout != ADRT_MOMENTS_SHARED;
+  const size_t mom_per = d->moment_layout == ADRT_MOMENTS_PER_WAVENUMBER ? M : L * M;
   struct Arr {
     const double* h;
-    size_t n;
+    size_t per;   // elements per wavenumber, or total elements when shared
+    bool per_w;
   };
-  const Arr ins[11] = {{hin->delta_tau, W * L},
-                       {hin->single_scat_albedo, W * L},
-                       {hin->phase_moments, nmom},
-                       {hin->temperature, (d->temperature_per_wavenumber ? W : 1) * (L + 1)},
-                       {hin->planck_levels, W * (L + 1)},
-                       {hin->surface_albedo, W},
-                       {hin->solar_mu, W},
-                       {hin->wavenumber_low, W},
-                       {hin->wavenumber_high, W},
-                       {hin->surface_emission, W},
-                       {hin->top_emission, W}};
+  const Arr ins[11] = {{hin->delta_tau, L, true},
+                       {hin->single_scat_albedo, L, true},
+                       {hin->phase_moments, mom_w ? mom_per : L * M, mom_w},
+                       {hin->temperature, L + 1, d->temperature_per_wavenumber != 0},
+                       {hin->planck_levels, L + 1, true},
+                       {hin->surface_albedo, 1, true},
+                       {hin->solar_mu, 1, true},
+                       {hin->wavenumber_low, 1, true},
+                       {hin->wavenumber_high, 1, true},
+                       {hin->surface_emission, 1, true},
+                       {hin->top_emission, 1, true}};
   double* const* outs_h = &hout->flux_up;
-  const size_t out_n[8] = {W * (L + 1), W * (L + 1), W * (L + 1), W * (L + 1),
-                           W * (L + 1), W, W, W};
-  size_t total = 0;
-  for (const auto& a : ins)
-    if (a.h) total += (a.n * sizeof(double) + 255) & ~size_t(255);
-  for (int i = 0; i < 8; ++i)
-    if (outs_h[i]) total += (out_n[i] * sizeof(double) + 255) & ~size_t(255);
-  char* dbuf = nullptr;
-  if (cudaMalloc(&dbuf, total) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(ADRT_ERR_OUT_OF_MEMORY, "host-entry staging allocation of %zu B failed", total);
+  const size_t out_per[8] = {L + 1, L + 1, L + 1, L + 1, L + 1, 1, 1, 1};
+  const int nchunks = (int)std::max<size_t>(1, std::min<size_t>(4, W / kHostChunkMin));
+  const size_t wc = (W + nchunks - 1) / nchunks;
+  auto a256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t shared_b = 0, set_b = 0;
+  for (const auto& a : ins) {
+    if (!a.h) continue;
+    if (a.per_w)
+      set_b += a256(wc * a.per * sizeof(double));
+    else
+      shared_b += a256(a.per * sizeof(double));
   }
-  cudaStream_t s = nullptr;
-  adrt_inputs din{};
-  adrt_outputs dout{};
-  const double** din_p = &din.delta_tau;
-  double** dout_p = &dout.flux_up;
+  for (int i = 0; i < 8; ++i)
+    if (outs_h[i]) set_b += a256(wc * out_per[i] * sizeof(double));
+  const int nsets = nchunks > 1 ? 2 : 1;
+  const size_t total = shared_b + nsets * set_b;
+  if (!e->hs[0]) {
+    for (auto& st : e->hs) CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    for (auto& ev : e->hev) CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  }
+  if (total > e->hstage_bytes) {
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->hstage);
+    e->hstage = nullptr;
+    e->hstage_bytes = 0;
+    if (cudaMalloc(&e->hstage, total) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "host-entry staging allocation of %zu B failed", total);
+    }
+    e->hstage_bytes = total;
+  }
+  cudaStream_t sin = e->hs[0], scmp = e->hs[1], sout = e->hs[2];
+  const double* shared_d[11] = {};
   size_t off = 0;
   rc = ADRT_OK;
   for (int i = 0; i < 11 && rc == ADRT_OK; ++i) {
-    if (!ins[i].h) continue;
-    double* dp = reinterpret_cast<double*>(dbuf + off);
-    off += (ins[i].n * sizeof(double) + 255) & ~size_t(255);
-    if (cudaMemcpyAsync(dp, ins[i].h, ins[i].n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    if (!ins[i].h || ins[i].per_w) continue;
+    double* dp = reinterpret_cast<double*>(e->hstage + off);
+    off += a256(ins[i].per * sizeof(double));
+    if (cudaMemcpyAsync(dp, ins[i].h, ins[i].per * sizeof(double), cudaMemcpyHostToDevice,
+                        sin) != cudaSuccess)
       rc = fail(ADRT_ERR_CUDA, "host-to-device copy failed");
-    din_p[i] = dp;
+    shared_d[i] = dp;
   }
-  for (int i = 0; i < 8 && rc == ADRT_OK; ++i) {
-    if (!outs_h[i]) continue;
-    dout_p[i] = reinterpret_cast<double*>(dbuf + off);
-    off += (out_n[i] * sizeof(double) + 255) & ~size_t(255);
+  const size_t set0 = off;
+  for (int c = 0; c < nchunks && rc == ADRT_OK; ++c) {
+    const size_t w0 = c * wc, n = std::min(wc, W - w0);
+    if (n == 0) break;
+    const int b = c % nsets;
+    char* base = e->hstage + set0 + b * set_b;
+    adrt_inputs din{};
+    adrt_outputs dout{};
+    const double** din_p = &din.delta_tau;
+    double** dout_p = &dout.flux_up;
+    size_t o = 0;
+    // copy-in of this set waits for the solve that last read it
+    if (c >= nsets) CUDA_TRY(cudaStreamWaitEvent(sin, e->hev[2 + b], 0));
+    for (int i = 0; i < 11 && rc == ADRT_OK; ++i) {
+      if (!ins[i].h) continue;
+      if (!ins[i].per_w) {
+        din_p[i] = shared_d[i];
+        continue;
+      }
+      double* dp = reinterpret_cast<double*>(base + o);
+      o += a256(wc * ins[i].per * sizeof(double));
+      if (cudaMemcpyAsync(dp, ins[i].h + w0 * ins[i].per, n * ins[i].per * sizeof(double),
+                          cudaMemcpyHostToDevice, sin) != cudaSuccess)
+        rc = fail(ADRT_ERR_CUDA, "host-to-device copy failed");
+      din_p[i] = dp;
+    }
+    for (int i = 0; i < 8; ++i) {
+      if (!outs_h[i]) continue;
+      dout_p[i] = reinterpret_cast<double*>(base + o);
+      o += a256(wc * out_per[i] * sizeof(double));
+    }
+    if (rc != ADRT_OK) break;
+    CUDA_TRY(cudaEventRecord(e->hev[b], sin));
+    // the solve waits for its inputs and for the copy-out of this set's last chunk
+    CUDA_TRY(cudaStreamWaitEvent(scmp, e->hev[b], 0));
+    if (c >= nsets) CUDA_TRY(cudaStreamWaitEvent(scmp, e->hev[4 + b], 0));
+    adrt_batch_desc dc = *d;
+    dc.num_wavenumbers = (int)n;
+    if ((rc = adrt_solve_batch(e, &dc, &din, &dout, scmp))) break;
+    CUDA_TRY(cudaEventRecord(e->hev[2 + b], scmp));
+    CUDA_TRY(cudaStreamWaitEvent(sout, e->hev[2 + b], 0));
+    for (int i = 0; i < 8 && rc == ADRT_OK; ++i) {
+      if (!outs_h[i]) continue;
+      if (cudaMemcpyAsync(outs_h[i] + w0 * out_per[i], dout_p[i], n * out_per[i] * sizeof(double),
+                          cudaMemcpyDeviceToHost, sout) != cudaSuccess)
+        rc = fail(ADRT_ERR_CUDA, "device-to-host copy failed");
+    }
+    CUDA_TRY(cudaEventRecord(e->hev[4 + b], sout));
   }
-  if (rc == ADRT_OK) rc = adrt_solve_batch(e, d, &din, &dout, s);
-  for (int i = 0; i < 8 && rc == ADRT_OK; ++i) {
-    if (!outs_h[i]) continue;
-    if (cudaMemcpyAsync(outs_h[i], dout_p[i], out_n[i] * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-      rc = fail(ADRT_ERR_CUDA, "device-to-host copy failed");
-  }
-  cudaError_t se = cudaStreamSynchronize(s);
-  cudaFree(dbuf);
+  cudaError_t se = cudaStreamSynchronize(sout);
+  if (se == cudaSuccess) se = cudaStreamSynchronize(scmp);
+  if (se == cudaSuccess) se = cudaStreamSynchronize(sin);
   if (rc == ADRT_OK && se != cudaSuccess)
     rc = fail(ADRT_ERR_CUDA, "solve failed: %s", cudaGetErrorString(se));
   return rc;

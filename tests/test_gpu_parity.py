@@ -197,6 +197,29 @@ def test_host_entry_equals_device_entry(eng):
         assert np.array_equal(dev[k], host[k]), k
 
 
+@pytest.mark.parametrize("layout", [_abi.MOMENTS_SHARED, _abi.MOMENTS_PER_WAVENUMBER])
+def test_chunked_host_entry_equals_device_entry(eng, layout):
+    """A batch large enough for the host entry's overlapped chunks (and not a
+    multiple of their count), shared or per-wavenumber moments, one shared
+    temperature profile: every output equals the device entry's bit for bit."""
+    W, L, N, M = 37_003, 12, 8, 16
+    rng = np.random.default_rng(11 + layout)
+    d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
+                       moment_layout=layout, use_thermal_emission=1,
+                       wavenumber_low=900.0, wavenumber_high=905.0, solar_flux=1.0,
+                       solar_mu=0.5, surface_albedo=0.1)
+    b = workloads.Batch(d)
+    b.set("delta_tau", 10.0 ** rng.uniform(-3, 0.5, (W, L)))
+    b.set("single_scat_albedo", rng.uniform(0.0, 0.95, (W, L)))
+    b.set("phase_moments", workloads.hg_moments(rng.uniform(0.2, 0.8, L if layout == 0 else W),
+                                                M))
+    b.set("temperature", np.linspace(200.0, 300.0, L + 1))
+    dev = run_device(eng, b)
+    host = eng.solve_host(b)
+    for k in _abi.OUTPUT_FIELDS:
+        assert np.array_equal(dev[k], host[k]), k
+
+
 def test_toa_outputs_and_spectrum_scaling(eng):
     b = workloads.config1(W=16)
     b.desc.spectrum_scaling = 0.25
