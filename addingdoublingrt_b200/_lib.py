@@ -35,6 +35,8 @@ EXPORTS = (
     "adrt_solve_batch_noalloc",
     "adrt_adjoint",
     "adrt_solve_batch_raw",
+    "adrt_adjoint_host",
+    "adrt_planck_band_deriv",
 )
 
 
@@ -72,10 +74,14 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         lib.adrt_probe_fma_tflops.argtypes = [P(C.c_double), P(C.c_double)]
         lib.adrt_gauss_legendre.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         lib.adrt_planck_band.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double)]
+        lib.adrt_planck_band_deriv.argtypes = [C.c_double, C.c_double, C.c_double,
+                                               P(C.c_double)]
         lib.adrt_solve_batch_f32.argtypes = [C.c_void_p, P(_abi.BatchDesc), C.c_void_p,
                                              C.c_void_p, C.c_void_p]
         lib.adrt_solve_batch_noalloc.argtypes = [P(_abi.BatchDesc), P(_abi.Inputs),
                                                  P(_abi.Outputs), C.c_void_p]
+        lib.adrt_adjoint_host.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),
+                                          P(_abi.Cotangents), P(_abi.Gradients)]
         lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),
                                              P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
         lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),

@@ -1285,7 +1285,10 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       bBs = pub;
     }
     if (C->thermal) {
-      if (C->surface_temperature < 0.0) bB[nL] += bBs;
+      if (C->surface_temperature < 0.0)
+        bB[nL] += bBs;  // the surface emits B(T_L)
+      else if (AD.g_semis)
+        AD.g_semis[w] = bBs;  // d L / d B(surface_temperature)
       if (C->top_temperature < 0.0) bB[0] += pBtop;
     } else if (AD.g_semis) {
       AD.g_semis[w] = bBs;

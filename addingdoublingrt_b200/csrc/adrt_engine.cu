@@ -722,6 +722,14 @@ int adrt_planck_band(double lo, double hi, double temp, double* out) {
   return ADRT_OK;
 }
 
+int adrt_planck_band_deriv(double lo, double hi, double temp, double* out) {
+  if (!out) return fail(ADRT_ERR_INVALID_ARGUMENT, "null output");
+  if (temp < 0.0 || hi < lo || lo < 0.0)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "planckFunctionDeriv: invalid arguments");
+  *out = planck_band_deriv(lo, hi, temp);
+  return ADRT_OK;
+}
+
 int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
                  const adrt_outputs* out, const adrt_cotangents* cot, const adrt_gradients* gr,
                  void* stream_ptr) {
@@ -729,9 +737,13 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   int rc = check_desc(d);
   if (rc) return rc;
   if ((rc = check_inputs(d, in))) return rc;
-  if (d->use_delta_m && d->num_moments > 2 * d->num_quadrature)
+  // with delta-M truncation the source gradients stand, but those with respect
+  // to the unscaled optical properties and moments are not formed
+  if (d->use_delta_m && d->num_moments > 2 * d->num_quadrature &&
+      (gr->delta_tau || gr->single_scat_albedo || gr->phase_moments))
     return fail(ADRT_ERR_UNSUPPORTED,
-                "adjoint: delta-M truncation (use_delta_m with num_moments > 2N) is not supported");
+                "adjoint: with delta-M truncation (use_delta_m, num_moments > 2N) only "
+                "temperature, planck_levels and surface_emission gradients are formed");
   std::lock_guard<std::mutex> lk(e->mu);
   if ((rc = set_device(e))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
@@ -1131,6 +1143,84 @@ int adrt_solve_batch_host(adrt_engine* e, const adrt_batch_desc* d, const adrt_i
   if (se == cudaSuccess) se = cudaStreamSynchronize(sin);
   if (rc == ADRT_OK && se != cudaSuccess)
     rc = fail(ADRT_ERR_CUDA, "solve failed: %s", cudaGetErrorString(se));
+  return rc;
+}
+
+int adrt_adjoint_host(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* hin,
+                      const adrt_cotangents* hcot, const adrt_gradients* hgr) {
+  if (!e || !hin || !hcot || !hgr)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine, inputs, cotangents or gradients");
+  int rc = check_desc(d);
+  if (rc) return rc;
+  if ((rc = check_inputs(d, hin))) return rc;
+  {
+    std::lock_guard<std::mutex> lk(e->mu);
+    if ((rc = set_device(e))) return rc;
+  }
+  const size_t W = d->num_wavenumbers, L = d->num_layers, M = d->num_moments;
+  const size_t nmom = d->moment_layout == ADRT_MOMENTS_SHARED ? L * M
+                      : d->moment_layout == ADRT_MOMENTS_PER_WAVENUMBER ? W * M : W * L * M;
+  const size_t ntemp = (d->temperature_per_wavenumber ? W : 1) * (L + 1);
+  struct Arr {
+    const double* h;
+    size_t n;
+  };
+  const Arr ins[11] = {{hin->delta_tau, W * L}, {hin->single_scat_albedo, W * L},
+                       {hin->phase_moments, nmom}, {hin->temperature, ntemp},
+                       {hin->planck_levels, W * (L + 1)}, {hin->surface_albedo, W},
+                       {hin->solar_mu, W}, {hin->wavenumber_low, W},
+                       {hin->wavenumber_high, W}, {hin->surface_emission, W},
+                       {hin->top_emission, W}};
+  const Arr cots[4] = {{hcot->flux_up, W * (L + 1)}, {hcot->flux_down, W * (L + 1)},
+                       {hcot->mean_intensity, W * (L + 1)}, {hcot->flux_direct, W * (L + 1)}};
+  double* const grads_h[6] = {hgr->delta_tau, hgr->single_scat_albedo, hgr->phase_moments,
+                              hgr->temperature, hgr->planck_levels, hgr->surface_emission};
+  const size_t grad_n[6] = {W * L, W * L, nmom, ntemp, W * (L + 1), W};
+  auto a256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+  size_t total = 0;
+  for (const auto& a : ins)
+    if (a.h) total += a256(a.n * sizeof(double));
+  for (const auto& a : cots)
+    if (a.h) total += a256(a.n * sizeof(double));
+  for (int i = 0; i < 6; ++i)
+    if (grads_h[i]) total += a256(grad_n[i] * sizeof(double));
+  char* dbuf = nullptr;
+  if (cudaMalloc(&dbuf, total) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "host-entry staging allocation of %zu B failed", total);
+  }
+  cudaStream_t s = nullptr;
+  adrt_inputs din{};
+  adrt_cotangents dcot{};
+  adrt_gradients dgr{};
+  const double** din_p = &din.delta_tau;
+  const double** dcot_p = &dcot.flux_up;
+  double** dgr_p = &dgr.delta_tau;
+  size_t off = 0;
+  rc = ADRT_OK;
+  auto put = [&](const double* h, size_t n) -> double* {
+    double* dp = reinterpret_cast<double*>(dbuf + off);
+    off += a256(n * sizeof(double));
+    if (cudaMemcpyAsync(dp, h, n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      rc = fail(ADRT_ERR_CUDA, "host-to-device copy failed");
+    return dp;
+  };
+  for (int i = 0; i < 11 && rc == ADRT_OK; ++i)
+    if (ins[i].h) din_p[i] = put(ins[i].h, ins[i].n);
+  for (int i = 0; i < 4 && rc == ADRT_OK; ++i)
+    if (cots[i].h) dcot_p[i] = put(cots[i].h, cots[i].n);
+  // gradients that the adjoint adds to start from the caller's values
+  for (int i = 0; i < 6 && rc == ADRT_OK; ++i)
+    if (grads_h[i]) dgr_p[i] = put(grads_h[i], grad_n[i]);
+  if (rc == ADRT_OK) rc = adrt_adjoint(e, d, &din, nullptr, &dcot, &dgr, s);
+  for (int i = 0; i < 6 && rc == ADRT_OK; ++i)
+    if (grads_h[i] && cudaMemcpyAsync(grads_h[i], dgr_p[i], grad_n[i] * sizeof(double),
+                                      cudaMemcpyDeviceToHost, s) != cudaSuccess)
+      rc = fail(ADRT_ERR_CUDA, "device-to-host copy failed");
+  cudaError_t se = cudaStreamSynchronize(s);
+  cudaFree(dbuf);
+  if (rc == ADRT_OK && se != cudaSuccess)
+    rc = fail(ADRT_ERR_CUDA, "adjoint failed: %s", cudaGetErrorString(se));
   return rc;
 }
 

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "adrt/adding_doubling.hpp"
+#include "adrt/constants.hpp"
 #include "adrt/cuda_solver.hpp"
 #include "adrt_b200.h"
 
@@ -153,6 +154,99 @@ void* SolverWorkspace::engine() {
 // One column = a batch of one wavenumber in FP64; per-layer moments of
 // unequal length are zero-padded to the longest, which leaves the phase sums
 // and the delta-M truncation fraction of every layer unchanged.
+namespace {
+
+// ADConfig::compute_temperature_jacobian (src/solver.cpp:117-341).  Row k of
+// the Jacobian of F_up, F_down or J is the gradient of that output at
+// interface k, so all 3 (L+1) rows come from one batched adjoint over copies
+// of the column, each with a unit cotangent on its own output (temperatures,
+// or Planck levels, per copy so the gradients stay apart).  Columns 0..L are
+// the level temperatures (Planck levels without thermal emission), column
+// L+1 the surface skin temperature when the surface radiates independently
+// of the bottom level.  The flux-divergence rows follow from the J rows,
+// divF_k = 4 pi (1 - omega) (J_k - B_k).
+void temperature_jacobian(const ADConfig& c, adrt_batch_desc d, const std::vector<double>& moments,
+                          adrt_engine* e, RTOutput& r) {
+  const int L = c.num_layers, nint = L + 1, ndof = L + 2, K = 3 * nint;
+  const bool thermal = c.use_thermal_emission;
+  const bool planck_mode = !thermal && (int)c.planck_levels.size() == L + 1;
+  double Bs = c.surface_emission;
+  if (thermal) {
+    const double Ts = c.surface_temperature >= 0.0 ? c.surface_temperature : c.temperature[
+        c.index_from_bottom ? 0 : L];
+    Bs = planckFunction(c.wavenumber_low, c.wavenumber_high, Ts);
+  }
+  const bool has_surface = !c.use_diffusion_lower_bc && (c.surface_albedo > 0.0 || Bs > 0.0);
+  const bool surf_indep = has_surface && (thermal ? c.surface_temperature >= 0.0 : planck_mode);
+
+  d.num_wavenumbers = K;
+  d.moment_layout = ADRT_MOMENTS_SHARED;
+  d.temperature_per_wavenumber = 1;
+  auto rep = [&](const std::vector<double>& v) {
+    std::vector<double> o((size_t)K * v.size());
+    for (int k = 0; k < K; ++k) std::copy(v.begin(), v.end(), o.begin() + (size_t)k * v.size());
+    return o;
+  };
+  const std::vector<double> dt = rep(c.delta_tau), om = rep(c.single_scat_albedo);
+  const std::vector<double> src =
+      rep(thermal ? c.temperature
+                  : (planck_mode ? c.planck_levels : std::vector<double>(L + 1, 0.0)));
+  adrt_inputs in{};
+  in.delta_tau = dt.data();
+  in.single_scat_albedo = om.data();
+  in.phase_moments = moments.data();
+  (thermal ? in.temperature : in.planck_levels) = src.data();
+  std::vector<double> cot[3];
+  for (int o = 0; o < 3; ++o) cot[o].assign((size_t)K * nint, 0.0);
+  for (int row = 0; row < K; ++row) cot[row / nint][(size_t)row * nint + row % nint] = 1.0;
+  adrt_cotangents ct{};
+  ct.flux_up = cot[0].data();
+  ct.flux_down = cot[1].data();
+  ct.mean_intensity = cot[2].data();
+  std::vector<double> g((size_t)K * nint, 0.0), gs(K, 0.0);
+  adrt_gradients gr{};
+  (thermal ? gr.temperature : gr.planck_levels) = g.data();
+  gr.surface_emission = gs.data();
+  check(adrt_adjoint_host(e, &d, &in, &ct, &gr));
+
+  double ts_chain = 0.0;  // dB/dT at the skin temperature
+  if (thermal && surf_indep) {
+    check(adrt_planck_band_deriv(c.wavenumber_low, c.wavenumber_high, c.surface_temperature,
+                                 &ts_chain));
+  }
+  std::vector<std::vector<double>>* J[3] = {&r.flux_up_temperature_jac,
+                                            &r.flux_down_temperature_jac,
+                                            &r.mean_intensity_temperature_jac};
+  for (int o = 0; o < 3; ++o) J[o]->assign(nint, std::vector<double>(ndof, 0.0));
+  const int bottom = c.index_from_bottom ? 0 : L;  // the bottom level's column
+  for (int row = 0; row < K; ++row) {
+    std::vector<double>& jr = (*J[row / nint])[row % nint];
+    for (int m = 0; m <= L; ++m) jr[m] = g[(size_t)row * nint + m];
+    if (surf_indep)
+      jr[L + 1] = thermal ? gs[row] * ts_chain : gs[row];
+    else if (has_surface && !thermal)
+      jr[bottom] += gs[row];  // the surface source counts as the bottom level's
+  }
+  // divF_k = 4 pi (1 - omega_lyr) (J_k - B_k), lyr = the layer above interface k
+  // (layer 0 at the top), in the caller's order
+  auto& Jd = r.flux_divergence_temperature_jac;
+  Jd.assign(nint, std::vector<double>(ndof, 0.0));
+  for (int k = 0; k < nint; ++k) {
+    const int ki = c.index_from_bottom ? L - k : k;  // top-first interface
+    const int li = (ki == 0) ? 0 : ki - 1;
+    const int lyr = c.index_from_bottom ? L - 1 - li : li;
+    const double pref = 4.0 * PI * (1.0 - c.single_scat_albedo[lyr]);
+    double chain_k = 1.0;  // dB_k / d(column k)
+    if (thermal)
+      check(adrt_planck_band_deriv(c.wavenumber_low, c.wavenumber_high, c.temperature[k],
+                                   &chain_k));
+    for (int m = 0; m < ndof; ++m)
+      Jd[k][m] = pref * (r.mean_intensity_temperature_jac[k][m] - (m == k ? chain_k : 0.0));
+  }
+}
+
+}  // namespace
+
 RTOutput solve(const ADConfig& config, SolverWorkspace& workspace) {
   config.validate();
   const int L = config.num_layers;
@@ -207,6 +301,8 @@ RTOutput solve(const ADConfig& config, SolverWorkspace& workspace) {
   out.mean_intensity = r.mean_intensity.data();
   out.flux_divergence = r.flux_divergence.data();
   check(adrt_solve_batch_host(static_cast<adrt_engine*>(workspace.engine()), &d, &in, &out));
+  if (config.compute_temperature_jacobian)
+    temperature_jacobian(config, d, moments, static_cast<adrt_engine*>(workspace.engine()), r);
   return r;
 }
 
@@ -224,6 +320,12 @@ void gaussLegendre(int n, std::vector<double>& nodes, std::vector<double>& weigh
 double planckFunction(double wnumlo, double wnumhi, double temp) {
   double v = 0.0;
   check(adrt_planck_band(wnumlo, wnumhi, temp, &v));
+  return v;
+}
+
+double planckFunctionDeriv(double wnumlo, double wnumhi, double temp) {
+  double v = 0.0;
+  check(adrt_planck_band_deriv(wnumlo, wnumhi, temp, &v));
   return v;
 }
 

@@ -21,8 +21,8 @@ struct RTOutput {
   std::vector<double> mean_intensity;   ///< includes the direct beam
   std::vector<double> flux_divergence;  ///< 4 pi (1 - omega)(J - B), layer above
   std::vector<double> flux_direct;
-  /// Temperature Jacobians: produced by the reference's CPU path only; the
-  /// engine leaves them empty (the GPU adjoint is a separate entry point).
+  /// Temperature Jacobians [L+1][L+2] (levels 0..L, then the surface skin
+  /// temperature) when ADConfig::compute_temperature_jacobian is set.
   std::vector<std::vector<double>> flux_up_temperature_jac;
   std::vector<std::vector<double>> flux_down_temperature_jac;
   std::vector<std::vector<double>> mean_intensity_temperature_jac;
@@ -94,5 +94,8 @@ void gaussLegendre(int n, std::vector<double>& nodes, std::vector<double>& weigh
 
 /// Band-integrated Planck function (src/planck.cpp:35-131), host evaluation.
 double planckFunction(double wnumlo, double wnumhi, double temp);
+
+/// Its temperature derivative (src/planck.cpp:135-175).
+double planckFunctionDeriv(double wnumlo, double wnumhi, double temp);
 
 }  // namespace adrt

@@ -278,7 +278,10 @@ typedef struct adrt_gradients {
   double* phase_moments;
   double* temperature;
   double* planck_levels;
-  double* surface_emission; /* [W], overwritten; raw-source (non-thermal) batches only */
+  double* surface_emission; /* [W], overwritten: d/d(surface emission) -- the
+                               surface_emission input without thermal emission, or
+                               B(surface_temperature) with thermal emission and
+                               surface_temperature >= 0 (times dB/dT gives d/dT_s) */
 } adrt_gradients;
 
 /* Reverse-mode adjoint of the batched solve: given the loss cotangents,
@@ -287,13 +290,23 @@ typedef struct adrt_gradients {
  * planckFunctionDeriv, src/planck.cpp:135-175) or the Planck levels.  The
  * derivative is that of the discrete scheme at fixed doubling counts; it
  * generalises the reference's analytic temperature Jacobian
- * (src/solver.cpp:117-341) to all inputs.  FP64; every layer's doubling chain
- * is recomputed in the backward pass (not stored).  `out` may be NULL or
- * receive the forward outputs.  Not supported: delta-M truncation in effect
- * (use_delta_m with num_moments > 2N). */
+ * (src/solver.cpp:117-341) to all inputs.  FP64; the forward pass records
+ * every layer's doubling chain for the backward pass (in chunks of
+ * wavenumbers; chains beyond the record pool are recomputed).  `out` may be
+ * NULL or receive the forward outputs.  With delta-M truncation in effect
+ * (use_delta_m with num_moments > 2N) only the temperature, planck_levels and
+ * surface_emission gradients are formed. */
 int adrt_adjoint(adrt_engine* engine, const adrt_batch_desc* desc, const adrt_inputs* in,
                  const adrt_outputs* out, const adrt_cotangents* cot,
                  const adrt_gradients* grads, void* cuda_stream);
+
+/* adrt_adjoint from host buffers: copies in (the gradients too, since some
+ * are added to), runs the adjoint, copies the gradients back and
+ * synchronises.  Serves adrt::solve with ADConfig::compute_temperature_jacobian
+ * (src/solver.cpp:117-341), whose Jacobian rows are gradients of single
+ * outputs. */
+int adrt_adjoint_host(adrt_engine* engine, const adrt_batch_desc* desc, const adrt_inputs* in,
+                      const adrt_cotangents* cotangents, const adrt_gradients* gradients);
 
 /* ------------------------------------------------------- uneven batches */
 
@@ -328,6 +341,11 @@ int adrt_gauss_legendre(int n, double* nodes, double* weights);
  * ADRT_ERR_INVALID_ARGUMENT where the reference throws. */
 int adrt_planck_band(double wavenumber_low, double wavenumber_high, double temperature,
                      double* out);
+
+/* d/dT of the band-integrated Planck function: replaces
+ * adrt::planckFunctionDeriv (src/planck.cpp:135-175, declared in
+ * src/planck.hpp:27). */
+int adrt_planck_band_deriv(double wnumlo, double wnumhi, double temp, double* out);
 
 /* --------------------------------------------------------------- errors */
 const char* adrt_last_status_detail(void);

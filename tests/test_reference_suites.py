@@ -2,7 +2,9 @@
 
 oracle/Makefile (`engine-tests`) compiles the reference's
 tests/test_ad_solver.cpp (the column solver: known answers from published
-tables, energy conservation, validation errors, workspace reuse) and
+tables, energy conservation, validation errors, workspace reuse),
+tests/test_temperature_jacobian.cpp (the analytic temperature Jacobians of
+ADConfig::compute_temperature_jacobian against central differences) and
 tests/test_cuda_solver.cu (the batched GPU API: solveBatch, solveBatchHost and
 the raw-coefficient solveBatchFromCoefficients) unmodified, against
 include/adrt/*.hpp and libadrt_host.so, so every adrt::solve / adrt::cuda::*
