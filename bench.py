@@ -252,6 +252,28 @@ def run_config4(args, eng):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- ranks
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's value (every rank calls this in the same order)."""
+    if not dist:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: int, world: int, seconds: float) -> float:
+    """Whole-job throughput of a weak-scaling run: every rank processes its own
+    units_per_rank, and the job takes as long as its slowest rank."""
+    return units_per_rank * world / seconds
+
+
+def rank_seed(rank: int) -> int:
+    """Each rank solves its own shard of synthetic wavenumbers."""
+    return 2 + rank
+
+
 # ---------------------------------------------------------------- engine arm
 def main():
     args = parse()
@@ -288,7 +310,7 @@ def main():
     for pname in precisions:
         prec = _abi.PRECISION_FP64 if pname == "fp64" else _abi.PRECISION_MIXED
         # weak scaling: every rank solves its own batch of the full size
-        b = workloads.config2(W=args.wavenumbers, seed=2 + rank, precision=prec)
+        b = workloads.config2(W=args.wavenumbers, seed=rank_seed(rank), precision=prec)
         di = to_device(b)
         do = alloc_device_outputs(b, which=_abi.INTERFACE_OUTPUTS)
         eng.reserve(b.desc)
@@ -307,11 +329,7 @@ def main():
                 eng.solve_device(b.desc, di, do, stream)
             ev1.record(stream)
             torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / args.steps
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, "cuda")
         status = eng.read_status()
         results[pname] = {"ms": ms, "clocks": clk.summary(), "status": status,
                           "batch": b, "out": do}
@@ -353,11 +371,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         eng.solve_host(hb, out=hout)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps, dist, "cuda")
     h2d = int(sum(v.nbytes for v in hb.arrays.values()))
     d2h = int(sum(v.nbytes for v in hout.values()))
 
@@ -386,7 +400,7 @@ def main():
                 "flops_per_launch": fl}
         line = {
             "metric": METRIC,
-            "value": args.wavenumbers * world / (ms * 1e-3),
+            "value": job_rate(args.wavenumbers, world, ms * 1e-3),
             "unit": "wavenumber-solves/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -396,13 +410,13 @@ def main():
                        "wavenumbers_per_gpu": args.wavenumbers,
                        "l2": "inputs 190 MB > 126 MB L2, no flush",
                        "parallelism": f"replicas x{world} (wavenumber shards)"},
-            **{f"{p}_solves_per_s": args.wavenumbers * world / (results[p]["ms"] * 1e-3)
+            **{f"{p}_solves_per_s": job_rate(args.wavenumbers, world, results[p]["ms"] * 1e-3)
                for p in precisions},
             "mixed_over_fp64": (results["fp64"]["ms"] / results["mixed"]["ms"]
                                 if len(precisions) == 2 else None),
             "accuracy_vs_oracle": acc,
             "roofline": roof,
-            "e2e": {"value": args.wavenumbers * world / e2e_s, "unit": "wavenumber-solves/s",
+            "e2e": {"value": job_rate(args.wavenumbers, world, e2e_s), "unit": "wavenumber-solves/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             **adj,
