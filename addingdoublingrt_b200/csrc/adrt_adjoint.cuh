@@ -136,7 +136,7 @@ struct GemmX {
 };
 
 template <class Gm, int NSEG, int NRANK>
-__device__ __noinline__ void op_gemm_x(const GemmX g, int t) {
+__device__ __forceinline__ void op_gemm_x(const GemmX g, int t) {
   using Real = typename Gm::Real;
   constexpr int NP = Gm::NP, LD = Gm::LD;
   const Real* add = (g.add == kNoMat) ? nullptr : sp<Real>(g.add);
