@@ -466,10 +466,29 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     };
     // 1. this step's record; h = z + g y
     X.sync();
-    op_g2s<Gm, GC>(tk + Tp::OFF_R, X.mo(J_R), X.mo(J_Rc), t);
-    op_g2s<Gm, GC>(tk + Tp::OFF_T, kNoMat, X.mo(J_Tc), t);
-    op_g2s<Gm, GC>(tk + Tp::OFF_TG, X.mo(J_TGc), X.mo(J_TG), t);  // record holds TG^T
-    op_g2s<Gm, GC>(tk + Tp::OFF_AI, kNoMat, X.mo(J_Ac), t);       // (I - R R)^{-1} (cm)
+    {  // the step's four matrices from the record (in GC's tile order), one pass:
+       // R (rm + cm), T (cm), TG^T (rm + cm), (I - R R)^{-1} (cm)
+      const Tile<Gm> tl(t);
+      if (tl.valid()) {
+        Real mR[TR][TC], mT[TR][TC], mG[TR][TC], mA[TR][TC];
+#pragma unroll
+        for (int a = 0; a < TR; ++a)
+#pragma unroll
+          for (int b = 0; b < TC; ++b) {
+            const int e = tile_index<GC>(tl.row(a), tl.col(b));
+            mR[a][b] = tk[Tp::OFF_R + e];
+            mT[a][b] = tk[Tp::OFF_T + e];
+            mG[a][b] = tk[Tp::OFF_TG + e];
+            mA[a][b] = tk[Tp::OFF_AI + e];
+          }
+        tl.store_rm(mR, X.m(J_R));
+        tl.store_cm(mR, X.m(J_Rc));
+        tl.store_cm(mT, X.m(J_Tc));
+        tl.store_rm(mG, X.m(J_TGc));
+        tl.store_cm(mG, X.m(J_TG));
+        tl.store_cm(mA, X.m(J_Ac));
+      }
+    }
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
       const double y = tk[Tp::OFF_VEC + i], z = tk[Tp::OFF_VEC + NP + i];
