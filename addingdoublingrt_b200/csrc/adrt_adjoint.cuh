@@ -444,10 +444,34 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   const double d_Bb = 0.5 * pBbar + pBd / tau, d_Bt = 0.5 * pBbar - pBd / tau;
   double bg = 0.0, bgam = 0.0;
   int cs = 0;  // which cotangent set holds the current dR, dT
-  for (int k = nn - 1; k >= 0; --k) {
+  // the record of step k - 1 is fetched into registers while step k runs
+  const Tile<Gm> tlp(t);
+  Real nR[TR][TC], nT[TR][TC], nG[TR][TC], nA[TR][TC];
+  double nv[4] = {0.0, 0.0, 0.0, 0.0}, ngam = 0.0;
+  auto fetch = [&](int k) {
     const double* tk = tape + (size_t)k * Tp::STEP;
+    if (tlp.valid()) {
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          const int e = tile_index<GC>(tlp.row(a), tlp.col(b));
+          nR[a][b] = tk[Tp::OFF_R + e];
+          nT[a][b] = tk[Tp::OFF_T + e];
+          nG[a][b] = tk[Tp::OFF_TG + e];
+          nA[a][b] = tk[Tp::OFF_AI + e];
+        }
+    }
+    if (X.warp == 0 && X.lane < NP) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) nv[j] = tk[Tp::OFF_VEC + j * NP + X.lane];
+    }
+    ngam = tk[Tp::OFF_VEC + 4 * NP];
+  };
+  fetch(nn - 1);
+  for (int k = nn - 1; k >= 0; --k) {
     const double g = ldexp(tau0, k - 1);
-    const double gam = tk[Tp::OFF_VEC + 4 * NP];
+    const double gam = ngam;
     const unsigned bRr = X.mo(cs ? J_bR1 : J_bR0), bRc = X.mo(cs ? J_bR1c : J_bR0c);
     const unsigned bTr = X.mo(cs ? J_bT1 : J_bT0), bTc = X.mo(cs ? J_bT1c : J_bT0c);
     const unsigned nRr = X.mo(cs ? J_bR0 : J_bR1), nRc = X.mo(cs ? J_bR0c : J_bR1c);
@@ -466,38 +490,25 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     };
     // 1. this step's record; h = z + g y
     X.sync();
-    {  // the step's four matrices from the record (in GC's tile order), one pass:
-       // R (rm + cm), T (cm), TG^T (rm + cm), (I - R R)^{-1} (cm)
-      const Tile<Gm> tl(t);
-      if (tl.valid()) {
-        Real mR[TR][TC], mT[TR][TC], mG[TR][TC], mA[TR][TC];
-#pragma unroll
-        for (int a = 0; a < TR; ++a)
-#pragma unroll
-          for (int b = 0; b < TC; ++b) {
-            const int e = tile_index<GC>(tl.row(a), tl.col(b));
-            mR[a][b] = tk[Tp::OFF_R + e];
-            mT[a][b] = tk[Tp::OFF_T + e];
-            mG[a][b] = tk[Tp::OFF_TG + e];
-            mA[a][b] = tk[Tp::OFF_AI + e];
-          }
-        tl.store_rm(mR, X.m(J_R));
-        tl.store_cm(mR, X.m(J_Rc));
-        tl.store_cm(mT, X.m(J_Tc));
-        tl.store_rm(mG, X.m(J_TGc));
-        tl.store_cm(mG, X.m(J_TG));
-        tl.store_cm(mA, X.m(J_Ac));
-      }
+    // the step's record (fetched during the step before): R (rm + cm), T (cm),
+    // TG^T (rm + cm), (I - R R)^{-1} (cm) and y, z, s_up, s_dn
+    if (tlp.valid()) {
+      tlp.store_rm(nR, X.m(J_R));
+      tlp.store_cm(nR, X.m(J_Rc));
+      tlp.store_cm(nT, X.m(J_Tc));
+      tlp.store_rm(nG, X.m(J_TGc));
+      tlp.store_cm(nG, X.m(J_TG));
+      tlp.store_cm(nA, X.m(J_Ac));
     }
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
-      const double y = tk[Tp::OFF_VEC + i], z = tk[Tp::OFF_VEC + NP + i];
-      VA(A_Y)[i] = y;
-      VA(A_Z)[i] = z;
-      VA(A_H)[i] = z + g * y;
-      VA(A_SU)[i] = tk[Tp::OFF_VEC + 2 * NP + i];
-      VA(A_SD)[i] = tk[Tp::OFF_VEC + 3 * NP + i];
+      VA(A_Y)[i] = nv[0];
+      VA(A_Z)[i] = nv[1];
+      VA(A_H)[i] = nv[1] + g * nv[0];
+      VA(A_SU)[i] = nv[2];
+      VA(A_SD)[i] = nv[3];
     }
+    if (k > 0) fetch(k - 1);
     X.sync();
     // 2. TGR = TG R;  dTGR = dR T^T - bz h^T + by y^T;  ru = R sd + gam su, rd = gam R su + sd
     op_gemm_x<Gm, 1, 0>(gx(X.mo(J_TGc), X.mo(J_R), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat,
