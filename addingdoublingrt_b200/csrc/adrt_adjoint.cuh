@@ -338,8 +338,10 @@ struct AdjScratch {
   static __host__ __device__ size_t tape() {
     return ((size_t)Tp::layer(kMaxDoublings) * sizeof(double) + 255) & ~size_t(255);
   }
+  // two matrices in tile order (Tp::TILE Reals each: the thread grid can be
+  // wider than NP x NP) and two vectors
   static __host__ __device__ size_t pacc() {
-    return ((size_t)2 * NP * NP * sizeof(double) + 2 * NP * sizeof(double) + 255) & ~size_t(255);
+    return ((size_t)2 * Tp::TILE * sizeof(double) + 2 * NP * sizeof(double) + 255) & ~size_t(255);
   }
   static __host__ __device__ size_t brb() { return (Tp::TILE * sizeof(double) + 255) & ~size_t(255); }
   static __host__ __device__ size_t acc(int lmax) {
@@ -924,6 +926,26 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   const double* hw = X.DV(D_HW);
   const size_t wo = (size_t)w * (nL + 1);
   auto ui = [&](int l) { return fb ? nL - l : l; };  // user level index
+  // moment set of internal layer l, its effective count and delta-M fraction,
+  // as the forward pass formed them (f < 0: no truncation scaling)
+  auto moments = [&](int l, int& nuse, double& f) -> const double* {
+    const int u = fb ? nL - 1 - l : l;
+    const double* chi = C->moments + (layout == 0 ? (size_t)u * M
+                                      : layout == 1 ? (size_t)w * M
+                                                    : ((size_t)w * nL + u) * M);
+    nuse = M;
+    f = -1.0;
+    if (C->delta_m) {
+      const double ff = (M > 2 * N) ? chi[2 * N] : 0.0;
+      if (ff > 1e-12 && ff < 1.0 - 1e-12) {
+        f = ff;
+        nuse = 2 * N;
+      } else {
+        nuse = (M < 2 * N) ? M : 2 * N;
+      }
+    }
+    return chi;
+  };
   auto cot = [&](const double* a, int l) { return a ? a[wo + ui(l)] : 0.0; };
   Real* vb = X.m(J_VEC);
   auto VA = [&](int s) { return vb + s * NP; };
@@ -937,7 +959,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     gtau[l] = 0.0;
     gom[l] = 0.0;
   }
-  for (int e = t; e < 2 * NP * NP + 2 * NP; e += G) pacc[e] = 0.0;
+  for (int e = t; e < 2 * TILE + 2 * NP; e += G) pacc[e] = 0.0;
   X.sync();
 
   // ======== 1. downward-pass adjoint (interface L-1 .. 0); bId carried in A_BDN
@@ -1038,6 +1060,13 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     }
   }
   int nuse_l1 = M;
+  if (layout == 1) {  // one moment set per wavenumber: the solar phase vectors once
+    int nuse;
+    double f;
+    const double* chi = moments(0, nuse, f);
+    nuse_l1 = nuse;
+    build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+  }
   for (int l = 0; l < nL; ++l) {
     const double* rl = recs + (size_t)l * REC;
     const double* rb = recs + (size_t)(l + 1) * REC;
@@ -1200,12 +1229,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     const double Bt = lv.B[l], Bb = lv.B[l + 1];
     if (scat) {
       int nuse;
-      double f = -1.0;
-      const int u = fb ? nL - 1 - l : l;
-      const double* chi = C->moments + (layout == 0 ? (size_t)u * M
-                                        : layout == 1 ? (size_t)w * M
-                                                      : ((size_t)w * nL + u) * M);
-      nuse = C->delta_m ? ((M < 2 * N) ? M : 2 * N) : M;
+      double f;
+      const double* chi = moments(l, nuse, f);
       nuse_l1 = nuse;
       if (layout != 1)
         build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
@@ -1226,7 +1251,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       } else {  // one moment set per wavenumber: accumulate the phase cotangents
         if (tl.valid()) {
           double* aP = pacc + t * Gm::TE;
-          double* aM = pacc + NP * NP + t * Gm::TE;
+          double* aM = pacc + TILE + t * Gm::TE;
 #pragma unroll
           for (int a = 0; a < TR; ++a)
 #pragma unroll
@@ -1236,8 +1261,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
             }
         }
         if (X.warp == 0 && X.lane < NP) {
-          pacc[2 * NP * NP + X.lane] += VA(A_T0)[X.lane];
-          pacc[2 * NP * NP + NP + X.lane] += VA(A_T1)[X.lane];
+          pacc[2 * TILE + X.lane] += VA(A_T0)[X.lane];
+          pacc[2 * TILE + NP + X.lane] += VA(A_T1)[X.lane];
         }
       }
     } else if (tau > 0.0) {
@@ -1277,10 +1302,10 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   // one moment set per wavenumber: its adjoint once
   if (layout == 1 && AD.g_mom) {
     op_g2s<Gm>(pacc, X.mo(J_T1), kNoMat, t);
-    op_g2s<Gm>(pacc + NP * NP, X.mo(J_T2), kNoMat, t);
+    op_g2s<Gm>(pacc + TILE, X.mo(J_T2), kNoMat, t);
     if (X.warp == 0 && X.lane < NP) {
-      VA(A_T0)[X.lane] = pacc[2 * NP * NP + X.lane];
-      VA(A_T1)[X.lane] = pacc[2 * NP * NP + NP + X.lane];
+      VA(A_T0)[X.lane] = pacc[2 * TILE + X.lane];
+      VA(A_T1)[X.lane] = pacc[2 * TILE + NP + X.lane];
     }
     X.sync();
     const double* chi = C->moments + (size_t)w * M;

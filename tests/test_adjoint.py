@@ -194,3 +194,136 @@ def test_temperature_gradient_matches_reference_analytic_jacobian(eng):
             g += cot[k].reshape(b.W, L + 1)[w] @ J
         e = np.max(np.abs(ad[w] - g)) / np.max(np.abs(g))
         assert e < 1e-6, (w, e)
+
+
+def fd_moments(b, cot, h=1e-5):
+    """d loss / d chi by central differences over every moment set."""
+    M = b.desc.num_moments
+    chi = b.arrays["phase_moments"].reshape(-1, M)
+    fd = np.zeros_like(chi)
+    for s in range(chi.shape[0]):
+        for m in range(M):
+            vals = []
+            for sgn in (1.0, -1.0):
+                c = chi.copy()
+                c[s, m] += sgn * h
+                bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+                bb.set("phase_moments", c)
+                vals.append(loss_per_wav(bb, cot).sum())
+            fd[s, m] = (vals[0] - vals[1]) / (2 * h)
+    return fd
+
+
+def fd_temperature(b, cot, h=1e-3):
+    """d loss / d T_l by central differences: per wavenumber when the level
+    temperatures are (wavenumbers are independent), else of the summed loss."""
+    T = b.arrays["temperature"]
+    per_w = bool(b.desc.temperature_per_wavenumber)
+    Tm = T.reshape(b.W if per_w else 1, b.L + 1)
+    fd = np.zeros(Tm.shape)
+    for l in range(b.L + 1):
+        vals = []
+        for sgn in (1.0, -1.0):
+            a = Tm.copy()
+            a[:, l] += sgn * h
+            bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+            bb.set("temperature", a.reshape(T.shape))
+            v = loss_per_wav(bb, cot)
+            vals.append(v if per_w else v.sum())
+        fd[:, l] = (vals[0] - vals[1]) / (2 * h)
+    return fd.reshape(T.shape)
+
+
+@pytest.mark.parametrize("layout", [_abi.MOMENTS_PER_WAVENUMBER, _abi.MOMENTS_PER_LAYER])
+def test_adjoint_moment_layouts_match_finite_differences(eng, layout):
+    """One moment set per wavenumber (its cotangent accumulated over the
+    layers) and one per wavenumber and layer: tau, omega and moment gradients."""
+    b = small_batch(31 + layout, 4, W=3, L=4, layout=layout)
+    rng = np.random.default_rng(31 + layout)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot)
+    for name in ("delta_tau", "single_scat_albedo"):
+        fd = fd_layer_param(b, cot, name)
+        e = rel_err(ad[name].reshape(b.W, b.L), fd)
+        assert e < 2e-5, (name, layout, e)
+    fd = fd_moments(b, cot)
+    e = rel_err(ad["phase_moments"].reshape(fd.shape), fd)
+    assert e < 1e-4, ("phase_moments", layout, e)
+
+
+def thick_batch(seed, N, W=6, L=5, M=None, temp_per_wav=False):
+    """Optically thick scattering layers (tau 300..1000, omega >= 0.3): about
+    25 doublings per layer against the 12 per layer the record pool holds on
+    average, so only part of the batch gets records and the reverse pass
+    recomputes the other wavenumbers' doubling chains."""
+    b = small_batch(seed, N, W=W, L=L, temp_per_wav=temp_per_wav)
+    rng = np.random.default_rng(seed + 100)
+    b.set("delta_tau", 10.0 ** rng.uniform(2.5, 3.0, size=(W, L)))
+    b.set("single_scat_albedo", rng.uniform(0.3, 0.95, size=(W, L)))
+    if M is not None:
+        d = _abi.BatchDesc.from_buffer_copy(b.desc)
+        d.num_moments = M
+        arrays = dict(b.arrays)
+        arrays["phase_moments"] = workloads.hg_moments(rng.uniform(0.4, 0.85, size=L), M)
+        b = workloads.Batch(d, arrays)
+    return b
+
+
+PER_WAVENUMBER = ("delta_tau", "single_scat_albedo", "temperature", "surface_albedo",
+                  "solar_mu", "wavenumber_low", "wavenumber_high")
+
+
+def joined(a, b):
+    """Batch of a's wavenumbers followed by b's (a's phase moments)."""
+    d = _abi.BatchDesc.from_buffer_copy(a.desc)
+    d.num_wavenumbers = a.W + b.W
+    arrays = dict(a.arrays)
+    for k in PER_WAVENUMBER:
+        arrays[k] = np.concatenate([a.arrays[k].reshape(a.W, -1),
+                                    b.arrays[k].reshape(b.W, -1)]).reshape(-1)
+    return workloads.Batch(d, arrays)
+
+
+def test_recomputed_doubling_chains_equal_recorded_ones(eng):
+    """Chains that found no room in the record pool are recomputed in the
+    reverse pass.  Six thick wavenumbers alone overflow the pool (most are
+    recomputed); joined with sixty thin ones the pool holds every chain.  Their
+    per-wavenumber gradients agree, and the temperature gradient of the
+    recomputing batch matches finite differences."""
+    N = 8
+    thick = thick_batch(41, N, temp_per_wav=True)
+    tau = thick.arrays["delta_tau"].reshape(thick.W, thick.L)
+    om = thick.arrays["single_scat_albedo"].reshape(thick.W, thick.L)
+    nn = np.array([[nn_of(tau[w, l], om[w, l]) for l in range(thick.L)]
+                   for w in range(thick.W)])
+    assert nn.mean() > 2 * 12, nn.mean()  # twice the pool's average allowance
+    thin = small_batch(42, N, W=60, L=thick.L, temp_per_wav=True)
+    thin.set("delta_tau", 10.0 ** np.random.default_rng(42).uniform(-4, -3, size=(60, thick.L)))
+    both = joined(thick, thin)
+    rng = np.random.default_rng(41)
+    cot_both = {k: rng.normal(size=both.W * (both.L + 1)) for k in COT}
+    cot = {k: v.reshape(both.W, -1)[:thick.W].reshape(-1).copy() for k, v in cot_both.items()}
+    rec = run_adjoint(eng, both, cot_both)
+    ad = run_adjoint(eng, thick, cot)
+    for name in ("delta_tau", "single_scat_albedo", "temperature"):
+        r = rec[name].reshape(both.W, -1)[:thick.W]
+        g = ad[name].reshape(thick.W, -1)
+        e = np.max(np.abs(g - r)) / np.max(np.abs(r))
+        assert e < 1e-9, (name, e)
+    fd = fd_temperature(thick, cot)
+    e = rel_err(ad["temperature"].reshape(fd.shape), fd)
+    assert e < 1e-4, ("temperature", e)
+
+
+def test_delta_m_truncated_temperature_gradient_matches_finite_differences(eng):
+    """delta-M with more than 2N moments scales tau, omega and the phase
+    moments by the truncated fraction chi_2N; the temperature gradient of that
+    scheme (here with recomputed chains as well) against finite differences."""
+    N = 4
+    b = thick_batch(43, N, M=3 * N)
+    assert b.desc.use_delta_m and b.desc.num_moments > 2 * N
+    rng = np.random.default_rng(43)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot, which=("temperature",))
+    e = rel_err(ad["temperature"], fd_temperature(b, cot))
+    assert e < 1e-4, ("temperature", e)
