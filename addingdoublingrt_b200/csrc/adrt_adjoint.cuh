@@ -293,6 +293,9 @@ enum AdjMat {
 // work memory when the engine has no workspace limit.
 constexpr int kTapeStepsPerLayer = 12;
 constexpr size_t kAdjointMemory = size_t(16) << 30;
+// Moment sets shared by every wavenumber: the reverse sums their phase-matrix
+// cotangents per block (2 NP^2 doubles per set and block) when that fits here.
+constexpr size_t kPhaseSumMemory = size_t(1) << 30;
 
 // Vector slots inside the J_VEC buffers (each NP Reals; 2 DIM LD >= 20 NP).
 enum AdjVec {
@@ -347,8 +350,11 @@ struct AdjScratch {
   static __host__ __device__ size_t acc(int lmax) {
     return ((size_t)4 * (lmax + 1) * sizeof(double) + 255) & ~size_t(255);
   }
-  static __host__ __device__ size_t bytes(int lmax) {
-    return dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256;
+  static __host__ __device__ size_t plm(int m) {  // P_l(mu0), l < M
+    return ((size_t)m * sizeof(double) + 255) & ~size_t(255);
+  }
+  static __host__ __device__ size_t bytes(int lmax, int m) {
+    return dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256 + plm(m);
   }
 };
 
@@ -379,6 +385,13 @@ struct AdjDev {
   double* pool;
   long long pool_cap;               // doubles
   unsigned long long* pool_used;    // zeroed before each chunk
+  // moment sets shared by all wavenumbers (one per layer): their phase
+  // matrices ([set][P++, P+-], row-major, pitch NP; null: built per layer),
+  // and the per-block sums of the phase-matrix cotangents ([set][block]
+  // [P++, P+-] in the reverse group's tile order; null: per layer)
+  const double* ptab;
+  double* pacc;
+  int pacc_blocks;
 };
 
 // ---------------------------------------------------------------- doubling adjoint
@@ -707,11 +720,16 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
 // Cotangents of the phase moments from those of P++ (J_T1), P+- (J_T2) and of
 // the solar phase vectors (A_T0 = p+, A_T1 = p-), through the Hansen column
 // renormalisation (src/phase_matrix.hpp:61-111, 131-181).  Adds into dchi[l]
-// for l < nuse (global, atomically).
-template <class Gm>
+// for l < nuse (global, atomically).  The two parts are linear in their
+// cotangents and independent: MAT the matrices' (which, for a moment set
+// shared by all wavenumbers, runs once on the cotangents summed over them),
+// SOL the solar vectors' (which depend on each wavenumber's mu0; plm0[l] =
+// P_l(mu0) for l < nuse).
+template <class Gm, bool MAT = true, bool SOL = true>
 __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, int bar,
                                            const double* chi, int nuse, int N, const double* pl,
-                                           bool solar, double mu0, double* dchi) {
+                                           bool solar, double mu0, double* dchi,
+                                           const double* plm0) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, G = Gm::G, LD = Gm::LD;
@@ -727,64 +745,71 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   Real* bsar = vb + A_BSU * NP;  // d s_j
   Real* qp = vb + A_H * NP;
   Real* qm = vb + A_RU * NP;
-  // un-normalised Q
-  if constexpr (UsePhaseMMA<Gm>::value)
-    phase_products<Gm>(chi, nuse, -1.0, N, pl, Qpp, Qpm, LD, t);
-  else
-  for (int e = t; e < NP * NP; e += G) {
-    const int r = e / NP, c = e % NP;
-    double spp = 0.0, spm = 0.0;
-    if (r < N && c < N) {
-      double sign = 1.0;
-      for (int l = 0; l < nuse; ++l) {
-        const double term = (2 * l + 1) * chi[l] * pl[l * N + r] * pl[l * N + c];
-        spp += term;
-        spm += sign * term;
-        sign = -sign;
+  solar = SOL && solar;
+  if constexpr (MAT) {
+    // un-normalised Q
+    if constexpr (UsePhaseMMA<Gm>::value)
+      phase_products<Gm>(chi, nuse, -1.0, N, pl, Qpp, Qpm, LD, t);
+    else
+    for (int e = t; e < NP * NP; e += G) {
+      const int r = e / NP, c = e % NP;
+      double spp = 0.0, spm = 0.0;
+      if (r < N && c < N) {
+        double sign = 1.0;
+        for (int l = 0; l < nuse; ++l) {
+          const double term = (2 * l + 1) * chi[l] * pl[l * N + r] * pl[l * N + c];
+          spp += term;
+          spm += sign * term;
+          sign = -sign;
+        }
       }
+      Qpp[r * LD + c] = spp / (2.0 * kPi);
+      Qpm[r * LD + c] = spm / (2.0 * kPi);
     }
-    Qpp[r * LD + c] = spp / (2.0 * kPi);
-    Qpm[r * LD + c] = spm / (2.0 * kPi);
-  }
-  X.sync();
-  if (t < NP) {
-    const int c = t;
-    double s = 0.0, bc = 0.0;
-    for (int i = 0; i < N; ++i) s += (Qpp[i * LD + c] + Qpm[i * LD + c]) * wt[i];
-    const double corr = (s > 0.0) ? 1.0 / (2.0 * kPi * s) : 1.0;
-    for (int i = 0; i < N; ++i) bc += dPpp[i * LD + c] * Qpp[i * LD + c] + dPpm[i * LD + c] * Qpm[i * LD + c];
-    sarr[c] = s;
-    carr[c] = corr;
-    bsar[c] = (s > 0.0) ? -bc * corr / s : 0.0;
-  }
-  X.sync();
-  for (int e = t; e < NP * NP; e += G) {  // dQ = dP corr_j + w_i ds_j (in place)
-    const int r = e / NP, c = e % NP;
-    dPpp[r * LD + c] = dPpp[r * LD + c] * carr[c] + wt[r] * bsar[c];
-    dPpm[r * LD + c] = dPpm[r * LD + c] * carr[c] + wt[r] * bsar[c];
+    X.sync();
+    if (t < NP) {
+      const int c = t;
+      double s = 0.0, bc = 0.0;
+      for (int i = 0; i < N; ++i) s += (Qpp[i * LD + c] + Qpm[i * LD + c]) * wt[i];
+      const double corr = (s > 0.0) ? 1.0 / (2.0 * kPi * s) : 1.0;
+      for (int i = 0; i < N; ++i)
+        bc += dPpp[i * LD + c] * Qpp[i * LD + c] + dPpm[i * LD + c] * Qpm[i * LD + c];
+      sarr[c] = s;
+      carr[c] = corr;
+      bsar[c] = (s > 0.0) ? -bc * corr / s : 0.0;
+    }
+    X.sync();
+    for (int e = t; e < NP * NP; e += G) {  // dQ = dP corr_j + w_i ds_j (in place)
+      const int r = e / NP, c = e % NP;
+      dPpp[r * LD + c] = dPpp[r * LD + c] * carr[c] + wt[r] * bsar[c];
+      dPpm[r * LD + c] = dPpm[r * LD + c] * carr[c] + wt[r] * bsar[c];
+    }
   }
   double bqscale = 0.0;
   if (solar) {
-    // un-normalised solar vectors and their normalisation
+    // un-normalised solar vectors and their normalisation; plm0[l] = P_l(mu0),
+    // the small tables' loads issued eight at a time (they mostly miss L1)
     if (t < NP) {
       double sp = 0.0, sm = 0.0;
       if (t < N) {
-        double sign = 1.0, p0 = 1.0, p1 = mu0;
-        for (int l = 0; l < nuse; ++l) {
-          double plm;
-          if (l == 0) {
-            plm = 1.0;
-          } else if (l == 1) {
-            plm = mu0;
-          } else {
-            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);  // off the chain
-            p0 = p1;
-            p1 = plm;
+        for (int l0 = 0; l0 < nuse; l0 += 8) {
+          double c[8], p[8], q[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int l = (l0 + j < nuse) ? l0 + j : 0;
+            c[j] = chi[l];
+            p[j] = pl[l * N + t];
+            q[j] = plm0[l];
           }
-          const double term = (2 * l + 1) * chi[l] * pl[l * N + t] * plm;
-          sp += term;
-          sm += sign * term;
-          sign = -sign;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int l = l0 + j;
+            if (l < nuse) {
+              const double term = (2 * l + 1) * c[j] * p[j] * q[j];
+              sp += term;
+              sm += (l & 1) ? -term : term;
+            }
+          }
         }
       }
       qp[t] = sp / (2.0 * kPi);
@@ -792,11 +817,15 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
     }
     X.sync();
     double ss = 0.0, bcs = 0.0;
-    for (int i = 0; i < N; ++i) ss += (qp[i] + qm[i]) * wt[i];
-    const double cs = (ss > 0.0) ? 1.0 / (2.0 * kPi * ss) : 1.0;
     const Real* dpp = vb + A_T0 * NP;
     const Real* dpm = vb + A_T1 * NP;
-    for (int i = 0; i < N; ++i) bcs += dpp[i] * qp[i] + dpm[i] * qm[i];
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+      if (i < N) ss += (qp[i] + qm[i]) * wt[i];
+    const double cs = (ss > 0.0) ? 1.0 / (2.0 * kPi * ss) : 1.0;
+#pragma unroll
+    for (int i = 0; i < NP; ++i)
+      if (i < N) bcs += dpp[i] * qp[i] + dpm[i] * qm[i];
     bqscale = (ss > 0.0) ? -bcs * cs / ss : 0.0;
     X.sync();
     if (t < NP) {  // dq = dp cs + w dss
@@ -806,8 +835,8 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   }
   X.sync();
   // dchi_l = (2l+1)/(2 pi) [P_l^T (dQpp + s_l dQpm) P_l + p0_l P_l . (dqp + s_l dqm)]
-  bool forms_done = false;
-  if constexpr (UsePhaseMMA<Gm>::value) {
+  bool forms_done = !MAT;
+  if constexpr (MAT && UsePhaseMMA<Gm>::value) {
     // the quadratic forms on the tensor cores: V = S B with S = dQpp + dQpm
     // (even l) or dQpp - dQpm (odd l) and B[j][k] = P_l(k)(mu_j), l(k) = 2k or
     // 2k + 1; the form of moment l(k) is column k of V dotted with P_l(k)(mu_.)
@@ -841,39 +870,50 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
     }
     forms_done = true;
   }
-  for (int l = t; l < nuse; l += G) {
-    const double sg = (l & 1) ? -1.0 : 1.0;
-    double acc = 0.0;
-    if (!forms_done) {
-      for (int i = 0; i < N; ++i) {
-        double ri = 0.0;
-        for (int j = 0; j < N; ++j)
-          ri += (dPpp[i * LD + j] + sg * dPpm[i * LD + j]) * pl[l * N + j];
-        acc += pl[l * N + i] * ri;
-      }
-    }
-    if (solar) {
-      double p0 = 1.0, p1 = mu0, plm = 1.0;
-      for (int m = 0; m <= l; ++m) {
-        if (m == 0) {
-          plm = 1.0;
-        } else if (m == 1) {
-          plm = mu0;
-        } else {
-          plm = ((2 * m - 1) * mu0 * p1 - (m - 1) * p0) * recip((double)m);  // off the chain
-          p0 = p1;
-          p1 = plm;
+  if (!forms_done || solar) {
+    for (int l = t; l < nuse; l += G) {
+      const double sg = (l & 1) ? -1.0 : 1.0;
+      double acc = 0.0;
+      if (!forms_done) {
+        for (int i = 0; i < N; ++i) {
+          double ri = 0.0;
+          for (int j = 0; j < N; ++j)
+            ri += (dPpp[i * LD + j] + sg * dPpm[i * LD + j]) * pl[l * N + j];
+          acc += pl[l * N + i] * ri;
         }
       }
-      double sv = 0.0;
-      for (int i = 0; i < N; ++i) sv += pl[l * N + i] * (qp[i] + sg * qm[i]);
-      acc += plm * sv;
+      if (solar) {
+        const double plm = plm0[l];
+        double sv = 0.0;
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+          if (i < N) sv += pl[l * N + i] * (qp[i] + sg * qm[i]);
+        acc += plm * sv;
+      }
+      atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
     }
-    if (!forms_done || solar) atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
   }
   X.sync();
 }
 
+
+// Effective moment count and delta-M fraction of a moment set, as the forward
+// pass forms them (f < 0: no truncation scaling).
+__device__ __forceinline__ void moment_use(const ColumnDev* C, const double* chi, int& nuse,
+                                           double& f) {
+  const int N = C->N, M = C->M;
+  nuse = M;
+  f = -1.0;
+  if (C->delta_m) {
+    const double ff = (M > 2 * N) ? chi[2 * N] : 0.0;
+    if (ff > 1e-12 && ff < 1.0 - 1e-12) {
+      f = ff;
+      nuse = 2 * N;
+    } else {
+      nuse = (M < 2 * N) ? M : 2 * N;
+    }
+  }
+}
 
 // ---------------------------------------------------------------- one wavenumber
 // Runs on the state a taping forward left for wavenumber w (WavState: the
@@ -914,6 +954,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   double* brb = reinterpret_cast<double*>(p += AS::pacc());       // carried d R_base (tiles)
   double* acc = reinterpret_cast<double*>(p += AS::brb());        // bB, btc, dtau, dom
   double* scal = reinterpret_cast<double*>(p += AS::acc(lmax));   // 32 doubles
+  double* plm0 = reinterpret_cast<double*>(p += 256);              // P_l(mu0), l < M
   const long long tbase = toff[nL];                               // this wavenumber's records
   double* tape_all = (tbase >= 0) ? AD.pool + tbase : nullptr;
   double* bB = acc;
@@ -926,24 +967,13 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   const double* hw = X.DV(D_HW);
   const size_t wo = (size_t)w * (nL + 1);
   auto ui = [&](int l) { return fb ? nL - l : l; };  // user level index
-  // moment set of internal layer l, its effective count and delta-M fraction,
-  // as the forward pass formed them (f < 0: no truncation scaling)
+  // moment set of internal layer l, its effective count and delta-M fraction
   auto moments = [&](int l, int& nuse, double& f) -> const double* {
     const int u = fb ? nL - 1 - l : l;
     const double* chi = C->moments + (layout == 0 ? (size_t)u * M
                                       : layout == 1 ? (size_t)w * M
                                                     : ((size_t)w * nL + u) * M);
-    nuse = M;
-    f = -1.0;
-    if (C->delta_m) {
-      const double ff = (M > 2 * N) ? chi[2 * N] : 0.0;
-      if (ff > 1e-12 && ff < 1.0 - 1e-12) {
-        f = ff;
-        nuse = 2 * N;
-      } else {
-        nuse = (M < 2 * N) ? M : 2 * N;
-      }
-    }
+    moment_use(C, chi, nuse, f);
     return chi;
   };
   auto cot = [&](const double* a, int l) { return a ? a[wo + ui(l)] : 0.0; };
@@ -952,6 +982,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   auto vo = [&](int s) { return X.mo(J_VEC) + (unsigned)(s * NP * sizeof(Real)); };
   const Tile<Gm> tl(t);
   int singular = 0;
+  const bool table = (layout == 0) && (AD.ptab != nullptr);
 
   for (int l = t; l <= nL; l += G) {
     bB[l] = 0.0;
@@ -960,6 +991,22 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     gom[l] = 0.0;
   }
   for (int e = t; e < 2 * TILE + 2 * NP; e += G) pacc[e] = 0.0;
+  if (solar && t == 0) {  // P_l(mu0) by the recurrence the phase vectors use
+    double p0 = 1.0, p1 = mu0;
+    for (int l = 0; l < M; ++l) {
+      double plm;
+      if (l == 0) {
+        plm = 1.0;
+      } else if (l == 1) {
+        plm = mu0;
+      } else {
+        plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);
+        p0 = p1;
+        p1 = plm;
+      }
+      plm0[l] = plm;
+    }
+  }
   X.sync();
 
   // ======== 1. downward-pass adjoint (interface L-1 .. 0); bId carried in A_BDN
@@ -1231,23 +1278,56 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       int nuse;
       double f;
       const double* chi = moments(l, nuse, f);
+      const size_t set = (size_t)(chi - C->moments) / (size_t)M;
       nuse_l1 = nuse;
-      if (layout != 1)
-        build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+      const double* lPpp = Ppp;
+      const double* lPpm = Ppm;
+      if (table) {  // shared moments: the layer's matrices from the table
+        lPpp = AD.ptab + set * 2 * NP * NP;
+        lPpm = lPpp + NP * NP;
+        if (solar)
+          build_phase<Gm, false, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar,
+                                       mu0, nullptr, nullptr, plm0);
+      } else if (layout != 1) {
+        build_phase<Gm, true, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar,
+                                    mu0, Ppp, Ppm, plm0);
+      }
       const long long to = tape_all ? toff[l] : -1;
       doubling_adjoint<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,
-                           Ppp, Ppm, to >= 0 ? tape_all + to : tape, to < 0, scal, &singular);
-      if (t == 0) {
-        gtau[l] += scal[0];
-        gom[l] += scal[1];
-        bB[l] += scal[2];
-        bB[l + 1] += scal[3];
-        if (solar) btc[l] += scal[4] * F0 * exp(-lv.tc[l] / mu0) * (-1.0 / mu0);
+                           lPpp, lPpm, to >= 0 ? tape_all + to : tape, to < 0, scal, &singular);
+      if (t == 0) {  // every load first: the regions are disjoint
+        const double s0 = scal[0], s1 = scal[1], s2 = scal[2], s3 = scal[3], s4 = scal[4];
+        const double a0 = gtau[l], a1 = gom[l], a2 = bB[l], a3 = bB[l + 1], a4 = btc[l];
+        const double tc = lv.tc[l];
+        gtau[l] = a0 + s0;
+        gom[l] = a1 + s1;
+        bB[l] = a2 + s2;
+        bB[l + 1] = a3 + s3;
+        if (solar) btc[l] = a4 + s4 * F0 * exp(-tc / mu0) * (-1.0 / mu0);
       }
       if (layout != 1) {
         double* dchi = AD.g_mom ? AD.g_mom + (chi - C->moments) : nullptr;
-        if (dchi)
-          phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl, solar, mu0, dchi);
+        if (dchi && table && AD.pacc) {
+          // the matrix part is linear in the cotangents: summed per block and
+          // set here (no return value: fire-and-forget reductions), run once
+          // per set after the last chunk; the solar part now
+          if (tl.valid()) {
+            double* a = AD.pacc + (set * AD.pacc_blocks + blockIdx.x) * 2 * TILE + t * Gm::TE;
+#pragma unroll
+            for (int i = 0; i < TR; ++i)
+#pragma unroll
+              for (int j = 0; j < TC; ++j) {
+                atomicAdd(a + i * TC + j, X.m(J_T1)[tl.row(i) * LD + tl.col(j)]);
+                atomicAdd(a + TILE + i * TC + j, X.m(J_T2)[tl.row(i) * LD + tl.col(j)]);
+              }
+          }
+          if (solar)
+            phase_adjoint<Gm, false, true>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl,
+                                           solar, mu0, dchi, plm0);
+        } else if (dchi) {
+          phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl, solar, mu0, dchi,
+                            plm0);
+        }
       } else {  // one moment set per wavenumber: accumulate the phase cotangents
         if (tl.valid()) {
           double* aP = pacc + t * Gm::TE;
@@ -1310,7 +1390,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     X.sync();
     const double* chi = C->moments + (size_t)w * M;
     phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse_l1, N, C->quad.pl, solar, mu0,
-                      AD.g_mom + (size_t)w * M);
+                      AD.g_mom + (size_t)w * M, plm0);
   }
   // ======== 3. lower boundary, beam and Planck chain rules
   double pub = 0.0, pubmu = 0.0;
@@ -1490,6 +1570,86 @@ __global__ void __launch_bounds__(AdjKern<NP>::kThreads) adjoint_kernel(SolvePar
     wav_prologue<NP, adjoint_group<NP>()>(goff, t, bar, w, st, P.max_layers, P.status, 0);
     wav_adjoint<NP>(goff, tb, t, bar, w, st, scr, P.max_layers, P.status, AD);
   }
+}
+
+// One reverse-geometry group per block, for the per-moment-set kernels below:
+// cleared shared memory, the column and the quadrature constants.
+template <int NP>
+__device__ __forceinline__ Ctx<AdjGeo<NP>> set_group(const ColumnDev& col0, int t) {
+  using Gm = AdjGeo<NP>;
+  constexpr int G = Gm::G;
+  for (unsigned i = (unsigned)t * 4u; i < (unsigned)AdjGroup<NP>::bytes; i += (unsigned)G * 4u)
+    *sp<unsigned>(i) = 0u;
+  gsync<G>(1);
+  if (t == 0) *sp<ColumnDev>(CommonLayout<NP>::col) = col0;
+  const Ctx<Gm> X(0u, (unsigned)CommonLayout<NP>::bytes, t, 1);
+  if (t < NP) {
+    const bool q = t < col0.N;
+    const double mu = q ? col0.quad.mu[t] : 1.0, wt = q ? col0.quad.wt[t] : 0.0;
+    X.DV(D_MU)[t] = mu;
+    X.DV(D_WT)[t] = wt;
+    X.DV(D_CW)[t] = 2.0 * kPi * wt * mu;
+    X.DV(D_HW)[t] = 0.5 * wt;
+  }
+  gsync<G>(1);
+  return X;
+}
+
+// Phase matrices of the moment sets that every wavenumber shares (one per
+// layer), once per adjoint call instead of once per wavenumber and layer:
+// block u forms set u's normalised P++ / P+- into tab[u] (row-major, pitch NP).
+template <int NP>
+__global__ void __launch_bounds__(AdjGeo<NP>::G) phase_table_kernel(ColumnDev col0, double* tab) {
+  using Gm = AdjGeo<NP>;
+  const int t = threadIdx.x;
+  const Ctx<Gm> X = set_group<NP>(col0, t);
+  const size_t u = blockIdx.x;
+  const double* chi = col0.moments + u * col0.M;
+  int nuse;
+  double f;
+  moment_use(&col0, chi, nuse, f);
+  double* P = tab + u * 2 * NP * NP;
+  build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, col0.N, col0.quad.pl, false, 1.0, P,
+                  P + NP * NP);
+}
+
+// The moment gradients of the shared sets from the phase-matrix cotangents
+// that the reverse pass summed per block: block u adds the blocks' sums of
+// set u and runs the matrix part of phase_adjoint once.
+template <int NP>
+__global__ void __launch_bounds__(AdjGeo<NP>::G) phase_finish_kernel(ColumnDev col0, AdjDev AD) {
+  using Gm = AdjGeo<NP>;
+  constexpr int TR = Gm::TR, TC = Gm::TC, TE = Gm::TE, TILE = Gm::G * Gm::TE;
+  const int t = threadIdx.x;
+  const Ctx<Gm> X = set_group<NP>(col0, t);
+  const size_t u = blockIdx.x;
+  const Tile<Gm> tl(t);
+  if (tl.valid()) {
+    double sP[TR][TC], sM[TR][TC];
+#pragma unroll
+    for (int i = 0; i < TR; ++i)
+#pragma unroll
+      for (int j = 0; j < TC; ++j) sP[i][j] = sM[i][j] = 0.0;
+    const double* a = AD.pacc + u * AD.pacc_blocks * 2 * TILE + t * TE;
+#pragma unroll 4
+    for (int b = 0; b < AD.pacc_blocks; ++b, a += 2 * TILE)
+#pragma unroll
+      for (int i = 0; i < TR; ++i)
+#pragma unroll
+        for (int j = 0; j < TC; ++j) {
+          sP[i][j] += a[i * TC + j];
+          sM[i][j] += a[TILE + i * TC + j];
+        }
+    tl.store_rm(sP, X.m(J_T1));
+    tl.store_rm(sM, X.m(J_T2));
+  }
+  X.sync();
+  const double* chi = col0.moments + u * col0.M;
+  int nuse;
+  double f;
+  moment_use(&col0, chi, nuse, f);
+  phase_adjoint<Gm, true, false>(X.goff, X.tb, t, X.bar, chi, nuse, col0.N, col0.quad.pl, false,
+                                 1.0, AD.g_mom + u * col0.M, nullptr);
 }
 
 }  // namespace adrt_dev

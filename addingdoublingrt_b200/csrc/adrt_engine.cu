@@ -754,12 +754,15 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   // leaves each wavenumber's state and doubling records in HBM, then
   // adjoint_kernel runs the reverse on them.
   struct AK {
-    int groups, threads, fgroups, fthreads;
-    size_t smem, fsmem, scr, state;
+    int groups, threads, fgroups, fthreads, gthreads, np, tile;
+    size_t smem, fsmem, gsmem, scr, state;
     long long step;  // doubles per recorded doubling step
-    const void *fn, *ffn;
+    const void *fn, *ffn, *tfn, *pfn;
     void (*launch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
     void (*flaunch)(const SolveParams&, const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
+    // per shared moment set: phase table, and the moment gradients' finish
+    void (*tlaunch)(const ColumnDev&, double*, int, size_t, cudaStream_t);
+    void (*plaunch)(const ColumnDev&, const AdjDev&, int, size_t, cudaStream_t);
   } k{};
   const int L = d->num_layers;
   auto make = [&](auto tag) {
@@ -769,7 +772,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
     k.groups = AdjKern<NP>::kGroups;
     k.threads = AdjKern<NP>::kThreads;
     k.smem = (size_t)k.groups * AdjGroup<NP>::bytes;
-    k.scr = align256(AdjScratch<GD>::bytes(L));
+    k.scr = align256(AdjScratch<GD>::bytes(L, d->num_moments));
     k.state = align256(WavState<GC>::bytes(L));
     k.step = TapeLayout<GC>::STEP;
     k.fthreads = Kern<NP, KIND_FP64>::kThreads;
@@ -785,6 +788,18 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
                    size_t smem, cudaStream_t st) {
       tape_kernel<NP><<<grid, Kern<NP, KIND_FP64>::kThreads, smem, st>>>(p, c, a);
     };
+    k.np = NP;
+    k.tile = GD::G * GD::TE;
+    k.gthreads = GD::G;
+    k.gsmem = AdjGroup<NP>::bytes;
+    k.tfn = reinterpret_cast<const void*>(phase_table_kernel<NP>);
+    k.pfn = reinterpret_cast<const void*>(phase_finish_kernel<NP>);
+    k.tlaunch = [](const ColumnDev& c, double* tab, int sets, size_t smem, cudaStream_t st) {
+      phase_table_kernel<NP><<<sets, GD::G, smem, st>>>(c, tab);
+    };
+    k.plaunch = [](const ColumnDev& c, const AdjDev& a, int sets, size_t smem, cudaStream_t st) {
+      phase_finish_kernel<NP><<<sets, GD::G, smem, st>>>(c, a);
+    };
   };
   switch (np) {
     case 4: make(std::integral_constant<int, 4>{}); break;
@@ -794,6 +809,8 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   }
   CUDA_TRY(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
   CUDA_TRY(cudaFuncSetAttribute(k.ffn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.fsmem));
+  CUDA_TRY(cudaFuncSetAttribute(k.tfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.gsmem));
+  CUDA_TRY(cudaFuncSetAttribute(k.pfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.gsmem));
   int bps = 0, fbps = 0;
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k.fn, k.threads, k.smem));
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fbps, k.ffn, k.fthreads, k.fsmem));
@@ -805,13 +822,27 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   const size_t rev_bytes = (size_t)rgroups * k.scr;
   const size_t per_w = k.state + (size_t)L * kTapeStepsPerLayer * k.step * sizeof(double);
   const size_t budget = e->max_ws ? e->max_ws : kAdjointMemory;
-  if (budget < rev_bytes + per_w)
+  // moment sets shared by every wavenumber (one per layer): their phase
+  // matrices once per call, and per-block sums of the phase-matrix cotangents
+  // (within kPhaseSumMemory and the budget; else the sets' adjoint runs per
+  // layer)
+  const bool shared_sets = d->moment_layout == ADRT_MOMENTS_SHARED;
+  const int sum_blocks = bps * e->num_sms;
+  const size_t ptab_bytes = shared_sets ? align256((size_t)L * 2 * k.np * k.np * sizeof(double)) : 0;
+  size_t psum_bytes = (shared_sets && gr->phase_moments)
+                          ? align256((size_t)L * sum_blocks * 2 * k.tile * sizeof(double)) : 0;
+  if (psum_bytes > kPhaseSumMemory || budget < rev_bytes + per_w + ptab_bytes + psum_bytes)
+    psum_bytes = 0;
+  const size_t fixed = rev_bytes + ptab_bytes + psum_bytes + 512;
+  if (budget < fixed + per_w)
     return fail(ADRT_ERR_WORKSPACE, "workspace limit below one adjoint chunk (%zu B)",
-                rev_bytes + per_w);
+                fixed + per_w);
   long long wc = std::min<long long>(W, (long long)fbps * e->num_sms * k.fgroups);
-  wc = std::max<long long>(1, std::min<long long>(wc, (long long)((budget - rev_bytes) / per_w)));
+  wc = std::max<long long>(1, std::min<long long>(wc, (long long)((budget - fixed) / per_w)));
   const long long pool_cap = wc * L * kTapeStepsPerLayer * k.step;
-  const size_t need = rev_bytes + (size_t)wc * k.state + (size_t)pool_cap * sizeof(double) + 256;
+  const size_t ext = align256(rev_bytes + (size_t)wc * k.state + (size_t)pool_cap * sizeof(double) +
+                              sizeof(unsigned long long));
+  const size_t need = ext + ptab_bytes + psum_bytes;
   if (need > e->adj_scratch_bytes) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cap);
@@ -852,6 +883,14 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   a.pool = reinterpret_cast<double*>(a.state + (size_t)wc * k.state);
   a.pool_cap = pool_cap;
   a.pool_used = reinterpret_cast<unsigned long long*>(a.pool + pool_cap);
+  a.ptab = ptab_bytes ? reinterpret_cast<double*>(e->adj_scratch + ext) : nullptr;
+  a.pacc = psum_bytes ? reinterpret_cast<double*>(e->adj_scratch + ext + ptab_bytes) : nullptr;
+  a.pacc_blocks = sum_blocks;
+  if (ptab_bytes) {
+    k.tlaunch(c0, const_cast<double*>(a.ptab), L, k.gsmem, s);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (psum_bytes) CUDA_TRY(cudaMemsetAsync(a.pacc, 0, psum_bytes, s));
   for (long long w0 = 0; w0 < W; w0 += wc) {
     const long long nw = std::min(wc, W - w0);
     a.w0 = w0;
@@ -867,6 +906,10 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
     k.launch(p, c0, a, rgrid, k.smem, s);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (psum_bytes) {
+    k.plaunch(c0, a, L, k.gsmem, s);
     CUDA_TRY(cudaGetLastError());
   }
   return ADRT_OK;

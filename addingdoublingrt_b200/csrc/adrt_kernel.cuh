@@ -277,48 +277,55 @@ __device__ __forceinline__ void phase_products(const double* chi, int nuse, doub
   }
 }
 
-template <class Gm>
+// Phase matrices P++ / P+- (normalised, row-major, pitch NP) into Ppp / Ppm
+// and, with `solar`, the solar phase vectors into D_PP / D_PM; without MAT
+// the solar vectors only (the matrices of a moment set shared by every
+// wavenumber come from a table).  With PL0, plm0[l] = P_l(mu0) for l < nuse
+// (formed once per wavenumber by the same recurrence).
+template <class Gm, bool MAT = true, bool PL0 = false>
 __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
                                          const double* chi, int nuse, double f, int N,
                                          const double* pl, bool solar, double mu0, double* Ppp,
-                                         double* Ppm) {
+                                         double* Ppm, const double* plm0 = nullptr) {
   constexpr int NP = Gm::NP, G = Gm::G;
   const Ctx<Gm> X(goff, tb, t_, bar);
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
-  if constexpr (UsePhaseMMA<Gm>::value)
-    // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
-    phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
-  else
-  for (int e = t; e < NP * NP; e += G) {
-    const int r = e / NP, c = e % NP;
-    double spp = 0.0, spm = 0.0;
-    if (r < N && c < N) {
-      double sign = 1.0;
-      for (int l = 0; l < nuse; ++l) {
-        const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
-        const double term = (2 * l + 1) * cl * pl[l * N + r] * pl[l * N + c];
-        spp += term;
-        spm += sign * term;
-        sign = -sign;
+  if constexpr (MAT) {
+    if constexpr (UsePhaseMMA<Gm>::value)
+      // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
+      phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
+    else
+    for (int e = t; e < NP * NP; e += G) {
+      const int r = e / NP, c = e % NP;
+      double spp = 0.0, spm = 0.0;
+      if (r < N && c < N) {
+        double sign = 1.0;
+        for (int l = 0; l < nuse; ++l) {
+          const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
+          const double term = (2 * l + 1) * cl * pl[l * N + r] * pl[l * N + c];
+          spp += term;
+          spm += sign * term;
+          sign = -sign;
+        }
+        spp /= (2.0 * kPi);
+        spm /= (2.0 * kPi);
       }
-      spp /= (2.0 * kPi);
-      spm /= (2.0 * kPi);
+      Ppp[e] = spp;
+      Ppm[e] = spm;
     }
-    Ppp[e] = spp;
-    Ppm[e] = spm;
-  }
-  X.sync();
-  if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
-    const int c = t;
-    double sum = 0.0;
-    for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
-    if (sum > 0.0) {
-      const double corr = 1.0 / (2.0 * kPi * sum);
-      for (int i = 0; i < N; ++i) {
-        Ppp[i * NP + c] *= corr;
-        Ppm[i * NP + c] *= corr;
+    X.sync();
+    if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
+      const int c = t;
+      double sum = 0.0;
+      for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
+      if (sum > 0.0) {
+        const double corr = 1.0 / (2.0 * kPi * sum);
+        for (int i = 0; i < N; ++i) {
+          Ppp[i * NP + c] *= corr;
+          Ppm[i * NP + c] *= corr;
+        }
       }
     }
   }
@@ -328,23 +335,48 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
     if (t < NP) {
       double sp = 0.0, sm = 0.0;
       if (t < N) {
-        double sign = 1.0, p0 = 1.0, p1 = mu0;
-        for (int l = 0; l < nuse; ++l) {
-          double plm;
-          if (l == 0) {
-            plm = 1.0;
-          } else if (l == 1) {
-            plm = mu0;
-          } else {
-            plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);  // off the chain
-            p0 = p1;
-            p1 = plm;
+        if constexpr (PL0) {
+          // the same sums, their loads issued eight at a time (these small
+          // tables mostly miss L1 beside the adjoint's shared memory)
+          for (int l0 = 0; l0 < nuse; l0 += 8) {
+            double c[8], p[8], q[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int l = (l0 + j < nuse) ? l0 + j : 0;
+              c[j] = chi[l];
+              p[j] = pl[l * N + t];
+              q[j] = plm0[l];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int l = l0 + j;
+              if (l < nuse) {
+                const double cl = (f >= 0.0) ? (c[j] - f) * inv_1mf : c[j];
+                const double term = (2 * l + 1) * cl * p[j] * q[j];
+                sp += term;
+                sm += (l & 1) ? -term : term;
+              }
+            }
           }
-          const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
-          const double term = (2 * l + 1) * cl * pl[l * N + t] * plm;
-          sp += term;
-          sm += sign * term;
-          sign = -sign;
+        } else {
+          double sign = 1.0, p0 = 1.0, p1 = mu0;
+          for (int l = 0; l < nuse; ++l) {
+            double plm;
+            if (l == 0) {
+              plm = 1.0;
+            } else if (l == 1) {
+              plm = mu0;
+            } else {
+              plm = ((2 * l - 1) * mu0 * p1 - (l - 1) * p0) * recip((double)l);  // off the chain
+              p0 = p1;
+              p1 = plm;
+            }
+            const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
+            const double term = (2 * l + 1) * cl * pl[l * N + t] * plm;
+            sp += term;
+            sm += sign * term;
+            sign = -sign;
+          }
         }
         sp /= (2.0 * kPi);
         sm /= (2.0 * kPi);
