@@ -353,8 +353,11 @@ struct AdjScratch {
   static __host__ __device__ size_t plm(int m) {  // P_l(mu0), l < M
     return ((size_t)m * sizeof(double) + 255) & ~size_t(255);
   }
+  static __host__ __device__ size_t svec(int lmax) {  // per layer: p+, p-, q+, q-
+    return ((size_t)lmax * 4 * NP * sizeof(double) + 255) & ~size_t(255);
+  }
   static __host__ __device__ size_t bytes(int lmax, int m) {
-    return dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256 + plm(m);
+    return dvec(lmax) + tape() + pacc() + brb() + acc(lmax) + 256 + plm(m) + svec(lmax);
   }
 };
 
@@ -724,7 +727,8 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
 // cotangents and independent: MAT the matrices' (which, for a moment set
 // shared by all wavenumbers, runs once on the cotangents summed over them),
 // SOL the solar vectors' (which depend on each wavenumber's mu0; plm0[l] =
-// P_l(mu0) for l < nuse).
+// P_l(mu0) for l < nuse, the un-normalised vectors in D_LAM0 / D_LAM1 as
+// build_phase<Gm, true> leaves them).
 template <class Gm, bool MAT = true, bool SOL = true>
 __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, int bar,
                                            const double* chi, int nuse, int N, const double* pl,
@@ -787,45 +791,20 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   }
   double bqscale = 0.0;
   if (solar) {
-    // un-normalised solar vectors and their normalisation; plm0[l] = P_l(mu0),
-    // the small tables' loads issued eight at a time (they mostly miss L1)
-    if (t < NP) {
-      double sp = 0.0, sm = 0.0;
-      if (t < N) {
-        for (int l0 = 0; l0 < nuse; l0 += 8) {
-          double c[8], p[8], q[8];
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l = (l0 + j < nuse) ? l0 + j : 0;
-            c[j] = chi[l];
-            p[j] = pl[l * N + t];
-            q[j] = plm0[l];
-          }
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l = l0 + j;
-            if (l < nuse) {
-              const double term = (2 * l + 1) * c[j] * p[j] * q[j];
-              sp += term;
-              sm += (l & 1) ? -term : term;
-            }
-          }
-        }
-      }
-      qp[t] = sp / (2.0 * kPi);
-      qm[t] = sm / (2.0 * kPi);
-    }
-    X.sync();
-    double ss = 0.0, bcs = 0.0;
+    // the un-normalised solar vectors (left in D_LAM0 / D_LAM1 by the build)
+    // and their normalisation
+    const double* qpu = X.DV(D_LAM0);
+    const double* qmu = X.DV(D_LAM1);
     const Real* dpp = vb + A_T0 * NP;
     const Real* dpm = vb + A_T1 * NP;
+    double ss = 0.0, bcs = 0.0;
 #pragma unroll
     for (int i = 0; i < NP; ++i)
-      if (i < N) ss += (qp[i] + qm[i]) * wt[i];
+      if (i < N) ss += (qpu[i] + qmu[i]) * wt[i];
     const double cs = (ss > 0.0) ? 1.0 / (2.0 * kPi * ss) : 1.0;
 #pragma unroll
     for (int i = 0; i < NP; ++i)
-      if (i < N) bcs += dpp[i] * qp[i] + dpm[i] * qm[i];
+      if (i < N) bcs += dpp[i] * qpu[i] + dpm[i] * qmu[i];
     bqscale = (ss > 0.0) ? -bcs * cs / ss : 0.0;
     X.sync();
     if (t < NP) {  // dq = dp cs + w dss
@@ -955,6 +934,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   double* acc = reinterpret_cast<double*>(p += AS::brb());        // bB, btc, dtau, dom
   double* scal = reinterpret_cast<double*>(p += AS::acc(lmax));   // 32 doubles
   double* plm0 = reinterpret_cast<double*>(p += 256);              // P_l(mu0), l < M
+  double* svec = reinterpret_cast<double*>(p += AS::plm(M));       // [L][p+, p-, q+, q-]
   const long long tbase = toff[nL];                               // this wavenumber's records
   double* tape_all = (tbase >= 0) ? AD.pool + tbase : nullptr;
   double* bB = acc;
@@ -1008,6 +988,67 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     }
   }
   X.sync();
+  if (table && solar) {
+    // every layer's solar phase vectors at once (they depend on the layer's
+    // moments and this wavenumber's mu0): q = sum_k (2k+1) chi_k P_k(mu_i)
+    // P_k(mu0) / 2 pi with the sign (-1)^k for q-, then p = q / (2 pi s)
+    for (int e = t; e < nL * NP; e += G) {
+      const int l = e / NP, i = e - l * NP;
+      double sp = 0.0, sm = 0.0;
+      if (i < N) {
+        int nuse;
+        double f;
+        const double* chi = moments(l, nuse, f);
+        const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
+        for (int k0 = 0; k0 < nuse; k0 += 8) {
+          double c[8], pk[8], q[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int k = (k0 + j < nuse) ? k0 + j : 0;
+            c[j] = chi[k];
+            pk[j] = C->quad.pl[k * N + i];
+            q[j] = plm0[k];
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int k = k0 + j;
+            if (k < nuse) {
+              const double cl = (f >= 0.0) ? (c[j] - f) * inv_1mf : c[j];
+              const double term = (2 * k + 1) * cl * pk[j] * q[j];
+              sp += term;
+              sm += (k & 1) ? -term : term;
+            }
+          }
+        }
+        sp /= (2.0 * kPi);
+        sm /= (2.0 * kPi);
+      }
+      svec[(size_t)l * 4 * NP + 2 * NP + i] = sp;
+      svec[(size_t)l * 4 * NP + 3 * NP + i] = sm;
+    }
+    X.sync();
+    const double* wq = X.DV(D_WT);
+    for (int l = t; l < nL; l += G) {
+      double* q = svec + (size_t)l * 4 * NP;
+      double qp[NP], qm[NP];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        qp[i] = q[2 * NP + i];
+        qm[i] = q[3 * NP + i];
+      }
+      double ss = 0.0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i)
+        if (i < N) ss += (qp[i] + qm[i]) * wq[i];
+      const double cs = (ss > 0.0) ? 1.0 / (2.0 * kPi * ss) : 1.0;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        q[i] = (i < N) ? qp[i] * cs : qp[i];
+        q[NP + i] = (i < N) ? qm[i] * cs : qm[i];
+      }
+    }
+    X.sync();
+  }
 
   // ======== 1. downward-pass adjoint (interface L-1 .. 0); bId carried in A_BDN
   if (X.warp == 0 && X.lane < NP) {
@@ -1112,7 +1153,8 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     double f;
     const double* chi = moments(0, nuse, f);
     nuse_l1 = nuse;
-    build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp, Ppm);
+    build_phase<Gm, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
+                          Ppm, plm0);
   }
   for (int l = 0; l < nL; ++l) {
     const double* rl = recs + (size_t)l * REC;
@@ -1285,12 +1327,13 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       if (table) {  // shared moments: the layer's matrices from the table
         lPpp = AD.ptab + set * 2 * NP * NP;
         lPpm = lPpp + NP * NP;
-        if (solar)
-          build_phase<Gm, false, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar,
-                                       mu0, nullptr, nullptr, plm0);
+        if (solar) {  // and its solar vectors from this wavenumber's start
+          if (t < 4 * NP) X.DV(D_PP)[t] = svec[(size_t)l * 4 * NP + t];
+          X.sync();
+        }
       } else if (layout != 1) {
-        build_phase<Gm, true, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar,
-                                    mu0, Ppp, Ppm, plm0);
+        build_phase<Gm, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0,
+                              Ppp, Ppm, plm0);
       }
       const long long to = tape_all ? toff[l] : -1;
       doubling_adjoint<Gm>(X.goff, X.tb, t, X.bar, tau, om, Bt, Bb, lv.tc[l], N, solar, F0, mu0,

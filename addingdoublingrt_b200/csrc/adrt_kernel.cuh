@@ -278,11 +278,10 @@ __device__ __forceinline__ void phase_products(const double* chi, int nuse, doub
 }
 
 // Phase matrices P++ / P+- (normalised, row-major, pitch NP) into Ppp / Ppm
-// and, with `solar`, the solar phase vectors into D_PP / D_PM; without MAT
-// the solar vectors only (the matrices of a moment set shared by every
-// wavenumber come from a table).  With PL0, plm0[l] = P_l(mu0) for l < nuse
-// (formed once per wavenumber by the same recurrence).
-template <class Gm, bool MAT = true, bool PL0 = false>
+// and, with `solar`, the solar phase vectors into D_PP / D_PM.  With PL0,
+// plm0[l] = P_l(mu0) for l < nuse (formed once per wavenumber by the same
+// recurrence) and the un-normalised solar vectors also go to D_LAM0 / D_LAM1.
+template <class Gm, bool PL0 = false>
 __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
                                          const double* chi, int nuse, double f, int N,
                                          const double* pl, bool solar, double mu0, double* Ppp,
@@ -292,40 +291,38 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
-  if constexpr (MAT) {
-    if constexpr (UsePhaseMMA<Gm>::value)
-      // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
-      phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
-    else
-    for (int e = t; e < NP * NP; e += G) {
-      const int r = e / NP, c = e % NP;
-      double spp = 0.0, spm = 0.0;
-      if (r < N && c < N) {
-        double sign = 1.0;
-        for (int l = 0; l < nuse; ++l) {
-          const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
-          const double term = (2 * l + 1) * cl * pl[l * N + r] * pl[l * N + c];
-          spp += term;
-          spm += sign * term;
-          sign = -sign;
-        }
-        spp /= (2.0 * kPi);
-        spm /= (2.0 * kPi);
+  if constexpr (UsePhaseMMA<Gm>::value)
+    // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
+    phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
+  else
+  for (int e = t; e < NP * NP; e += G) {
+    const int r = e / NP, c = e % NP;
+    double spp = 0.0, spm = 0.0;
+    if (r < N && c < N) {
+      double sign = 1.0;
+      for (int l = 0; l < nuse; ++l) {
+        const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
+        const double term = (2 * l + 1) * cl * pl[l * N + r] * pl[l * N + c];
+        spp += term;
+        spm += sign * term;
+        sign = -sign;
       }
-      Ppp[e] = spp;
-      Ppm[e] = spm;
+      spp /= (2.0 * kPi);
+      spm /= (2.0 * kPi);
     }
-    X.sync();
-    if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
-      const int c = t;
-      double sum = 0.0;
-      for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
-      if (sum > 0.0) {
-        const double corr = 1.0 / (2.0 * kPi * sum);
-        for (int i = 0; i < N; ++i) {
-          Ppp[i * NP + c] *= corr;
-          Ppm[i * NP + c] *= corr;
-        }
+    Ppp[e] = spp;
+    Ppm[e] = spm;
+  }
+  X.sync();
+  if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
+    const int c = t;
+    double sum = 0.0;
+    for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
+    if (sum > 0.0) {
+      const double corr = 1.0 / (2.0 * kPi * sum);
+      for (int i = 0; i < N; ++i) {
+        Ppp[i * NP + c] *= corr;
+        Ppm[i * NP + c] *= corr;
       }
     }
   }
@@ -383,6 +380,10 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
       }
       pp[t] = sp;
       pm[t] = sm;
+      if constexpr (PL0) {
+        X.DV(D_LAM0)[t] = sp;
+        X.DV(D_LAM1)[t] = sm;
+      }
     }
     X.sync();
     double corr = 1.0;
