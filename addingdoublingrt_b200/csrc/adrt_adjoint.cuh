@@ -301,7 +301,9 @@ constexpr size_t kPhaseSumMemory = size_t(1) << 30;
 enum AdjVec {
   A_BY = 0, A_BZ, A_BSU, A_BSD, A_H, A_RU, A_RD, A_BRU, A_BRD, A_BH, A_Y, A_Z, A_SU, A_SD,
   A_BUP, A_BDN, A_T0, A_T1,
-  A_CUB  // the adding adjoint's carried d U_base (not touched by the layer adjoints)
+  A_CUB,  // the adding adjoint's carried d U_base (not touched by the layer adjoints)
+  A_X4, A_X5, A_X6,  // a doubling-adjoint step's TGR^T bsd, TGR^T bsu, R su
+  kAdjVecs
 };
 // Partial products of one doubling-adjoint step, in slots that are scratch
 // inside the step loop (z is only needed for h; T0 / T1 are written after it).
@@ -413,6 +415,7 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
                                               int* singular) {
   using Real = typename Gm::Real;
   static_assert(sizeof(Real) == 8, "the adjoint runs in FP64");
+  static_assert(kAdjVecs * Gm::NP <= 2 * Gm::MAT, "vector slots fit the two J_VEC buffers");
   using Tp = TapeLayout<Gm>;
   using GC = Geo<Gm::NP, double>;  // record order
   const Ctx<Gm> X(goff, tb, t_, bar);
@@ -546,6 +549,7 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
         const int i = X.lane;
         VA(A_RU)[i] = yv[0] + gam * VA(A_SU)[i];
         VA(A_RD)[i] = gam * yv[1] + VA(A_SD)[i];
+        VA(A_X6)[i] = yv[1];  // R su
       }
     }
     X.sync();
@@ -569,7 +573,17 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
                            X.mo(J_C), X.mo(J_Cc)), t);
     op_gemm_x<Gm, 2, 0>(gx(X.mo(J_TG), bTr, X.mo(J_TGR), bRr, kNoMat, kNoMat, X.mo(J_W), nTr,
                            nTc), t);
-    // the vector cotangents' products, one warp each
+    // the vector cotangents' products, one warp each; R^T TG^T = TGR^T turns
+    // the next phase's R^T brd, R^T bru into TGR^T bsd, TGR^T bsu, here
+    if (X.warp == 0) {
+      const Real* v0[2] = {VA(A_BSD), VA(A_BSU)};
+      Real rt[2];
+      matvec<Gm, true, 2>(X.m(J_TGR), v0, rt, X.lane);
+      if (X.lane < NP) {
+        VA(A_X4)[X.lane] = rt[0];
+        VA(A_X5)[X.lane] = rt[1];
+      }
+    }
     if (X.warp == 1 % NWG) {
       const Real* v1[2] = {VA(A_BSU), VA(A_BSD)};
       Real tgs[2];
@@ -607,46 +621,30 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       rk(a, A_BRD, A_SU, gam);
       op_gemm_x<Gm, 3, 2>(a, t);
     }
-    if (X.warp == 1 % NWG) {
-      const Real* v3[2] = {VA(A_BRD), VA(A_BRU)};
-      Real rt[2];
-      matvec<Gm, true, 2>(X.m(J_R), v3, rt, X.lane);  // R^T brd, R^T bru
-      const Real* v4[1] = {VA(A_SU)};
-      Real rsu[1];
-      matvec<Gm, true, 1>(X.m(J_Rc), v4, rsu, X.lane);  // R su
-      double pg = 0.0, pgam = 0.0;
-      if (X.lane < NP) {
-        const int i = X.lane;
-        const double bz = VA(A_BZ)[i], by = VA(A_BY)[i];
-        const double bh = VA(A_X0)[i] - VA(A_X2)[i];    // (TG - TGR)^T bz
-        const double bt0 = VA(A_X1)[i] + VA(A_X3)[i];   // (TG + TGR)^T by
-        const double bsu = VA(A_BSU)[i], bsd = VA(A_BSD)[i];
-        const double y = VA(A_Y)[i], su = VA(A_SU)[i], sd = VA(A_SD)[i];
-        const double bru = VA(A_BRU)[i], brd = VA(A_BRD)[i];
-        pg = -y * bz + y * bh;
-        pgam = sd * bsd + su * bru + rsu[0] * brd;
-        VA(A_BZ)[i] = bz + bh;
-        VA(A_BY)[i] = -g * bz + bt0 + by + g * bh;
-        VA(A_BSU)[i] = bsu + gam * bru + gam * rt[0];
-        VA(A_BSD)[i] = gam * bsd + rt[1] + brd;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        pg += __shfl_xor_sync(0xffffffffu, pg, o);
-        pgam += __shfl_xor_sync(0xffffffffu, pgam, o);
-      }
-      if (X.lane == 0) {
-        red[0] = pg;
-        red[1] = pgam;
-      }
+    if (X.warp == 1 % NWG && X.lane < NP) {
+      // g and gamma's cotangents obey bg' = pg + 2 bg, bgam' = pgam + 2 gam bgam,
+      // linear in the per-row terms: each lane carries its rows' share, summed
+      // after the chain
+      const int i = X.lane;
+      const double bz = VA(A_BZ)[i], by = VA(A_BY)[i];
+      const double bh = VA(A_X0)[i] - VA(A_X2)[i];    // (TG - TGR)^T bz
+      const double bt0 = VA(A_X1)[i] + VA(A_X3)[i];   // (TG + TGR)^T by
+      const double bsu = VA(A_BSU)[i], bsd = VA(A_BSD)[i];
+      const double y = VA(A_Y)[i], su = VA(A_SU)[i], sd = VA(A_SD)[i];
+      const double bru = VA(A_BRU)[i], brd = VA(A_BRD)[i];
+      const double rtd = VA(A_X4)[i], rtu = VA(A_X5)[i], rsu = VA(A_X6)[i];
+      bg = (-y * bz + y * bh) + 2.0 * bg;
+      bgam = (sd * bsd + su * bru + rsu * brd) + 2.0 * gam * bgam;
+      VA(A_BZ)[i] = bz + bh;
+      VA(A_BY)[i] = -g * bz + bt0 + by + g * bh;
+      VA(A_BSU)[i] = bsu + gam * bru + gam * rtd;
+      VA(A_BSD)[i] = gam * bsd + rtu + brd;
     }
-    X.sync();
-    const double pg = red[0], pgam = red[1];
-    bgam = pgam + 2.0 * gam * bgam;
-    bg = pg + 2.0 * bg;
     cs ^= 1;
   }
   X.sync();
+  bg = gsum<G>(bg, red, bar);
+  bgam = gsum<G>(bgam, red, bar);
   // 3. first-order start: T0 = I - tau0 Gpp, R0 = tau0 Gpm, y0 = (1-om) tau0/mu,
   //    su0 / sd0 = om tau0 Ftop p-/p+ / mu, g0 = tau0/2, gam0 = exp(-tau0/mu0)
   const unsigned bRr = X.mo(cs ? J_bR1 : J_bR0), bTr = X.mo(cs ? J_bT1 : J_bT0);
