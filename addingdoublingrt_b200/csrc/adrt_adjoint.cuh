@@ -468,7 +468,7 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   // the record of step k - 1 is fetched into registers while step k runs
   const Tile<Gm> tlp(t);
   Real nR[TR][TC], nT[TR][TC], nG[TR][TC], nA[TR][TC];
-  double nv[4] = {0.0, 0.0, 0.0, 0.0}, ngam = 0.0;
+  double nv[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, ngam = 0.0;
   auto fetch = [&](int k) {
     const double* tk = tape + (size_t)k * Tp::STEP;
     if (tlp.valid()) {
@@ -486,6 +486,10 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
     if (X.warp == 0 && X.lane < NP) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) nv[j] = tk[Tp::OFF_VEC + j * NP + X.lane];
+      if (solar) {
+#pragma unroll
+        for (int j = 0; j < 3; ++j) nv[4 + j] = tk[Tp::OFF_SOL + j * NP + X.lane];
+      }
     }
     ngam = tk[Tp::OFF_VEC + 4 * NP];
   };
@@ -528,10 +532,13 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       VA(A_H)[i] = nv[1] + g * nv[0];
       VA(A_SU)[i] = nv[2];
       VA(A_SD)[i] = nv[3];
+      VA(A_RU)[i] = nv[4];  // R sd + gam su
+      VA(A_RD)[i] = nv[5];  // gam R su + sd
+      VA(A_X6)[i] = nv[6];  // R su
     }
     if (k > 0) fetch(k - 1);
     X.sync();
-    // 2. TGR = TG R;  dTGR = dR T^T - bz h^T + by y^T;  ru = R sd + gam su, rd = gam R su + sd
+    // 2. TGR = TG R;  dTGR = dR T^T - bz h^T + by y^T
     op_gemm_x<Gm, 1, 0>(gx(X.mo(J_TGc), X.mo(J_R), kNoMat, kNoMat, kNoMat, kNoMat, kNoMat,
                            X.mo(J_TGR), kNoMat), t);
     {
@@ -540,17 +547,6 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
       rk(a, A_BZ, A_H, -1.0);
       rk(a, A_BY, A_Y, 1.0);
       op_gemm_x<Gm, 1, 2>(a, t);
-    }
-    if (X.warp == 3 % NWG) {
-      const Real* vv[2] = {VA(A_SD), VA(A_SU)};
-      Real yv[2];
-      matvec<Gm, true, 2>(X.m(J_Rc), vv, yv, X.lane);
-      if (X.lane < NP) {
-        const int i = X.lane;
-        VA(A_RU)[i] = yv[0] + gam * VA(A_SU)[i];
-        VA(A_RD)[i] = gam * yv[1] + VA(A_SD)[i];
-        VA(A_X6)[i] = yv[1];  // R su
-      }
     }
     X.sync();
     // 3. dTG = dTGR R^T + dT T^T + bz h^T + by y^T + bsu ru^T + bsd rd^T (column-major)

@@ -75,15 +75,18 @@ struct SlotLayout {
 
 // One step of the adjoint's doubling record (per layer, nn steps): R, T, TG
 // tiles (TG taken from its column-major buffer, i.e. TG^T in tile order),
-// (I - R^2)^{-1}, then y, z, s_up, s_dn and gamma.  After the nn steps, a
-// tail holds the final y and z of the chain.
+// (I - R^2)^{-1}, then y, z, s_up, s_dn and gamma, and with a solar beam the
+// step's r_up = R s_dn + gamma s_up, r_dn = gamma R s_up + s_dn and R s_up
+// (unwritten without one).  After the nn steps, a tail holds the final y and
+// z of the chain.
 template <class Gm>
 struct TapeLayout {
   static constexpr int NP = Gm::NP;
   static constexpr int TILE = Gm::G * Gm::TE;
   static constexpr int OFF_R = 0, OFF_T = TILE, OFF_TG = 2 * TILE, OFF_AI = 3 * TILE;
   static constexpr int OFF_VEC = 4 * TILE;  // y, z, s_up, s_dn (NP each), gamma
-  static constexpr int STEP = (4 * TILE + 4 * NP + 1 + 1) / 2 * 2;
+  static constexpr int OFF_SOL = OFF_VEC + 4 * NP + 2;  // r_up, r_dn, R s_up
+  static constexpr int STEP = (OFF_SOL + 3 * NP + 1) / 2 * 2;
   static constexpr int TAIL = 2 * NP;
   static __host__ __device__ long long layer(int nn) { return (long long)nn * STEP + TAIL; }
 };
@@ -495,8 +498,15 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
       Real yv[2];
       matvec<Gm, false, 2>(Rrm, vv, yv, X.lane);
       if (X.lane < NP) {
-        X.V(V_RU)[X.lane] = yv[0] + gam * su[X.lane];
-        X.V(V_RD)[X.lane] = gam * yv[1] + sd[X.lane];
+        const Real ru = yv[0] + gam * su[X.lane], rd = gam * yv[1] + sd[X.lane];
+        X.V(V_RU)[X.lane] = ru;
+        X.V(V_RD)[X.lane] = rd;
+        if constexpr (taping) {
+          Real* tv = tape + (size_t)k * Tp::STEP + Tp::OFF_SOL;
+          tv[X.lane] = ru;
+          tv[NP + X.lane] = rd;
+          tv[2 * NP + X.lane] = yv[1];
+        }
       }
     }
     op_gemm<Gm, true>(oR, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2 (X = R row-major)
