@@ -260,6 +260,32 @@ __device__ __forceinline__ void op_gemm_x(const GemmX g, int t) {
   }
 }
 
+// N matrices from global memory into shared memory (row- and / or
+// column-major; kNoMat skips), every load issued before the first store so
+// that their latencies overlap.  Bit n of OWN: matrix n is in this group's
+// own tile order, else in GO's (a record of the taping forward).
+template <class Gm, class GO, int N, unsigned OWN>
+__device__ __forceinline__ void g2s_n(const double* const (&g)[N], const unsigned (&orm)[N],
+                                      const unsigned (&ocm)[N], int t) {
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  double X[N][TR][TC];
+#pragma unroll
+  for (int n = 0; n < N; ++n)
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+        X[n][a][b] = ((OWN >> n) & 1u) ? g[n][t * Gm::TE + a * TC + b]
+                                       : g[n][tile_index<GO>(tl.row(a), tl.col(b))];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    if (orm[n] != kNoMat) tl.store_rm(X[n], sp<double>(orm[n]));
+    if (ocm[n] != kNoMat) tl.store_cm(X[n], sp<double>(ocm[n]));
+  }
+}
+
 // Copy a row-major matrix into row-major and/or column-major buffers, scaled.
 template <class Gm>
 __device__ __noinline__ void op_copy(unsigned in_rm, unsigned orm, unsigned ocm, double scale,
@@ -1055,9 +1081,12 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     const int scat = rl[3 * TILE + 2 * NP] != 0.0;
     const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
     X.sync();
-    op_g2s<Gm, GC>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);  // R_base(l+1)
-    op_g2s<Gm, GC>(rl, X.mo(J_R), X.mo(J_Rc), t);               // R_l
-    op_g2s<Gm, GC>(rl + TILE, X.mo(J_TG), kNoMat, t);           // T_l (rm)
+    {  // R_base(l+1), R_l, T_l (rm)
+      const double* g[3] = {rb + 2 * TILE, rl, rl + TILE};
+      const unsigned orm[3] = {X.mo(J_TGR), X.mo(J_R), X.mo(J_TG)};
+      const unsigned ocm[3] = {X.mo(J_TGc), X.mo(J_Rc), kNoMat};
+      g2s_n<Gm, GC, 3, 0u>(g, orm, ocm, t);
+    }
     X.sync();
     if (X.warp == 0) {  // bIu(l+1), bx = Rb^T bIu + bId
       if (X.lane < NP) {
@@ -1157,10 +1186,12 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     const int cb = rb[3 * TILE + 2 * NP + 1] != 0.0;
     const double tau = lv.tau[l], om = lv.om[l];
     X.sync();
-    op_g2s<Gm, GC>(rl, X.mo(J_R), X.mo(J_Rc), t);
-    op_g2s<Gm, GC>(rl + TILE, X.mo(J_TG), X.mo(J_Tc), t);
-    op_g2s<Gm, GC>(rb + 2 * TILE, X.mo(J_TGR), X.mo(J_TGc), t);
-    op_g2s<Gm>(brb, X.mo(J_bTGR), X.mo(J_bTGRc), t);
+    {  // R_l, T_l, R_base(l+1) (records) and the carried d R_base (own order)
+      const double* g[4] = {rl, rl + TILE, rb + 2 * TILE, brb};
+      const unsigned orm[4] = {X.mo(J_R), X.mo(J_TG), X.mo(J_TGR), X.mo(J_bTGR)};
+      const unsigned ocm[4] = {X.mo(J_Rc), X.mo(J_Tc), X.mo(J_TGc), X.mo(J_bTGRc)};
+      g2s_n<Gm, GC, 4, 8u>(g, orm, ocm, t);
+    }
     if (X.warp == 0 && X.lane < NP) {
       const int i = X.lane;
       VA(A_Y)[i] = dv[(size_t)l * 2 * NP + i];                           // b_rhs(l)
