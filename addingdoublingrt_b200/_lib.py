@@ -37,6 +37,7 @@ EXPORTS = (
     "adrt_solve_batch_raw",
     "adrt_adjoint_host",
     "adrt_planck_band_deriv",
+    "adrt_band_integrate",
 )
 
 
@@ -84,6 +85,8 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                           P(_abi.Cotangents), P(_abi.Gradients)]
         lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),
                                              P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
+        lib.adrt_band_integrate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong,
+                                            C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),
                                      C.c_void_p, P(_abi.Cotangents), P(_abi.Gradients),
                                      C.c_void_p]

@@ -438,6 +438,43 @@ int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
 }  // namespace
 
 // ====================================================================== C ABI
+// Channel sums of a spectrum: one block per channel at a time (grid-stride
+// over channels), each thread a strided partial sum in wavenumber order, then
+// a fixed-shape block reduction.  HBM-bound: 8 or 16 bytes per wavenumber.
+__global__ void __launch_bounds__(256) band_integrate_kernel(const double* __restrict__ spec,
+                                                             const double* __restrict__ wgt,
+                                                             long long W,
+                                                             const long long* __restrict__ off,
+                                                             int nch, double* __restrict__ out,
+                                                             unsigned* status) {
+  __shared__ double part[8];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int b = blockIdx.x; b < nch; b += gridDim.x) {
+    const long long lo = off[b], hi = off[b + 1];
+    const bool ok = lo >= 0 && lo <= hi && hi <= W;
+    double acc = 0.0;
+    if (ok) {
+      for (long long w = lo + t; w < hi; w += blockDim.x)
+        acc += (wgt ? wgt[w] : 1.0) * spec[w];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) part[warp] = acc;
+    __syncthreads();
+    if (t == 0) {
+      double sum = 0.0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += part[i];
+      if (ok) {
+        out[b] = sum;
+      } else {
+        out[b] = __longlong_as_double(0x7ff8000000000000ll);
+        atomicOr(status, (unsigned)ADRT_FLAG_BAD_INPUT);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 extern "C" {
 
 const char* adrt_last_status_detail(void) { return g_detail.c_str(); }
@@ -727,6 +764,26 @@ int adrt_planck_band_deriv(double lo, double hi, double temp, double* out) {
   if (temp < 0.0 || hi < lo || lo < 0.0)
     return fail(ADRT_ERR_INVALID_ARGUMENT, "planckFunctionDeriv: invalid arguments");
   *out = planck_band_deriv(lo, hi, temp);
+  return ADRT_OK;
+}
+
+int adrt_band_integrate(adrt_engine* e, const double* spectrum, const double* weight,
+                        long long num_wavenumbers, const long long* offsets, int nchannels,
+                        double* out, void* stream_ptr) {
+  if (!e || !spectrum || !offsets || !out)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine, spectrum, offsets or output");
+  if (nchannels < 0 || num_wavenumbers < 0)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "negative channel or wavenumber count");
+  if (nchannels == 0) return ADRT_OK;
+  std::lock_guard<std::mutex> lk(e->mu);
+  int rc;
+  if ((rc = set_device(e))) return rc;
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  e->last_stream = s;
+  const int grid = std::min(nchannels, e->num_sms * 8);
+  band_integrate_kernel<<<grid, 256, 0, s>>>(spectrum, weight, num_wavenumbers, offsets, nchannels,
+                                             out, e->status);
+  CUDA_TRY(cudaGetLastError());
   return ADRT_OK;
 }
 

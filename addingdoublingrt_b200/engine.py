@@ -100,6 +100,24 @@ class Engine:
         _lib.check(self.lib.adrt_adjoint(self.handle, C.byref(desc), C.byref(ins), outp,
                                          C.byref(cot), C.byref(gr), s))
 
+    def band_integrate(self, spectrum, offsets, weight=None, out=None, stream=None):
+        """adrt_band_integrate on CUDA tensors: out[b] = sum of weight * spectrum over
+        wavenumbers offsets[b] .. offsets[b + 1] - 1 (float64 spectrum / weight, int64
+        offsets of nchannels + 1 entries); returns out (float64, nchannels)."""
+        import torch
+        if offsets.dtype != torch.int64 or not offsets.is_contiguous():
+            raise TypeError("offsets must be a contiguous int64 tensor")
+        nch = int(offsets.numel()) - 1
+        if out is None:
+            out = torch.empty(max(nch, 0), dtype=torch.float64, device=spectrum.device)
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        _lib.check(self.lib.adrt_band_integrate(self.handle, _ptr(spectrum), _ptr(weight),
+                                                int(spectrum.numel()), offsets.data_ptr(), nch,
+                                                _ptr(out), s))
+        return out
+
     def solve_uneven(self, columns: list, stream=None) -> None:
         """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
         arr = (_abi.ColumnDesc * len(columns))()

@@ -59,7 +59,8 @@ enum adrt_status {
 enum adrt_device_flag {
   ADRT_FLAG_SINGULAR_PIVOT = 1, /* an LU pivot was exactly zero (reference: silent inv=0) */
   ADRT_FLAG_NONFINITE = 2,      /* a non-finite flux was produced */
-  ADRT_FLAG_BAD_INPUT = 4       /* tau < 0, omega outside [0,1], T < 0 seen on the device */
+  ADRT_FLAG_BAD_INPUT = 4       /* tau < 0, omega outside [0,1], T < 0 seen on the device, or
+                                   a channel range outside the spectrum (band integration) */
 };
 
 /* ---------------------------------------------------------------- config */
@@ -346,6 +347,20 @@ int adrt_planck_band(double wavenumber_low, double wavenumber_high, double tempe
  * adrt::planckFunctionDeriv (src/planck.cpp:135-175, declared in
  * src/planck.hpp:27). */
 int adrt_planck_band_deriv(double wnumlo, double wnumhi, double temp, double* out);
+
+/* Band integration of a spectrum on the device, the reduction after a solve
+ * (e.g. TOA flux_up into instrument channels): for each channel b,
+ *   out[b] = sum over w in [offsets[b], offsets[b+1]) of weight[w] * spectrum[w]
+ * (weight null: 1).  offsets holds nchannels + 1 non-decreasing indices into
+ * [0, num_wavenumbers]; a channel whose range is not is written NaN and sets
+ * ADRT_FLAG_BAD_INPUT.  Device pointers, stream-ordered, no allocation; each
+ * channel is summed by one block in a fixed order, so the result does not
+ * depend on the launch.  The reference's batched path scales flux_up by
+ * spectrum_scaling (src_cuda/cuda_solver.cu:481, cuda_solver.cuh:39) and
+ * leaves this reduction to its caller. */
+int adrt_band_integrate(adrt_engine* engine, const double* spectrum, const double* weight,
+                        long long num_wavenumbers, const long long* offsets, int nchannels,
+                        double* out, void* stream);
 
 /* --------------------------------------------------------------- errors */
 const char* adrt_last_status_detail(void);
