@@ -260,32 +260,6 @@ __device__ __forceinline__ void op_gemm_x(const GemmX g, int t) {
   }
 }
 
-// N matrices from global memory into shared memory (row- and / or
-// column-major; kNoMat skips), every load issued before the first store so
-// that their latencies overlap.  Bit n of OWN: matrix n is in this group's
-// own tile order, else in GO's (a record of the taping forward).
-template <class Gm, class GO, int N, unsigned OWN>
-__device__ __forceinline__ void g2s_n(const double* const (&g)[N], const unsigned (&orm)[N],
-                                      const unsigned (&ocm)[N], int t) {
-  constexpr int TR = Gm::TR, TC = Gm::TC;
-  const Tile<Gm> tl(t);
-  if (!tl.valid()) return;
-  double X[N][TR][TC];
-#pragma unroll
-  for (int n = 0; n < N; ++n)
-#pragma unroll
-    for (int a = 0; a < TR; ++a)
-#pragma unroll
-      for (int b = 0; b < TC; ++b)
-        X[n][a][b] = ((OWN >> n) & 1u) ? g[n][t * Gm::TE + a * TC + b]
-                                       : g[n][tile_index<GO>(tl.row(a), tl.col(b))];
-#pragma unroll
-  for (int n = 0; n < N; ++n) {
-    if (orm[n] != kNoMat) tl.store_rm(X[n], sp<double>(orm[n]));
-    if (ocm[n] != kNoMat) tl.store_cm(X[n], sp<double>(ocm[n]));
-  }
-}
-
 // Copy a row-major matrix into row-major and/or column-major buffers, scaled.
 template <class Gm>
 __device__ __noinline__ void op_copy(unsigned in_rm, unsigned orm, unsigned ocm, double scale,

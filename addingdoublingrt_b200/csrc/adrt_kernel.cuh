@@ -1269,9 +1269,12 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
     const int scat = rl[3 * TILE + 2 * NP] != Real(0);
     const int cbase = rb[3 * TILE + 2 * NP + 1] != Real(0);
     X.sync();
-    op_g2s<Gm>(rl + TILE, kNoMat, X.mo(0), t);      // T (cm)
-    op_g2s<Gm>(rl, kNoMat, X.mo(1), t);             // R (cm)
-    op_g2s<Gm>(rb + 2 * TILE, X.mo(2), kNoMat, t);  // R_base (rm)
+    {  // T (cm), R (cm), R_base (rm), every load before the first store
+      const Real* g[3] = {rl + TILE, rl, rb + 2 * TILE};
+      const unsigned orm[3] = {kNoMat, kNoMat, X.mo(2)};
+      const unsigned ocm[3] = {X.mo(0), X.mo(1), kNoMat};
+      g2s_n<Gm, Gm, 3, 7u>(g, orm, ocm, t);
+    }
     if (X.warp == 0 && X.lane < NP) {
       X.V(V_UB)[X.lane] = rb[3 * TILE + NP + X.lane];
       X.V(V_SDN)[X.lane] = rl[3 * TILE + X.lane];

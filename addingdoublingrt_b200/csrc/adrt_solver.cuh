@@ -835,6 +835,33 @@ __device__ __noinline__ void op_g2s(const typename Gm::Real* g, unsigned orm_off
   if (out_cm) tl.store_cm(X, out_cm);
 }
 
+// N matrices from global memory into shared memory (row- and / or
+// column-major; kNoMat skips), every load issued before the first store so
+// that their latencies overlap.  Bit n of OWN: matrix n is in this group's
+// own tile order, else in GO's (a record of the taping forward).
+template <class Gm, class GO, int N, unsigned OWN>
+__device__ __forceinline__ void g2s_n(const typename Gm::Real* const (&g)[N],
+                                      const unsigned (&orm)[N], const unsigned (&ocm)[N], int t) {
+  using Real = typename Gm::Real;
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  Real X[N][TR][TC];
+#pragma unroll
+  for (int n = 0; n < N; ++n)
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b)
+        X[n][a][b] = ((OWN >> n) & 1u) ? g[n][t * Gm::TE + a * TC + b]
+                                       : g[n][tile_index<GO>(tl.row(a), tl.col(b))];
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+    if (orm[n] != kNoMat) tl.store_rm(X[n], sp<Real>(orm[n]));
+    if (ocm[n] != kNoMat) tl.store_cm(X[n], sp<Real>(ocm[n]));
+  }
+}
+
 template <class Gm, class GO = Gm>
 __device__ __noinline__ void op_s2g(unsigned in_off, typename Gm::Real* g, int t) {
   using Real = typename Gm::Real;
