@@ -327,3 +327,28 @@ def test_delta_m_truncated_temperature_gradient_matches_finite_differences(eng):
     ad = run_adjoint(eng, b, cot, which=("temperature",))
     e = rel_err(ad["temperature"], fd_temperature(b, cot))
     assert e < 1e-4, ("temperature", e)
+
+
+def test_shared_moments_without_block_sums_match_per_layer_sets(eng):
+    """Shared per-layer moments whose per-block cotangent sums would pass
+    1 GB (here 1800 layers at N = 16) take the per-layer moment adjoint beside
+    the phase-matrix table; the moment gradient equals that of the same
+    moments given per wavenumber and layer, summed over the wavenumbers, and
+    the other gradients are unchanged."""
+    N, L, W = 16, 1800, 3
+    b = small_batch(51, N, W=W, L=L)
+    M = b.desc.num_moments
+    rng = np.random.default_rng(51)
+    cot = {k: rng.normal(size=W * (L + 1)) for k in COT}
+    shared = run_adjoint(eng, b, cot)
+    d = _abi.BatchDesc.from_buffer_copy(b.desc)
+    d.moment_layout = _abi.MOMENTS_PER_LAYER
+    arrays = dict(b.arrays)
+    arrays["phase_moments"] = np.tile(b.arrays["phase_moments"].reshape(1, L, M),
+                                      (W, 1, 1)).reshape(-1).copy()
+    per = run_adjoint(eng, workloads.Batch(d, arrays), cot)
+    g_per = per["phase_moments"].reshape(W, L, M).sum(axis=0)
+    g_sh = shared["phase_moments"].reshape(L, M)
+    assert np.max(np.abs(g_sh - g_per)) <= 1e-9 * np.max(np.abs(g_per))
+    for k in ("delta_tau", "single_scat_albedo", "temperature"):
+        assert np.max(np.abs(shared[k] - per[k])) <= 1e-9 * np.max(np.abs(per[k])), k
