@@ -27,6 +27,9 @@ MOMENTS_SHARED = 0
 MOMENTS_PER_WAVENUMBER = 1
 MOMENTS_PER_LAYER = 2
 
+ADJOINT_RECORD = 0      # the forward pass records the doubling chains
+ADJOINT_RECOMPUTE = 1   # the backward pass recomputes them
+
 _dp = C.POINTER(C.c_double)
 
 

@@ -38,6 +38,7 @@ EXPORTS = (
     "adrt_adjoint_host",
     "adrt_planck_band_deriv",
     "adrt_band_integrate",
+    "adrt_engine_set_adjoint_mode",
 )
 
 
@@ -85,6 +86,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                           P(_abi.Cotangents), P(_abi.Gradients)]
         lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),
                                              P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
+        lib.adrt_engine_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
         lib.adrt_band_integrate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong,
                                             C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),

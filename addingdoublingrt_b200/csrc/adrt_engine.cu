@@ -183,6 +183,7 @@ struct adrt_engine {
   cudaEvent_t hev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::mutex hmu;  // one host-entry call at a time per engine
   std::mutex mu;
+  int adjoint_mode = ADRT_ADJOINT_RECORD;
 };
 
 namespace {
@@ -767,6 +768,15 @@ int adrt_planck_band_deriv(double lo, double hi, double temp, double* out) {
   return ADRT_OK;
 }
 
+int adrt_engine_set_adjoint_mode(adrt_engine* e, int mode) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  if (mode != ADRT_ADJOINT_RECORD && mode != ADRT_ADJOINT_RECOMPUTE)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "unknown adjoint mode %d", mode);
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->adjoint_mode = mode;
+  return ADRT_OK;
+}
+
 int adrt_band_integrate(adrt_engine* e, const double* spectrum, const double* weight,
                         long long num_wavenumbers, const long long* offsets, int nchannels,
                         double* out, void* stream_ptr) {
@@ -877,7 +887,9 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   // chunk: one wavenumber per resident forward group, within the memory budget
   const long long rgroups = (long long)bps * e->num_sms * k.groups;
   const size_t rev_bytes = (size_t)rgroups * k.scr;
-  const size_t per_w = k.state + (size_t)L * kTapeStepsPerLayer * k.step * sizeof(double);
+  const bool recompute = e->adjoint_mode == ADRT_ADJOINT_RECOMPUTE;
+  const size_t per_w =
+      k.state + (recompute ? 0 : (size_t)L * kTapeStepsPerLayer * k.step * sizeof(double));
   const size_t budget = e->max_ws ? e->max_ws : kAdjointMemory;
   // moment sets shared by every wavenumber (one per layer): their phase
   // matrices once per call, and per-block sums of the phase-matrix cotangents
@@ -896,7 +908,8 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
                 fixed + per_w);
   long long wc = std::min<long long>(W, (long long)fbps * e->num_sms * k.fgroups);
   wc = std::max<long long>(1, std::min<long long>(wc, (long long)((budget - fixed) / per_w)));
-  const long long pool_cap = wc * L * kTapeStepsPerLayer * k.step;
+  // ADRT_ADJOINT_RECOMPUTE: no record pool, every chain recomputed in the reverse
+  const long long pool_cap = recompute ? 0 : wc * L * kTapeStepsPerLayer * k.step;
   const size_t ext = align256(rev_bytes + (size_t)wc * k.state + (size_t)pool_cap * sizeof(double) +
                               sizeof(unsigned long long));
   const size_t need = ext + ptab_bytes + psum_bytes;

@@ -42,6 +42,11 @@ class Engine:
         _lib.check(self.lib.adrt_engine_workspace_bytes(self.handle, C.byref(v)))
         return int(v.value)
 
+    def set_adjoint_mode(self, mode: int) -> None:
+        """adrt_engine_set_adjoint_mode: _abi.ADJOINT_RECORD (default) or
+        _abi.ADJOINT_RECOMPUTE (every doubling chain recomputed in the backward pass)."""
+        _lib.check(self.lib.adrt_engine_set_adjoint_mode(self.handle, int(mode)))
+
     def read_status(self) -> int:
         v = C.c_int()
         _lib.check(self.lib.adrt_engine_read_status(self.handle, C.byref(v)))

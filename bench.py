@@ -177,13 +177,16 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- adjoint and uneven
-def time_adjoint(eng, W=10_000, reps=3):
+def time_adjoint(eng, W=10_000, reps=3, mode=_abi.ADJOINT_RECORD):
     """Forward and adjoint times of config 5 (10 000 x 60, N=16, thermal + solar,
     per-layer HG moments): gradients of TOA F_up and BOA F_down with respect to
     delta_tau, omega, the moments and the 61 level temperatures.  Returns
-    (forward ms, adjoint ms) on the device, median of `reps`."""
+    (forward ms, adjoint ms) on the device, median of `reps`; `mode` is the
+    engine's adjoint mode (doubling chains recorded, or recomputed in the
+    backward pass)."""
     import torch
     from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    eng.set_adjoint_mode(mode)
     b = workloads.config5(W=W)
     di = to_device(b)
     do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
@@ -208,6 +211,7 @@ def time_adjoint(eng, W=10_000, reps=3):
         torch.cuda.synchronize()
         fw.append(e0.elapsed_time(e1))
         ad.append(e1.elapsed_time(e2))
+    eng.set_adjoint_mode(_abi.ADJOINT_RECORD)
     return statistics.median(fw), statistics.median(ad)
 
 
@@ -300,10 +304,13 @@ def main():
     if args.workload == "adjoint":
         W = args.adjoint_wavenumbers
         fw, ad = time_adjoint(eng, W=W)
+        fw2, ad2 = time_adjoint(eng, W=W, mode=_abi.ADJOINT_RECOMPUTE)
         print(json.dumps({"metric": "adjoint time / forward time, config 5", "value": ad / fw,
                           "unit": "ratio", "higher_is_better": False, "forward_ms": fw,
-                          "adjoint_ms": ad, "config": {"workload": f"config5: W={W} x L=60, "
-                                                       "N=16, thermal + solar, FP64"}}))
+                          "adjoint_ms": ad, "adjoint_recompute_ms": ad2,
+                          "adjoint_recompute_over_forward": ad2 / fw2,
+                          "config": {"workload": f"config5: W={W} x L=60, "
+                                                 "N=16, thermal + solar, FP64"}}))
         return
     results = {}
     precisions = [args.only] if args.only else ["fp64", "mixed"]
@@ -378,7 +385,9 @@ def main():
     adj = {}
     if not args.no_adjoint:
         fw, ad = time_adjoint(eng)
-        adj = {"adjoint_over_forward": ad / fw, "adjoint_config5_ms": ad, "forward_config5_ms": fw}
+        fw2, ad2 = time_adjoint(eng, mode=_abi.ADJOINT_RECOMPUTE)
+        adj = {"adjoint_over_forward": ad / fw, "adjoint_config5_ms": ad, "forward_config5_ms": fw,
+               "adjoint_recompute_over_forward": ad2 / fw2, "adjoint_recompute_config5_ms": ad2}
     if rank == 0:
         from oracle import oracle
         fl = oracle.flops(b)  # algorithmic flops of the whole batch

@@ -285,6 +285,19 @@ typedef struct adrt_gradients {
                                surface_temperature >= 0 (times dB/dT gives d/dT_s) */
 } adrt_gradients;
 
+/* How adrt_adjoint's backward pass gets each layer's doubling chain. */
+enum adrt_adjoint_mode {
+  ADRT_ADJOINT_RECORD = 0,   /* default: the forward pass records the chains (up
+                                to a record pool; chains beyond it are recomputed) */
+  ADRT_ADJOINT_RECOMPUTE = 1 /* the forward pass keeps only the per-layer R, T and
+                                sources for the adding; every chain is recomputed in
+                                the backward pass */
+};
+
+/* Select the engine's adjoint mode (enum adrt_adjoint_mode); both give the
+ * same gradients to round-off. */
+int adrt_engine_set_adjoint_mode(adrt_engine* engine, int mode);
+
 /* Reverse-mode adjoint of the batched solve: given the loss cotangents,
  * the gradients with respect to delta_tau, single_scat_albedo, the phase
  * moments and the level temperatures (through dB/dT, the reference's
@@ -293,7 +306,8 @@ typedef struct adrt_gradients {
  * generalises the reference's analytic temperature Jacobian
  * (src/solver.cpp:117-341) to all inputs.  FP64; the forward pass records
  * every layer's doubling chain for the backward pass (in chunks of
- * wavenumbers; chains beyond the record pool are recomputed).  `out` may be
+ * wavenumbers; chains beyond the record pool are recomputed), or, in
+ * ADRT_ADJOINT_RECOMPUTE mode, the backward pass recomputes them all.  `out` may be
  * NULL or receive the forward outputs.  With delta-M truncation in effect
  * (use_delta_m with num_moments > 2N) only the temperature, planck_levels and
  * surface_emission gradients are formed. */

@@ -352,3 +352,20 @@ def test_shared_moments_without_block_sums_match_per_layer_sets(eng):
     assert np.max(np.abs(g_sh - g_per)) <= 1e-9 * np.max(np.abs(g_per))
     for k in ("delta_tau", "single_scat_albedo", "temperature"):
         assert np.max(np.abs(shared[k] - per[k])) <= 1e-9 * np.max(np.abs(per[k])), k
+
+
+def test_recompute_mode_matches_record_mode(eng):
+    """ADRT_ADJOINT_RECOMPUTE (every doubling chain recomputed in the backward
+    pass, only the per-layer R, T and sources kept from the forward) gives the
+    gradients of the default recording mode."""
+    b = small_batch(61, 16, W=40, L=12)
+    rng = np.random.default_rng(61)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    rec = run_adjoint(eng, b, cot)
+    eng.set_adjoint_mode(_abi.ADJOINT_RECOMPUTE)
+    try:
+        recomp = run_adjoint(eng, b, cot)
+    finally:
+        eng.set_adjoint_mode(_abi.ADJOINT_RECORD)
+    for k in rec:
+        assert np.max(np.abs(recomp[k] - rec[k])) <= 1e-9 * np.max(np.abs(rec[k])), k
