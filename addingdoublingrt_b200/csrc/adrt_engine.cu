@@ -1049,7 +1049,10 @@ int adrt_solve_batch_uneven(adrt_engine* e, const adrt_column_desc* cols, int nc
     }
   }
   CUDA_TRY(cudaMemcpyAsync(e->d_cols, e->h_cols, sizeof(ColumnDev) * ncols, cudaMemcpyHostToDevice, s));
-  if (e->cols_copied) CUDA_TRY(cudaEventRecord(e->cols_copied, s));
+  // (in a capture the copy runs at each replay, from the staging as it is
+  // then; recording the event there would leave it a captured event)
+  if (e->cols_copied && cap == cudaStreamCaptureStatusNone)
+    CUDA_TRY(cudaEventRecord(e->cols_copied, s));
   // columns of N <= 16: one launch of the multi-order kernel
   if (!small.empty()) {
     const size_t smem = 4 * kMultiGroupBytes;
