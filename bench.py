@@ -48,8 +48,10 @@ def parse():
                    help="time one precision form only (profiling runs)")
     p.add_argument("--adjoint-wavenumbers", type=int, default=10_000,
                    help="wavenumbers of the config-5 adjoint timing")
-    p.add_argument("--workload", default="config2", choices=["config2", "config4", "adjoint"],
-                   help="config2: the headline line; config4: uneven batch; adjoint: config 5")
+    p.add_argument("--workload", default="config2",
+                   choices=["config2", "config4", "adjoint", "band"],
+                   help="config2: the headline line; config4: uneven batch; adjoint: config 5; "
+                        "band: band integration of a spectrum (--wavenumbers x 1000)")
     p.add_argument("--no-adjoint", action="store_true",
                    help="skip the adjoint/forward timing of the headline line")
     return p.parse_args()
@@ -256,6 +258,49 @@ def run_config4(args, eng):
     print(json.dumps(line), flush=True)
 
 
+def run_band(args, eng):
+    """Band integration of a spectrum into channels (adrt_band_integrate):
+    --wavenumbers x 1000 wavenumbers of float64 spectrum and weights (inputs
+    resident in HBM, larger than L2) into channels of 1000 wavenumbers.  HBM-
+    bound: 16 bytes per wavenumber read."""
+    import torch
+    W = args.wavenumbers * 1000
+    per = 1000
+    g = torch.Generator(device="cuda").manual_seed(11)
+    spec = torch.rand(W, dtype=torch.float64, device="cuda", generator=g)
+    wgt = torch.rand(W, dtype=torch.float64, device="cuda", generator=g)
+    off = torch.arange(0, W + 1, per, dtype=torch.int64, device="cuda")
+    out = torch.empty(off.numel() - 1, dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        eng.band_integrate(spec, off, wgt, out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        eng.band_integrate(spec, off, wgt, out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    gbs = 16.0 * W / (ms * 1e-3) / 1e9
+    peak, src = None, "measured (MEASURED_PEAKS.json)"
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+    except (OSError, ValueError):
+        pass
+    if not peak:  # the pool's earlier copy-bandwidth measurement
+        peak, src = 6650.0, "fallback 6.65 TB/s copy bandwidth"
+    ref = float((spec * wgt).sum())
+    line = {"metric": "band integration GB/s", "value": gbs, "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"band integration: {W} wavenumbers into {out.numel()} "
+                                   f"channels of {per}, spectrum and weights in HBM"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "frac": gbs / peak,
+                         "unit": "GB/s", "peak_source": src},
+            "sum_check": abs(float(out.sum()) - ref) / ref}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- ranks
 def max_over_ranks(x: float, dist, device) -> float:
     """The slowest rank's value (every rank calls this in the same order)."""
@@ -301,6 +346,8 @@ def main():
     eng = Engine(device=local)
     if args.workload == "config4":
         return run_config4(args, eng)
+    if args.workload == "band":
+        return run_band(args, eng)
     if args.workload == "adjoint":
         W = args.adjoint_wavenumbers
         fw, ad = time_adjoint(eng, W=W)
