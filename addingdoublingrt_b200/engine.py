@@ -110,8 +110,8 @@ class Engine:
         wavenumbers offsets[b] .. offsets[b + 1] - 1 (float64 spectrum / weight, int64
         offsets of nchannels + 1 entries); returns out (float64, nchannels)."""
         import torch
-        if offsets.dtype != torch.int64 or not offsets.is_contiguous():
-            raise TypeError("offsets must be a contiguous int64 tensor")
+        if offsets.dtype != torch.int64 or not offsets.is_contiguous() or not offsets.is_cuda:
+            raise TypeError("offsets must be a contiguous int64 CUDA tensor")
         nch = int(offsets.numel()) - 1
         if out is None:
             out = torch.empty(max(nch, 0), dtype=torch.float64, device=spectrum.device)
@@ -139,10 +139,13 @@ class Engine:
 
 
 def _ptr(t):
+    """Device address of a float64 CUDA tensor for the device entry points (a
+    host array here would hand the kernels a host address)."""
     if t is None:
         return None
-    if isinstance(t, np.ndarray):
-        return t.ctypes.data
+    if isinstance(t, np.ndarray) or not getattr(t, "is_cuda", False):
+        raise TypeError("device entry points take CUDA tensors; host arrays go through "
+                        "the host entry (solve_host)")
     if not t.is_contiguous():
         raise ValueError("device arrays must be contiguous")
     import torch

@@ -99,3 +99,16 @@ def test_validate_diffusion_needs_sources():
 
 def test_version_string():
     assert b"sm_100a" in _lib.load().adrt_version()
+
+
+def test_device_entry_points_refuse_host_arrays():
+    """The device entry points' pointer helper refuses numpy arrays and CPU
+    tensors (their addresses are host memory) before anything reaches a kernel."""
+    import numpy as np
+    import pytest
+    import torch
+    from addingdoublingrt_b200.engine import _ptr
+    assert _ptr(None) is None
+    for host in (np.zeros(4), torch.zeros(4, dtype=torch.float64)):
+        with pytest.raises(TypeError):
+            _ptr(host)
