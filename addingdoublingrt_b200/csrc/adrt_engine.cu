@@ -552,6 +552,12 @@ int adrt_engine_workspace_bytes(const adrt_engine* e, size_t* bytes) {
   return ADRT_OK;
 }
 
+int adrt_engine_device(const adrt_engine* e, int* device) {
+  if (!e || !device) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
+  *device = e->device;
+  return ADRT_OK;
+}
+
 int adrt_engine_read_status(adrt_engine* e, int* flags) {
   if (!e || !flags) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
   std::lock_guard<std::mutex> lk(e->mu);

@@ -22,6 +22,16 @@ class Engine:
         h = C.c_void_p()
         _lib.check(self.lib.adrt_engine_create(C.byref(opts), C.byref(h)))
         self.handle = h
+        d = C.c_int()
+        _lib.check(self.lib.adrt_engine_device(h, C.byref(d)))
+        self.device = int(d.value)  # the CUDA ordinal the engine's kernels run on
+
+    def _dev(self, t):
+        """_ptr of a tensor that must live on the engine's device (another
+        GPU's address would be dereferenced as a peer address)."""
+        if t is not None and getattr(t, "is_cuda", False) and t.device.index != self.device:
+            raise ValueError(f"tensor on cuda:{t.device.index}, engine on cuda:{self.device}")
+        return _ptr(t)
 
     def close(self) -> None:
         if self.handle:
@@ -69,10 +79,10 @@ class Engine:
         ins = _abi.Inputs()
         for f in _abi.INPUT_FIELDS:
             t = dev_inputs.get(f)
-            setattr(ins, f, _ptr(t))
+            setattr(ins, f, self._dev(t))
         outs = _abi.Outputs()
         for f in _abi.OUTPUT_FIELDS:
-            setattr(outs, f, _ptr(dev_outputs.get(f)))
+            setattr(outs, f, self._dev(dev_outputs.get(f)))
         s = None
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
@@ -86,18 +96,18 @@ class Engine:
         phase_moments / temperature / planck_levels are added to)."""
         ins = _abi.Inputs()
         for f in _abi.INPUT_FIELDS:
-            setattr(ins, f, _ptr(dev_inputs.get(f)))
+            setattr(ins, f, self._dev(dev_inputs.get(f)))
         cot = _abi.Cotangents()
         for f in _abi.COTANGENT_FIELDS:
-            setattr(cot, f, _ptr(cotangents.get(f)))
+            setattr(cot, f, self._dev(cotangents.get(f)))
         gr = _abi.Gradients()
         for f in _abi.GRADIENT_FIELDS:
-            setattr(gr, f, _ptr(gradients.get(f)))
+            setattr(gr, f, self._dev(gradients.get(f)))
         outp = None
         if dev_outputs is not None:
             outs = _abi.Outputs()
             for f in _abi.OUTPUT_FIELDS:
-                setattr(outs, f, _ptr(dev_outputs.get(f)))
+                setattr(outs, f, self._dev(dev_outputs.get(f)))
             outp = C.byref(outs)
         s = None
         if stream is not None:
@@ -112,15 +122,17 @@ class Engine:
         import torch
         if offsets.dtype != torch.int64 or not offsets.is_contiguous() or not offsets.is_cuda:
             raise TypeError("offsets must be a contiguous int64 CUDA tensor")
+        if offsets.device.index != self.device:
+            raise ValueError(f"offsets on cuda:{offsets.device.index}, engine on cuda:{self.device}")
         nch = int(offsets.numel()) - 1
         if out is None:
             out = torch.empty(max(nch, 0), dtype=torch.float64, device=spectrum.device)
         s = None
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
-        _lib.check(self.lib.adrt_band_integrate(self.handle, _ptr(spectrum), _ptr(weight),
+        _lib.check(self.lib.adrt_band_integrate(self.handle, self._dev(spectrum), self._dev(weight),
                                                 int(spectrum.numel()), offsets.data_ptr(), nch,
-                                                _ptr(out), s))
+                                                self._dev(out), s))
         return out
 
     def solve_uneven(self, columns: list, stream=None) -> None:
@@ -129,9 +141,9 @@ class Engine:
         for i, (desc, di, do) in enumerate(columns):
             arr[i].desc = desc
             for f in _abi.INPUT_FIELDS:
-                setattr(arr[i].inp, f, _ptr(di.get(f)))
+                setattr(arr[i].inp, f, self._dev(di.get(f)))
             for f in _abi.OUTPUT_FIELDS:
-                setattr(arr[i].out, f, _ptr(do.get(f)))
+                setattr(arr[i].out, f, self._dev(do.get(f)))
         s = None
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))

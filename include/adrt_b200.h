@@ -153,6 +153,10 @@ int adrt_engine_reserve(adrt_engine* engine, const adrt_batch_desc* desc);
 /* Bytes of device work buffer the engine currently holds. */
 int adrt_engine_workspace_bytes(const adrt_engine* engine, size_t* bytes);
 
+/* The CUDA device ordinal the engine runs on; device pointers given to it
+ * must be memory of that device. */
+int adrt_engine_device(const adrt_engine* engine, int* device);
+
 /* Synchronise the engine's last stream and read (and clear) the device status
  * word (enum adrt_device_flag bits). */
 int adrt_engine_read_status(adrt_engine* engine, int* flags);

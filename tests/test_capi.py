@@ -112,3 +112,30 @@ def test_device_entry_points_refuse_host_arrays():
     for host in (np.zeros(4), torch.zeros(4, dtype=torch.float64)):
         with pytest.raises(TypeError):
             _ptr(host)
+
+
+@pytest.mark.gpu
+def test_device_methods_check_the_engine_device():
+    """The engine reports its device (adrt_engine_device), and the Python device
+    methods refuse tensors of another device before launching anything."""
+    import torch
+    from conftest import cuda_available
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    from addingdoublingrt_b200.engine import Engine, alloc_device_outputs, to_device
+    eng = Engine()
+    try:
+        assert eng.device == torch.cuda.current_device()
+        b = workloads.config5(W=8, L=4)
+        di = to_device(b)
+        do = alloc_device_outputs(b, ("toa_flux_up",))
+        eng.solve_device(b.desc, di, do)
+        torch.cuda.synchronize()
+        real = eng.device
+        eng.device = real + 1  # as if the tensors belonged to another GPU
+        with pytest.raises(ValueError):
+            eng.solve_device(b.desc, di, do)
+        eng.device = real
+        assert eng.read_status() == 0
+    finally:
+        eng.close()
