@@ -125,8 +125,12 @@ class Engine:
         if offsets.device.index != self.device:
             raise ValueError(f"offsets on cuda:{offsets.device.index}, engine on cuda:{self.device}")
         nch = int(offsets.numel()) - 1
+        if weight is not None and weight.numel() != spectrum.numel():
+            raise ValueError("weight must have one entry per wavenumber of the spectrum")
         if out is None:
             out = torch.empty(max(nch, 0), dtype=torch.float64, device=spectrum.device)
+        elif out.numel() < nch:
+            raise ValueError(f"out holds {out.numel()} values for {nch} channels")
         s = None
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))

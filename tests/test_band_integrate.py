@@ -73,3 +73,19 @@ def test_bad_offsets_flag_the_channel(eng):
     g = got.cpu().numpy()
     assert g[0] == spec[:4].sum() and np.isnan(g[1]) and g[2] == spec[3:].sum() and np.isnan(g[3])
     assert eng.read_status() & 4
+
+
+@pytest.mark.gpu
+def test_short_buffers_are_refused_before_the_launch(eng):
+    """An output buffer with fewer entries than channels, or weights of another
+    length than the spectrum, raise before anything is written."""
+    import torch
+    spec = torch.ones(100, dtype=torch.float64, device="cuda")
+    off = torch.tensor([0, 50, 100], dtype=torch.int64, device="cuda")
+    with pytest.raises(ValueError):
+        eng.band_integrate(spec, off, out=torch.zeros(1, dtype=torch.float64, device="cuda"))
+    with pytest.raises(ValueError):
+        eng.band_integrate(spec, off, torch.ones(99, dtype=torch.float64, device="cuda"))
+    got = eng.band_integrate(spec, off)
+    torch.cuda.synchronize()
+    assert got.cpu().tolist() == [50.0, 50.0]
