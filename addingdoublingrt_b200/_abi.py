@@ -128,6 +128,22 @@ class ColumnDesc(C.Structure):
     _fields_ = [("desc", BatchDesc), ("inp", Inputs), ("out", Outputs)]
 
 
+def array_counts(d: BatchDesc) -> dict:
+    """Elements of every input, output, cotangent and gradient array of a batch
+    (the sizes adrt_solve_batch and adrt_adjoint read and write)."""
+    W, L, M = d.num_wavenumbers, d.num_layers, d.num_moments
+    mom = {MOMENTS_SHARED: L * M, MOMENTS_PER_WAVENUMBER: W * M}.get(d.moment_layout, W * L * M)
+    temp = (W if d.temperature_per_wavenumber else 1) * (L + 1)
+    n = {"delta_tau": W * L, "single_scat_albedo": W * L, "phase_moments": mom,
+         "temperature": temp, "planck_levels": W * (L + 1)}
+    for f in INPUT_FIELDS[5:]:
+        n[f] = W
+    out = {f: W * (L + 1) for f in INTERFACE_OUTPUTS}
+    out.update({f: W for f in OUTPUT_FIELDS[5:]})
+    return {"in": n, "out": out, "cot": {f: W * (L + 1) for f in COTANGENT_FIELDS},
+            "grad": {f: (n[f] if f != "surface_emission" else W) for f in GRADIENT_FIELDS}}
+
+
 class EngineOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("max_workspace_bytes", C.c_size_t)]
 

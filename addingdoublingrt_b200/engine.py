@@ -26,6 +26,17 @@ class Engine:
         _lib.check(self.lib.adrt_engine_device(h, C.byref(d)))
         self.device = int(d.value)  # the CUDA ordinal the engine's kernels run on
 
+    @staticmethod
+    def _sizes(desc, groups):
+        """Refuse arrays shorter than the batch needs (the kernels would read or
+        write past their ends): groups = [(kind, {name: tensor}), ...]."""
+        n = _abi.array_counts(desc)
+        for kind, arrays in groups:
+            for name, t in (arrays or {}).items():
+                if t is not None and name in n[kind] and t.numel() < n[kind][name]:
+                    raise ValueError(f"{name}: {t.numel()} elements, the batch needs "
+                                     f"{n[kind][name]}")
+
     def _dev(self, t):
         """_ptr of a tensor that must live on the engine's device (another
         GPU's address would be dereferenced as a peer address)."""
@@ -76,6 +87,7 @@ class Engine:
     def solve_device(self, desc: _abi.BatchDesc, dev_inputs: dict, dev_outputs: dict,
                      stream=None) -> None:
         """adrt_solve_batch on CUDA tensors (float64, contiguous); stream ordered."""
+        self._sizes(desc, [("in", dev_inputs), ("out", dev_outputs)])
         ins = _abi.Inputs()
         for f in _abi.INPUT_FIELDS:
             t = dev_inputs.get(f)
@@ -94,6 +106,8 @@ class Engine:
         """adrt_adjoint on CUDA tensors: gradients of sum(cotangent * output) with respect to
         the inputs named in `gradients` (delta_tau and single_scat_albedo are overwritten,
         phase_moments / temperature / planck_levels are added to)."""
+        self._sizes(desc, [("in", dev_inputs), ("cot", cotangents), ("grad", gradients),
+                           ("out", dev_outputs)])
         ins = _abi.Inputs()
         for f in _abi.INPUT_FIELDS:
             setattr(ins, f, self._dev(dev_inputs.get(f)))
@@ -143,6 +157,7 @@ class Engine:
         """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
         arr = (_abi.ColumnDesc * len(columns))()
         for i, (desc, di, do) in enumerate(columns):
+            self._sizes(desc, [("in", di), ("out", do)])
             arr[i].desc = desc
             for f in _abi.INPUT_FIELDS:
                 setattr(arr[i].inp, f, self._dev(di.get(f)))

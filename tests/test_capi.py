@@ -139,3 +139,42 @@ def test_device_methods_check_the_engine_device():
         assert eng.read_status() == 0
     finally:
         eng.close()
+
+
+@pytest.mark.parametrize("make", [workloads.config1, workloads.config2, workloads.config5])
+def test_array_counts_match_the_batch_arrays(make):
+    """The element counts the Python engine checks device arrays against are
+    those of every input and output array of a batch."""
+    b = make(W=40)
+    n = _abi.array_counts(b.desc)
+    for k, v in b.arrays.items():
+        assert v.size == n["in"][k], k
+    for k, v in b.alloc_outputs().items():
+        assert v.size == n["out"][k], k
+
+
+@pytest.mark.gpu
+def test_short_device_arrays_are_refused_before_the_launch():
+    import torch
+    from conftest import cuda_available
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    from addingdoublingrt_b200.engine import Engine, alloc_device_outputs, to_device
+    eng = Engine()
+    try:
+        b = workloads.config5(W=16, L=6)
+        di = to_device(b)
+        do = alloc_device_outputs(b, ("flux_up", "toa_flux_up"))
+        short = dict(do)
+        short["flux_up"] = do["flux_up"][:-1].contiguous()
+        with pytest.raises(ValueError):
+            eng.solve_device(b.desc, di, short)
+        bad = dict(di)
+        bad["delta_tau"] = di["delta_tau"].reshape(-1)[:-3].contiguous()
+        with pytest.raises(ValueError):
+            eng.solve_device(b.desc, bad, do)
+        eng.solve_device(b.desc, di, do)
+        torch.cuda.synchronize()
+        assert eng.read_status() == 0
+    finally:
+        eng.close()
