@@ -46,6 +46,9 @@ constexpr double kFp64NearConservative = 1e-2;  // 1 - omega below this ...
 constexpr double kFp64ThickTau = 1.0;           // ... with tau above this -> FP64 layer
 
 enum SolveMode { MODE_FP64 = 0, MODE_MIX_S = 1, MODE_MIX_D = 2 };
+#ifndef ADRT_MIX_FORCE_D
+#define ADRT_MIX_FORCE_D 0  // tuning: every mixed wavenumber takes class D
+#endif
 enum KernelKind { KIND_FP64 = 0, KIND_MIXED = 1 };
 constexpr int kLevelArrays = 6;  // B, tau_cum, tau', omega', omega, FP64-layer flag
 
@@ -1380,7 +1383,7 @@ __global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev 
       wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else if (colp->precision == 0) {  // an FP64 column of an uneven batch
       wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
-    } else if (!any) {
+    } else if (!any && !ADRT_MIX_FORCE_D) {
       wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else {
       wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,

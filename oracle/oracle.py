@@ -25,9 +25,27 @@ _lock = threading.Lock()
 _libs = {}
 
 
+def reference_dir() -> str:
+    """The reference checkout the recipe builds from: $ADRT_REFERENCE, else the
+    conventional read-only checkout location.  May not exist (the GPU machine
+    has only the prebuilt _ref/ files)."""
+    return os.environ.get("ADRT_REFERENCE", "/root/reference")
+
+
+def reference_present() -> bool:
+    return os.path.isdir(os.path.join(reference_dir(), "src"))
+
+
+def make(target: str, quiet: bool = True, **kw) -> subprocess.CompletedProcess:
+    """`make -C oracle <target> REF=<reference_dir()>`."""
+    cmd = ["make", "-s", "-C", HERE, target, f"REF={reference_dir()}"]
+    if quiet:
+        kw.setdefault("stdout", subprocess.DEVNULL)
+    return subprocess.run(cmd, **kw)
+
+
 def _make(target: str) -> None:
-    subprocess.run(["make", "-s", "-C", HERE, target], check=True,
-                   stdout=subprocess.DEVNULL)
+    make(target, check=True)
 
 
 def oracle_lib(fma: bool = False) -> C.CDLL:
@@ -74,7 +92,7 @@ def ref_lib(strict: bool = False) -> C.CDLL:
             path = os.path.join(HERE, "_ref", name)
             if not os.path.exists(path):
                 raise FileNotFoundError(
-                    f"{path} missing: build it with `make -C oracle ref` where the "
+                    f"{path} missing: build it with `make -C oracle ref REF=<checkout>` where the "
                     "reference sources are present")
             lib = C.CDLL(path)
             sig = [C.POINTER(_abi.BatchDesc), C.POINTER(_abi.Inputs), C.POINTER(_abi.Outputs)]

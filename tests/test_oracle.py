@@ -11,7 +11,6 @@
 import ctypes as C
 import math
 import os
-import subprocess
 
 import numpy as np
 import pytest
@@ -118,18 +117,10 @@ def test_validation_mirrors_reference():
         oracle.solve_oracle(b, 1)
 
 
-def _reference_dir():
-    """The reference checkout the oracle recipe builds from (its REF variable)."""
-    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
-                       capture_output=True, text=True)
-    return r.stdout.strip()
-
-
-@pytest.mark.skipif(not os.path.isdir(os.path.join(_reference_dir(), "tests")),
+@pytest.mark.skipif(not os.path.isdir(os.path.join(oracle.reference_dir(), "tests")),
                     reason="reference checkout absent")
 def test_reference_own_suites_pass_against_reference_build():
-    r = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "check-ref"],
-                       capture_output=True, text=True, timeout=900)
+    r = oracle.make("check-ref", quiet=False, capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "tests passed" in r.stdout
 
