@@ -33,6 +33,7 @@ EXPORTS = (
     "adrt_gauss_legendre",
     "adrt_planck_band",
     "adrt_solve_batch_noalloc",
+    "adrt_noalloc_read_status",
     "adrt_adjoint",
     "adrt_solve_batch_raw",
     "adrt_adjoint_host",
@@ -83,6 +84,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                              C.c_void_p, C.c_void_p]
         lib.adrt_solve_batch_noalloc.argtypes = [P(_abi.BatchDesc), P(_abi.Inputs),
                                                  P(_abi.Outputs), C.c_void_p]
+        lib.adrt_noalloc_read_status.argtypes = [C.c_void_p, P(C.c_int)]
         lib.adrt_adjoint_host.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),
                                           P(_abi.Cotangents), P(_abi.Gradients)]
         lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),

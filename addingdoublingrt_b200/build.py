@@ -19,6 +19,11 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libadrt_b200.so")
 HOST_LIB = os.path.join(PKG, "libadrt_host.so")
 HOST_SOURCES = ["adrt_host.cpp"]
+# The plain FP64 GPU form: the same engine with every product, right-solve and
+# phase build on the CUDA cores (DFMA, the pivoted scalar Gauss-Jordan) and no
+# tensor-core instruction -- the denominator of the mixed form's speed-up.
+CUDA_CORE_LIB = os.path.join(PKG, "libadrt_b200_cudacore.so")
+CUDA_CORE_FLAGS = ["-DADRT_GEMM_MMA=0", "-DADRT_GJ_MMA=0", "-DADRT_PHASE_MMA=0"]
 
 SOURCES = ["adrt_engine.cu", "adrt_probe.cu", "adrt_noalloc.cu"]
 HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh"]
@@ -70,8 +75,10 @@ def build(verbose: bool = False, force: bool = False, extra=(), out: str | None 
         return LIB
     objs = []
     tag = "" if out is None else "_" + os.path.basename(out).replace(".so", "")
+    objdir = os.path.join(PKG, "_build")
+    os.makedirs(objdir, exist_ok=True)
     for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", tag + ".o"))
+        obj = os.path.join(objdir, src.replace(".cu", tag + ".o"))
         cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
@@ -87,6 +94,18 @@ def build(verbose: bool = False, force: bool = False, extra=(), out: str | None 
     return target
 
 
+def build_all(verbose: bool = False) -> None:
+    """The engine (and its C++ drop-in library) and the CUDA-core FP64 form,
+    compiled in parallel."""
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(2) as ex:
+        jobs = [ex.submit(build, verbose, True),
+                ex.submit(build, verbose, True, CUDA_CORE_FLAGS, CUDA_CORE_LIB)]
+        for j in jobs:
+            j.result()
+
+
 if __name__ == "__main__":
-    build(verbose="--verbose" in sys.argv, force=True)
+    build_all(verbose="--verbose" in sys.argv)
     print(LIB)
+    print(CUDA_CORE_LIB)

@@ -193,14 +193,17 @@ int set_device(adrt_engine* e) {
   return ADRT_OK;
 }
 
-// Quadrature table for order n with Legendre rows up to mmax.
-int ensure_quad(adrt_engine* e, int n, int mmax) {
-  auto& q = e->quad[n];
-  if (q.buf && q.mmax >= mmax) return ADRT_OK;
-  mmax = std::max(mmax, 2 * n);
+}  // namespace
+
+// Host copy of the quadrature table of order n: nodes [n], weights [n], then
+// P_l(mu_i) for l < mmax ([mmax][n]); *xfac = 0.5 / sum(mu w).  Shared with
+// the allocation-free entry point (not exported), so both upload the same bits.
+__attribute__((visibility("hidden"))) void adrt_internal_quad_table(int n, int mmax,
+                                                                    std::vector<double>& host,
+                                                                    double* xfac) {
   std::vector<double> x, w;
   gauss_legendre01(n, x, w);
-  std::vector<double> host((size_t)2 * n + (size_t)mmax * n);
+  host.assign((size_t)2 * n + (size_t)mmax * n, 0.0);
   for (int i = 0; i < n; ++i) {
     host[i] = x[i];
     host[n + i] = w[i];
@@ -214,6 +217,19 @@ int ensure_quad(adrt_engine* e, int n, int mmax) {
       pl[l * n + i] = ((2 * l - 1) * x[i] * pl[(l - 1) * n + i] - (l - 1) * pl[(l - 2) * n + i]) / l;
   double s = 0.0;
   for (int i = 0; i < n; ++i) s += x[i] * w[i];
+  *xfac = 0.5 / s;
+}
+
+namespace {
+
+// Quadrature table for order n with Legendre rows up to mmax.
+int ensure_quad(adrt_engine* e, int n, int mmax) {
+  auto& q = e->quad[n];
+  if (q.buf && q.mmax >= mmax) return ADRT_OK;
+  mmax = std::max(mmax, 2 * n);
+  std::vector<double> host;
+  double xfac = 0.0;
+  adrt_internal_quad_table(n, mmax, host, &xfac);
   if (q.buf) {
     CUDA_TRY(cudaDeviceSynchronize());
     cudaFree(q.buf);
@@ -227,7 +243,7 @@ int ensure_quad(adrt_engine* e, int n, int mmax) {
   q.dev.wt = q.buf + n;
   q.dev.pl = q.buf + 2 * n;
   q.dev.mmax = mmax;
-  q.dev.xfac = 0.5 / s;
+  q.dev.xfac = xfac;
   return ADRT_OK;
 }
 
@@ -277,6 +293,19 @@ int check_inputs(const adrt_batch_desc* d, const adrt_inputs* in) {
                 "ADConfig: use_diffusion_lower_bc requires use_thermal_emission or planck_levels");
   return ADRT_OK;
 }
+
+}  // namespace
+
+// The argument checks of adrt_solve_batch (description, then inputs), for the
+// library's other entry points (not exported).
+__attribute__((visibility("hidden"))) int adrt_internal_check_batch(const adrt_batch_desc* d,
+                                                                    const adrt_inputs* in) {
+  int rc = check_desc(d);
+  if (rc) return rc;
+  return check_inputs(d, in);
+}
+
+namespace {
 
 ColumnDev make_column(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
                       const adrt_outputs* out) {

@@ -47,7 +47,16 @@ constexpr double kFp64ThickTau = 1.0;           // ... with tau above this -> FP
 
 enum SolveMode { MODE_FP64 = 0, MODE_MIX_S = 1, MODE_MIX_D = 2 };
 #ifndef ADRT_MIX_FORCE_D
-#define ADRT_MIX_FORCE_D 0  // tuning: every mixed wavenumber takes class D
+#define ADRT_MIX_FORCE_D 1  // every mixed wavenumber takes class D (FP64 adding)
+#endif
+// Scattering depth tau omega above which a layer doubles in FP64 in the mixed
+// form.  An FP32 doubling carries about 3e-7 of the largest entry of R and T
+// as round-off whatever the precision of its products (the rounding of R, T'
+// and the sources at each of the nn steps), so a layer's FP32 error in the
+// fluxes scales with its reflection and diffuse transmission, which grow with
+// tau omega: only weakly scattering layers double in FP32.
+#ifndef ADRT_MIX_SCAT_DEPTH
+#define ADRT_MIX_SCAT_DEPTH 0.003
 #endif
 enum KernelKind { KIND_FP64 = 0, KIND_MIXED = 1 };
 constexpr int kLevelArrays = 6;  // B, tau_cum, tau', omega', omega, FP64-layer flag
@@ -181,10 +190,14 @@ struct Levels {
 // even and the odd moments, E = A_e B_e and O = A_o B_o with
 // A[r][k] = d_l P_l(mu_r), B[k][c] = P_l(mu_c), d_l = (2l+1) chi_l, so that
 // P++ = (E + O) / 2pi and P+- = (E - O) / 2pi; rows and columns >= N are zero.
+#ifndef ADRT_PHASE_MMA
+#define ADRT_PHASE_MMA 1
+#endif
+
 template <class Gm>
 struct UsePhaseMMA {
   static constexpr int NT = Gm::NP / 8, NW = Gm::G / 32;
-  static constexpr bool value = Gm::NP >= 8 && (NT * NT) % NW == 0;
+  static constexpr bool value = ADRT_PHASE_MMA && Gm::NP >= 8 && (NT * NT) % NW == 0;
 };
 
 // Q+- (as above) into qpp / qpm with row stride ldq; with NORM, already
@@ -754,6 +767,235 @@ __device__ __noinline__ int doubling_lam(unsigned goff, unsigned tb, int t_, int
   return 2 + cur;
 }
 
+// ------------------------------------------------------------- doubling (Lambda-split, FP32 tensor cores)
+// doubling_lam with its four products on the tensor cores (tc32_tile: three
+// TF32 products each, FP32 accumulation) and the right-solve as the row-
+// parallel Gauss-Jordan without pivoting (op_gj_rows), for NP = 16 (one warp)
+// and NP = 32 (four warps, a 16 x 16 output tile each).  Each product reads
+// its left operand row-major and its right operand column-major.  Buffers:
+// m0 / m1 R (row- / column-major), m2 / m3 T (column-major, ping-pong), m4
+// I - R^2 then TGR (row-major), m5 G' (row-major), m6 / m7 T' (row-major,
+// ping-pong), m8 the right-hand side Lambda R^2 + T' and at the end T
+// row-major.  Returns 8 (the buffer of the row-major T); the layer sources
+// are left as by doubling_lam.
+template <class Gm>
+__device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int bar, double tau,
+                                        double om, double Bt, double Bb, double tcum, int N,
+                                        bool solar, double F0, double mu0, const double* Ppp,
+                                        const double* Ppm, int* singular, double* src64) {
+  static_assert(UseTC32<Gm>::value && UseGjRows<Gm>::value, "tensor-core FP32 geometry");
+  using Real = float;
+  const Ctx<Gm> X(goff, tb, t_, bar);
+  constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD;
+  const int t = X.t;
+  const double* mu = X.DV(D_MU);
+  const double* wt = X.DV(D_WT);
+  om = om > 1.0 ? 1.0 : om;
+  const double con = 2.0 * om * kPi;
+  const int nn = num_doublings(tau, om);
+  const double tau0 = ldexp(tau, -nn);
+  const double Ftop = solar ? F0 * exp(-tcum / mu0) : 0.0;
+  float* Rr = X.m(0);
+  float* Rc = X.m(1);
+  float* Tc[2] = {X.m(2), X.m(3)};
+  float* Am = X.m(4);
+  float* Gp = X.m(5);
+  float* Tp[2] = {X.m(6), X.m(7)};
+  float* RHS = X.m(8);
+  // first-order start: R = tau0 Gpm, T' = tau0 con Ppp w / mu, Lambda = 1 - tau0/mu
+  {
+    const Tile<Gm> tl(t);
+    if (tl.valid()) {
+      Real Rt[TR][TC], Tpt[TR][TC], Tt[TR][TC];
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) {
+          const int r = tl.row(a), c = tl.col(b);
+          double rv = 0.0, tp = 0.0, tv = (r == c) ? 1.0 : 0.0;
+          if (r < N && c < N) {
+            rv = tau0 * (con * (Ppm[r * NP + c] * wt[c]) / mu[r]);
+            tp = tau0 * (con * (Ppp[r * NP + c] * wt[c]) / mu[r]);
+            tv = tp + ((r == c) ? 1.0 - tau0 / mu[r] : 0.0);
+          }
+          Rt[a][b] = static_cast<Real>(rv);
+          Tpt[a][b] = static_cast<Real>(tp);
+          Tt[a][b] = static_cast<Real>(tv);
+        }
+      tl.store_rm(Rt, Rr);
+      tl.store_cm(Rt, Rc);
+      tl.store_rm(Tpt, Tp[0]);
+      tl.store_cm(Tt, Tc[0]);
+    }
+  }
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane;
+    double a = 0.0, su = 0.0, sd = 0.0, lam = 1.0;
+    if (i < N) {
+      lam = 1.0 - tau0 / mu[i];
+      a = 0.5 * tau0 * ((1.0 - om) * tau0 / mu[i]);  // g y at the start
+      if (solar) {
+        const double base = om * tau0 / mu[i] * Ftop;
+        su = base * X.DV(D_PM)[i];
+        sd = base * X.DV(D_PP)[i];
+      }
+    }
+    X.DV(D_LAM0)[i] = lam;
+    X.V(V_Y0)[i] = static_cast<Real>(a);
+    X.V(V_Z0)[i] = static_cast<Real>(-a);
+    X.V(V_SU0)[i] = static_cast<Real>(su);
+    X.V(V_SD0)[i] = static_cast<Real>(sd);
+  }
+  int r0, c0;
+  tc32_origin<Gm>(t, r0, c0);
+  const int g = X.lane >> 2, q = X.lane & 3;
+  double gam = solar ? exp(-tau0 / mu0) : 0.0;
+  int cur = 0;
+  for (int k = 0; k < nn; ++k) {
+    const int par = k & 1;
+    Real* av = X.V(V_Y0 + par);
+    Real* bv = X.V(V_Z0 + par);
+    Real* su = X.V(V_SU0 + par);
+    Real* sd = X.V(V_SD0 + par);
+    const double* lam = X.DV(D_LAM0 + par);
+    const Real gmv = static_cast<Real>(gam);
+    X.sync();  // R, T, T', Lambda and the vectors of the previous step are complete
+    if (solar && X.warp == 0) {  // ru = R sd + gam su, rd = gam R su + sd (old R)
+      const Real* vv[2] = {sd, su};
+      Real yv[2];
+      matvec<Gm, true, 2>(Rc, vv, yv, X.lane);
+      if (X.lane < NP) {
+        X.V(V_RU)[X.lane] = yv[0] + gmv * su[X.lane];
+        X.V(V_RD)[X.lane] = gmv * yv[1] + sd[X.lane];
+      }
+    }
+    {  // A = I - R^2, RHS = Lambda R^2 + T'
+      float acc[2][4];
+      tc32_tile<NP, LD>(Rr, Rc, r0, c0, X.lane, acc);
+      const float* tpc = Tp[cur];
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + g + 8 * h, c = c0 + 8 * j + 2 * q;
+          const float l = static_cast<float>(lam[r]);
+          const float v0 = acc[j][2 * h], v1 = acc[j][2 * h + 1];
+          const float2 tp = *reinterpret_cast<const float2*>(tpc + r * LD + c);
+          *reinterpret_cast<float2*>(Am + r * LD + c) =
+              make_float2(((r == c) ? 1.f : 0.f) - v0, ((r == c + 1) ? 1.f : 0.f) - v1);
+          *reinterpret_cast<float2*>(RHS + r * LD + c) = make_float2(fmaf(l, v0, tp.x), fmaf(l, v1, tp.y));
+        }
+    }
+    X.sync();
+    *singular |= op_gj_rows<Gm>(X.mo(4), X.mo(8), X.mo(5), t, X.bar);  // G' (row-major)
+    X.sync();
+    {  // TGR = G' R + Lambda R (row-major, over I - R^2)
+      float acc[2][4];
+      tc32_tile<NP, LD>(Gp, Rc, r0, c0, X.lane, acc);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + g + 8 * h, c = c0 + 8 * j + 2 * q;
+          const float l = static_cast<float>(lam[r]);
+          const float2 rv = *reinterpret_cast<const float2*>(Rr + r * LD + c);
+          *reinterpret_cast<float2*>(Am + r * LD + c) =
+              make_float2(fmaf(l, rv.x, acc[j][2 * h]), fmaf(l, rv.y, acc[j][2 * h + 1]));
+        }
+    }
+    X.sync();
+    {  // R <- R + TGR T;  T' <- G' T + Lambda T',  T <- T' + Lambda^2
+      float acc[2][4], acc2[2][4];
+      tc32_tile<NP, LD>(Am, Tc[cur], r0, c0, X.lane, acc);
+      tc32_tile<NP, LD>(Gp, Tc[cur], r0, c0, X.lane, acc2);
+      const float* tpc = Tp[cur];
+      float* tpn = Tp[cur ^ 1];
+      float* tcn = Tc[cur ^ 1];
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int r = r0 + g + 8 * h, c = c0 + 8 * j + 2 * q;
+          const float2 rv = *reinterpret_cast<const float2*>(Rr + r * LD + c);
+          const float n0 = rv.x + acc[j][2 * h], n1 = rv.y + acc[j][2 * h + 1];
+          *reinterpret_cast<float2*>(Rr + r * LD + c) = make_float2(n0, n1);
+          Rc[c * LD + r] = n0;
+          Rc[(c + 1) * LD + r] = n1;
+          const double ld = lam[r];
+          const float l = static_cast<float>(ld), l2 = static_cast<float>(ld * ld);
+          const float2 tp = *reinterpret_cast<const float2*>(tpc + r * LD + c);
+          const float p0 = fmaf(l, tp.x, acc2[j][2 * h]), p1 = fmaf(l, tp.y, acc2[j][2 * h + 1]);
+          *reinterpret_cast<float2*>(tpn + r * LD + c) = make_float2(p0, p1);
+          tcn[c * LD + r] = (r == c) ? p0 + l2 : p0;
+          tcn[(c + 1) * LD + r] = (r == c + 1) ? p1 + l2 : p1;
+        }
+    }
+    if (X.warp == 0) {
+      Real* an = X.V(V_Y0 + 1 - par);
+      Real* bn = X.V(V_Z0 + 1 - par);
+      Real* sun = X.V(V_SU0 + 1 - par);
+      Real* sdn = X.V(V_SD0 + 1 - par);
+      if (X.lane < NP) X.V(V_TMP)[X.lane] = Real(2) * av[X.lane] - bv[X.lane];
+      __syncwarp();
+      const Real* vc[2] = {X.V(V_TMP), bv};
+      Real gv[2], rv[2];
+      matvec<Gm, false, 2>(Gp, vc, gv, X.lane);  // G' c, G' b
+      matvec<Gm, false, 2>(Am, vc, rv, X.lane);  // TGR c, TGR b
+      Real gs[2] = {Real(0), Real(0)};
+      if (solar) {
+        const Real* vs[2] = {X.V(V_RU), X.V(V_RD)};
+        matvec<Gm, false, 2>(Gp, vs, gs, X.lane);
+      }
+      if (X.lane < NP) {
+        const int i = X.lane;
+        const Real l = static_cast<Real>(lam[i]);
+        const Real c = X.V(V_TMP)[i], a = av[i], b = bv[i];
+        an[i] = ((l * c + gv[0]) - rv[1]) + a;
+        bn[i] = ((l * b + gv[1]) - rv[0]) + (Real(2) * b - a);
+        if (solar) {
+          sun[i] = (l * X.V(V_RU)[i] + gs[0]) + su[i];
+          sdn[i] = (l * X.V(V_RD)[i] + gs[1]) + gmv * sd[i];
+        } else {
+          sun[i] = Real(0);
+          sdn[i] = Real(0);
+        }
+        X.DV(D_LAM0 + 1 - par)[i] = lam[i] * lam[i];
+      }
+    }
+    gam = gam * gam;
+    cur ^= 1;
+  }
+  X.sync();
+  {  // T row-major (into the right-hand-side buffer) for the adding
+    const Tile<Gm> tl(t);
+    if (tl.valid()) {
+      Real Tt[TR][TC];
+#pragma unroll
+      for (int a = 0; a < TR; ++a)
+#pragma unroll
+        for (int b = 0; b < TC; ++b) Tt[a][b] = Tc[cur][tl.col(b) * LD + tl.row(a)];
+      tl.store_rm(Tt, RHS);
+    }
+  }
+  if (X.warp == 0 && X.lane < NP) {
+    const int i = X.lane, par = nn & 1;
+    const double a = X.V(V_Y0 + par)[i], b = X.V(V_Z0 + par)[i];
+    const double su = X.V(V_SU0 + par)[i], sd = X.V(V_SD0 + par)[i];
+    double up = 0.0, dn = 0.0;
+    if (i < N) {
+      up = (a * Bb - b * Bt) / tau + su;
+      dn = (a * Bt - b * Bb) / tau + sd;
+    }
+    X.V(V_SUP)[i] = static_cast<Real>(up);
+    X.V(V_SDN)[i] = static_cast<Real>(dn);
+    if (src64) {
+      src64[i] = up;
+      src64[NP + i] = dn;
+    }
+  }
+  return 8;
+}
+
 // Class-D layers that double in FP32: run doubling_lam in the FP32 region
 // at `tbF` (which overlays this group's FP64 matrices), then widen R, T and
 // the sources into the FP64 buffers the adding reads (R -> m0 row-major,
@@ -769,8 +1011,13 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
   using GmF = Geo<GmD::NP, float, GmD::G>;
   constexpr int TR = GmD::TR, TC = GmD::TC, NP = GmD::NP;
   static_assert(GmF::TR == TR && GmF::TC == TC && GmF::G == GmD::G, "tile maps must agree");
-  const int tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0,
-                                   Ppp, Ppm, singular, src64);
+  int tF;
+  if constexpr (UseTC32<GmF>::value && UseGjRows<GmF>::value)
+    tF = doubling_tc<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
+                          singular, src64);
+  else
+    tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp,
+                           Ppm, singular, src64);
   const Ctx<GmF> XF(goff, tbF, t_, bar);
   const Ctx<GmD> XD(goff, tbD, t_, bar);
   XD.sync();
@@ -932,7 +1179,8 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
       const int nn = num_doublings(tau, omc);
       const double tau0 = ldexp(tau, -nn);
       if (nn > kFp64MaxDoublings || tau0 > kFp64StartRatio * mu_min ||
-          (1.0 - omc < kFp64NearConservative && tau > kFp64ThickTau)) {
+          (1.0 - omc < kFp64NearConservative && tau > kFp64ThickTau) ||
+          tau * omc > ADRT_MIX_SCAT_DEPTH) {
         fl = 1.0;
         flagged = 1;
       }
@@ -1407,7 +1655,7 @@ __device__ __noinline__ void multi_task(unsigned goff, int t, int bar, int w, ch
   const int any = wav_prologue<NP>(goff, t, bar, w, sl, lmax, status, precision != 0);
   if (precision == 0) {
     wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, lmax, status);
-  } else if (!any) {
+  } else if (!any && !ADRT_MIX_FORCE_D) {
     wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, lmax, status);
   } else {
     wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl, lmax,

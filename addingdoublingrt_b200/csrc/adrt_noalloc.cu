@@ -12,16 +12,18 @@
 // The work memory is a file-scope __device__ array of kNoAllocScratchBytes
 // (64 MiB) on every GPU that loads the library, held until the process
 // exits.  It holds a 256-byte header (work counter, status word), the
-// quadrature table of the call's N, and as many per-wavenumber work slots
-// as fit; fewer slots than the engine uses means fewer wavenumbers in flight
-// at once, not a different result.  Every call shares the array and it keeps
-// the last call's contents: the counter, status word and quadrature table are
-// rewritten by each call before its kernel runs, so calls that overlap on the
-// GPU (on different streams, or from different host threads) race and must
-// not be issued.
+// quadrature tables of every order N = 2..32 (uploaded once per device and
+// order, by the first call that uses that order), and as many
+// per-wavenumber work slots as fit; fewer slots than the engine uses means
+// fewer wavenumbers in flight at once, not a different result.  Every call
+// shares the array and it keeps the last call's contents: the counter is
+// reset by each call before its kernel runs and the status word collects
+// the flags of every call until adrt_noalloc_read_status clears it, so calls
+// that overlap on the GPU (on different streams, or from different host
+// threads) race and must not be issued.
 #include <cuda_runtime.h>
 
-#include <cmath>
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -33,65 +35,30 @@
 
 using namespace adrt_dev;
 
-void adrt_internal_set_detail(const char* msg);  // adrt_engine.cu
+// adrt_engine.cu (hidden, not exported)
+void adrt_internal_set_detail(const char* msg);
+int adrt_internal_check_batch(const adrt_batch_desc* d, const adrt_inputs* in);
+void adrt_internal_quad_table(int n, int mmax, std::vector<double>& host, double* xfac);
 
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
 constexpr size_t kHeaderBytes = 256;
 constexpr int kMaxDevices = 64;
+constexpr int kThreads = 128;
 
 static __device__ __align__(256) char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// The persistent solve loop of solve_kernel (adrt_kernel.cuh), with its
-// slots, counter and status word in the static work memory.
-template <int NP, int KIND>
-__global__ void __launch_bounds__(128) solve_kernel_static(SolveParams P, ColumnDev col0) {
-  using GD = Geo<NP, double>;
-  using GF = Geo<NP, float>;
-  using GL = GroupLayout<NP, KIND>;
-  constexpr int G = GD::G;
-  const int gib = threadIdx.x / G;
-  const int t = threadIdx.x % G;
-  const int bar = 1 + gib;
-  const unsigned goff = (unsigned)(gib * GL::bytes);
-  const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
-  const int slot = blockIdx.x * (blockDim.x / G) + gib;
-  if (slot >= P.nslots) return;  // the whole group leaves together
-  char* sl = P.scratch + (size_t)slot * P.slot_bytes;
-  for (unsigned i = (unsigned)t * 4u; i < (unsigned)GL::bytes; i += (unsigned)G * 4u)
-    *sp<unsigned>(goff + i) = 0u;
-  gsync<G>(bar);
-  ColumnDev* colp = sp<ColumnDev>(goff + CommonLayout<NP>::col);
-  if (t == 0) *colp = col0;
-  long long* task_s = sp<long long>(goff + CommonLayout<NP>::misc + 32);
-  for (;;) {
-    long long task;
-    if constexpr (G == 32) {
-      unsigned long long v = 0;
-      if (t == 0) v = atomicAdd(P.counter, 1ull);
-      task = (long long)__shfl_sync(0xffffffffu, v, 0);
-    } else {
-      gsync<G>(bar);
-      if (t == 0) *task_s = (long long)atomicAdd(P.counter, 1ull);
-      gsync<G>(bar);
-      task = *task_s;
-    }
-    if (task >= P.ntasks) break;
-    const int w = (int)task;
-    gsync<G>(bar);
-    const int any =
-        wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, KIND == KIND_MIXED);
-    if constexpr (KIND == KIND_FP64) {
-      wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
-    } else if (!any) {
-      wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
-    } else {
-      wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,
-                               P.max_layers, P.status);
-    }
-  }
+// Quadrature tables: order n at quad_offset(n), Legendre rows up to
+// kMaxMoments, so one table serves every moment count.
+constexpr size_t quad_doubles(int n) { return (size_t)(2 + kMaxMoments) * n; }
+constexpr size_t quad_offset(int n) {
+  size_t off = kHeaderBytes;
+  for (int m = 2; m < n; ++m) off += (quad_doubles(m) * sizeof(double) + 255) & ~size_t(255);
+  return off;
 }
+constexpr size_t kSlotsOffset = quad_offset(kMaxN + 1);
+static_assert(kSlotsOffset < kNoAllocScratchBytes / 8, "quadrature tables fit well inside");
 
 int na_fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -103,30 +70,118 @@ int na_fail(int code, const char* fmt, ...) {
   return code;
 }
 
-// Device address of the static work memory, looked up once per device.
-std::mutex g_na_mu;
-char* g_na_addr[kMaxDevices] = {};
+// Launch facts of one kernel instantiation, looked up once per device.
+struct NaKernState {
+  bool ready = false;
+  int blocks_per_sm = 0;
+};
 
-int na_setup(int dev, char** addr) {
-  std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_addr[dev]) {
+// Per-device state: the array's device address, the SM count, which
+// quadrature orders are uploaded (and their 0.5 / sum(mu w)), and the
+// kernels' launch facts [padded order index][kind].
+struct NaDevice {
+  char* addr = nullptr;
+  int sms = 0;
+  bool quad_ready[kMaxN + 1] = {};
+  double xfac[kMaxN + 1] = {};
+  NaKernState kern[4][2];
+};
+std::mutex g_na_mu;
+NaDevice g_na[kMaxDevices];
+
+// Set-up on the current device `dev` (its first call): the device address of
+// the static array (cudaGetSymbolAddress, checked) and the SM count.
+int na_device(int dev, NaDevice** out) {
+  NaDevice& d = g_na[dev];
+  if (!d.addr) {
     void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess)
       return na_fail(ADRT_ERR_CUDA, "cudaGetSymbolAddress of the static work memory: %s",
                      cudaGetErrorString(e));
-    g_na_addr[dev] = static_cast<char*>(p);
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || sms < 1)
+      return na_fail(ADRT_ERR_CUDA, "SM count of device %d: %s", dev, cudaGetErrorString(e));
+    d.sms = sms;
+    d.addr = static_cast<char*>(p);
   }
-  *addr = g_na_addr[dev];
+  *out = &d;
   return ADRT_OK;
 }
 
+// The quadrature table of order n in the static array, uploaded by the first
+// call of this order on this device (a synchronous copy: that call must not be
+// made during a stream capture).
+int na_quad(NaDevice& d, int n, cudaStream_t s) {
+  if (d.quad_ready[n]) return ADRT_OK;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return na_fail(ADRT_ERR_WORKSPACE,
+                   "the first call with num_quadrature=%d on this device uploads its quadrature "
+                   "table and cannot be captured: make one call with this order before capture",
+                   n);
+  std::vector<double> host;
+  double xfac = 0.0;
+  adrt_internal_quad_table(n, kMaxMoments, host, &xfac);
+  const cudaError_t e = cudaMemcpy(d.addr + quad_offset(n), host.data(),
+                                   host.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess)
+    return na_fail(ADRT_ERR_CUDA, "quadrature table upload: %s", cudaGetErrorString(e));
+  d.xfac[n] = xfac;
+  d.quad_ready[n] = true;
+  return ADRT_OK;
+}
+
+// A pointer the kernels may dereference on device `dev`: device memory of
+// `dev`, managed memory, or pinned host memory mapped into the device's
+// address space.  Plain (unregistered) host memory and other devices' memory
+// are refused.
+bool na_device_pointer(const void* p, int dev) {
+  if (!p) return true;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  switch (a.type) {
+    case cudaMemoryTypeDevice: return a.device == dev;
+    case cudaMemoryTypeManaged: return true;
+    case cudaMemoryTypeHost: return a.devicePointer != nullptr;
+    default: return false;
+  }
+}
+
+int na_check_pointers(const adrt_inputs* in, const adrt_outputs* out, int dev) {
+  const void* ins[] = {in->delta_tau,     in->single_scat_albedo, in->phase_moments,
+                       in->temperature,   in->planck_levels,      in->surface_albedo,
+                       in->solar_mu,      in->wavenumber_low,     in->wavenumber_high,
+                       in->surface_emission, in->top_emission};
+  const char* inames[] = {"delta_tau",     "single_scat_albedo", "phase_moments",
+                          "temperature",   "planck_levels",      "surface_albedo",
+                          "solar_mu",      "wavenumber_low",     "wavenumber_high",
+                          "surface_emission", "top_emission"};
+  for (int i = 0; i < 11; ++i)
+    if (!na_device_pointer(ins[i], dev))
+      return na_fail(ADRT_ERR_INVALID_ARGUMENT,
+                     "input %s is not device memory of device %d (host arrays go through "
+                     "adrt_solve_batch_host)", inames[i], dev);
+  const void* outs[] = {out->flux_up,          out->flux_down,     out->flux_direct,
+                        out->mean_intensity,   out->flux_divergence, out->toa_flux_up,
+                        out->toa_flux_down,    out->boa_flux_direct};
+  for (int i = 0; i < 8; ++i)
+    if (!na_device_pointer(outs[i], dev))
+      return na_fail(ADRT_ERR_INVALID_ARGUMENT, "output %d is not device memory of device %d",
+                     i, dev);
+  return ADRT_OK;
+}
+
+// The engine's persistent solve kernel, instantiated in this file.
 struct NaKern {
   int groups;
   size_t smem;
   size_t (*slot_bytes)(int);
-  cudaError_t (*prepare)(size_t);
-  int (*blocks_per_sm)(size_t);
+  cudaError_t (*prepare)(size_t, int*);
   void (*launch)(const SolveParams&, const ColumnDev&, int, size_t, cudaStream_t);
 };
 
@@ -134,25 +189,24 @@ template <int NP, int KIND>
 NaKern na_kern() {
   using GD = Geo<NP, double>;
   NaKern k;
-  k.groups = 128 / GD::G;
+  k.groups = kThreads / GD::G;
   k.smem = (size_t)k.groups * GroupLayout<NP, KIND>::bytes;
   k.slot_bytes = [](int lmax) { return SlotLayout<GD>::bytes(lmax); };
-  k.prepare = [](size_t smem) {
-    return cudaFuncSetAttribute(solve_kernel_static<NP, KIND>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  };
-  k.blocks_per_sm = [](size_t smem) {
-    int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, solve_kernel_static<NP, KIND>, 128, smem);
-    return nb > 0 ? nb : 1;
+  k.prepare = [](size_t smem, int* bps) {
+    cudaError_t e = cudaFuncSetAttribute(solve_kernel<NP, KIND>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, solve_kernel<NP, KIND>, kThreads,
+                                                         smem);
   };
   k.launch = [](const SolveParams& p, const ColumnDev& c, int grid, size_t smem,
-                cudaStream_t s) { solve_kernel_static<NP, KIND><<<grid, 128, smem, s>>>(p, c); };
+                cudaStream_t s) { solve_kernel<NP, KIND><<<grid, kThreads, smem, s>>>(p, c); };
   return k;
 }
 
-NaKern na_pick(int n, int precision) {
-  const int np = n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : 32;
+int na_order_index(int np) { return np == 4 ? 0 : np == 8 ? 1 : np == 16 ? 2 : 3; }
+
+NaKern na_pick(int np, int precision) {
   if (precision == ADRT_PRECISION_MIXED) {
     switch (np) {
       case 4: return na_kern<4, KIND_MIXED>();
@@ -173,76 +227,56 @@ NaKern na_pick(int n, int precision) {
 
 extern "C" int adrt_solve_batch_noalloc(const adrt_batch_desc* d, const adrt_inputs* in,
                                         const adrt_outputs* out, void* stream_ptr) {
-  if (!d || !in || !out) return na_fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
-  if (d->num_wavenumbers < 1 || d->num_layers < 1)
-    return na_fail(ADRT_ERR_INVALID_ARGUMENT, "num_wavenumbers and num_layers must be >= 1");
-  if (d->num_quadrature < 2 || d->num_quadrature > kMaxN)
-    return na_fail(ADRT_ERR_UNSUPPORTED, "num_quadrature %d outside 2..%d", d->num_quadrature,
-                   kMaxN);
-  if (d->num_moments < 1 || d->num_moments > kMaxMoments)
-    return na_fail(ADRT_ERR_INVALID_ARGUMENT, "num_moments must be in 1..%d", kMaxMoments);
-  if (d->moment_layout < 0 || d->moment_layout > 2)
-    return na_fail(ADRT_ERR_INVALID_ARGUMENT, "unknown moment_layout %d", d->moment_layout);
-  if (d->precision != ADRT_PRECISION_FP64 && d->precision != ADRT_PRECISION_MIXED)
-    return na_fail(ADRT_ERR_INVALID_ARGUMENT, "unknown precision %d", d->precision);
-  if (!in->delta_tau || !in->single_scat_albedo || !in->phase_moments ||
-      (d->use_thermal_emission && !in->temperature))
-    return na_fail(ADRT_ERR_INVALID_ARGUMENT, "missing input array");
+  // the checks of adrt_solve_batch, so both refuse the same batches
+  int rc = adrt_internal_check_batch(d, in);
+  if (rc) return rc;
+  if (!out) return na_fail(ADRT_ERR_INVALID_ARGUMENT, "null outputs");
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return na_fail(ADRT_ERR_CUDA, "no usable current device");
-  char* base = nullptr;
-  int rc = na_setup(dev, &base);
-  if (rc) return rc;
+  if ((rc = na_check_pointers(in, out, dev))) return rc;
 
-  // quadrature table of this N: nodes, weights, P_l(mu_i) for l < mmax
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  NaDevice* nd = nullptr;
+  if ((rc = na_device(dev, &nd))) return rc;
   const int n = d->num_quadrature;
-  const int mmax = d->num_moments > 2 * n ? d->num_moments : 2 * n;
-  std::vector<double> q((size_t)2 * n + (size_t)mmax * n);
-  if ((rc = adrt_gauss_legendre(n, q.data(), q.data() + n)))
-    return na_fail(rc, "quadrature set-up failed");
-  double* pl = q.data() + 2 * n;
-  double sum_mw = 0.0;
-  for (int i = 0; i < n; ++i) {
-    pl[i] = 1.0;
-    if (mmax > 1) pl[n + i] = q[i];
-    sum_mw += q[i] * q[n + i];
+  if ((rc = na_quad(*nd, n, s))) return rc;
+
+  const int np = n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : 32;
+  const int kind = d->precision == ADRT_PRECISION_MIXED ? 1 : 0;
+  NaKern k = na_pick(np, d->precision);
+  NaKernState& ks = nd->kern[na_order_index(np)][kind];
+  if (!ks.ready) {
+    int bps = 0;
+    const cudaError_t e = k.prepare(k.smem, &bps);
+    if (e != cudaSuccess || bps < 1)
+      return na_fail(ADRT_ERR_CUDA, "kernel set-up: %s", cudaGetErrorString(e));
+    ks.blocks_per_sm = bps;
+    ks.ready = true;
   }
-  for (int l = 2; l < mmax; ++l)
-    for (int i = 0; i < n; ++i)
-      pl[l * n + i] = ((2 * l - 1) * q[i] * pl[(l - 1) * n + i] - (l - 1) * pl[(l - 2) * n + i]) / l;
-  const size_t qbytes = (q.size() * sizeof(double) + 255) & ~size_t(255);
-
-  NaKern k = na_pick(n, d->precision);
   const size_t slot = (k.slot_bytes(d->num_layers) + 255) & ~size_t(255);
-  const size_t room = kNoAllocScratchBytes - kHeaderBytes - qbytes;
-  if (slot > room)
+  const size_t room = kNoAllocScratchBytes - kSlotsOffset;
+  // whole blocks of slots: every thread group of a launched block owns one
+  long long blocks = (long long)(room / slot) / k.groups;
+  if (blocks < 1)
     return na_fail(ADRT_ERR_WORKSPACE,
-                   "one wavenumber needs %zu bytes of work memory at L=%d, N=%d; the static "
-                   "work memory holds %zu (reduce num_layers)",
-                   slot, d->num_layers, n, room);
-  cudaError_t e = k.prepare(k.smem);
-  if (e != cudaSuccess) return na_fail(ADRT_ERR_CUDA, "kernel set-up: %s", cudaGetErrorString(e));
-  int sms = 0;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long resident = (long long)k.blocks_per_sm(k.smem) * sms * k.groups;
-  long long nslots = (long long)(room / slot);
-  if (nslots > resident) nslots = resident;
-  if (nslots > d->num_wavenumbers) nslots = d->num_wavenumbers;
-  const int grid = (int)((nslots + k.groups - 1) / k.groups);
+                   "one block of %d wavenumber slots needs %zu bytes of work memory at L=%d, "
+                   "N=%d; the static work memory holds %zu (reduce num_layers)",
+                   k.groups, slot * k.groups, d->num_layers, n, room);
+  blocks = std::min<long long>(blocks, (long long)ks.blocks_per_sm * nd->sms);
+  blocks = std::min<long long>(blocks, (d->num_wavenumbers + k.groups - 1) / k.groups);
 
-  double* qdev = reinterpret_cast<double*>(base + kHeaderBytes);
-  if ((e = cudaMemsetAsync(base, 0, kHeaderBytes, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(qdev, q.data(), q.size() * sizeof(double), cudaMemcpyHostToDevice,
-                           s)) != cudaSuccess)
-    return na_fail(ADRT_ERR_CUDA, "work memory set-up: %s", cudaGetErrorString(e));
+  char* base = nd->addr;
+  const cudaError_t e0 = cudaMemsetAsync(base, 0, sizeof(unsigned long long), s);
+  if (e0 != cudaSuccess)
+    return na_fail(ADRT_ERR_CUDA, "work counter reset: %s", cudaGetErrorString(e0));
 
   ColumnDev c{};
   c.W = d->num_wavenumbers;
   c.L = d->num_layers;
   c.N = n;
-  c.NP = n <= 4 ? 4 : n <= 8 ? 8 : n <= 16 ? 16 : 32;
+  c.NP = np;
   c.M = d->num_moments;
   c.moment_layout = d->moment_layout;
   c.thermal = d->use_thermal_emission;
@@ -280,11 +314,12 @@ extern "C" int adrt_solve_batch_noalloc(const adrt_batch_desc* d, const adrt_inp
   c.toa_fu = out->toa_flux_up;
   c.toa_fd = out->toa_flux_down;
   c.boa_fdir = out->boa_flux_direct;
-  c.quad.mu = qdev;
-  c.quad.wt = qdev + n;
-  c.quad.pl = qdev + 2 * n;
-  c.quad.mmax = mmax;
-  c.quad.xfac = 0.5 / sum_mw;
+  const double* q = reinterpret_cast<const double*>(base + quad_offset(n));
+  c.quad.mu = q;
+  c.quad.wt = q + n;
+  c.quad.pl = q + 2 * n;
+  c.quad.mmax = kMaxMoments;
+  c.quad.xfac = nd->xfac[n];
   c.task_begin = 0;
 
   SolveParams p{};
@@ -293,12 +328,34 @@ extern "C" int adrt_solve_batch_noalloc(const adrt_batch_desc* d, const adrt_inp
   p.ntasks = d->num_wavenumbers;
   p.counter = reinterpret_cast<unsigned long long*>(base);
   p.status = reinterpret_cast<unsigned int*>(base + 8);
-  p.scratch = base + kHeaderBytes + qbytes;
+  p.scratch = base + kSlotsOffset;
   p.slot_bytes = slot;
-  p.nslots = (int)nslots;
+  p.nslots = (int)(blocks * k.groups);
   p.max_layers = d->num_layers;
-  k.launch(p, c, grid, k.smem, s);
-  if ((e = cudaGetLastError()) != cudaSuccess)
+  k.launch(p, c, (int)blocks, k.smem, s);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
     return na_fail(ADRT_ERR_CUDA, "solve kernel launch: %s", cudaGetErrorString(e));
+  return ADRT_OK;
+}
+
+extern "C" int adrt_noalloc_read_status(void* stream_ptr, int* flags) {
+  if (!flags) return na_fail(ADRT_ERR_INVALID_ARGUMENT, "null flags");
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+    return na_fail(ADRT_ERR_CUDA, "no usable current device");
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  NaDevice* nd = nullptr;
+  int rc = na_device(dev, &nd);
+  if (rc) return rc;
+  unsigned int v = 0;
+  unsigned int* st = reinterpret_cast<unsigned int*>(nd->addr + 8);
+  cudaError_t e = cudaMemcpyAsync(&v, st, sizeof v, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(st, 0, sizeof v, s);
+  if (e != cudaSuccess)
+    return na_fail(ADRT_ERR_CUDA, "status read: %s", cudaGetErrorString(e));
+  *flags = (int)v;
   return ADRT_OK;
 }

@@ -808,6 +808,207 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
   return singular;
 }
 
+// ============================================================== FP32 on the tensor cores
+// FP32 products as three TF32 tensor-core products (mma.sync m16n8k8 tf32,
+// FP32 accumulation): x = x_hi + x_lo with x_hi = tf32(x) and x_lo =
+// tf32(x - x_hi) (both rounded to nearest), and X Y = X_lo Y_hi + X_hi Y_lo +
+// X_hi Y_hi (the X_lo Y_lo term, 2^-22 relative, is dropped).  The error per
+// product is about 2^-21 of |X| |Y|, close to an FP32 product's; the tensor
+// pipe issues the 16x16x16 product in 12 instructions against 128 FFMA.
+template <class Gm>
+struct UseTC32 {
+  static constexpr bool value = ADRT_GEMM_MMA && sizeof(typename Gm::Real) == 4 &&
+                                ((Gm::NP == 16 && Gm::G == 32) || (Gm::NP == 32 && Gm::G == 128));
+};
+
+__device__ __forceinline__ unsigned tf32_rna(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32_m16n8k8(float (&d)[4], const unsigned (&a)[4],
+                                                 const unsigned (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// The warp's 16 x 16 output tile at (r0, c0) of C = X Y: X row-major, Y given
+// column-major (YT[n * LD + k] = Y[k][n]), both FP32 in smem with pitch LD.
+// acc[j][e] is element (r0 + g + 8 (e >> 1), c0 + 8 j + 2 q + (e & 1)) with
+// g = lane / 4, q = lane % 4 (the m16n8 accumulator fragment of column tile j).
+// With LD = NP + 4 every operand load is free of bank conflicts.
+template <int NP, int LD>
+__device__ __forceinline__ void tc32_tile(const float* __restrict__ X, const float* __restrict__ YT,
+                                          int r0, int c0, int lane, float (&acc)[2][4]) {
+  const int g = lane >> 2, q = lane & 3;
+  float hi[2][4], lo[2][4];  // X_hi Y_hi and the two correction products, apart
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) hi[j][e] = lo[j][e] = 0.f;
+#pragma unroll
+  for (int k0 = 0; k0 < NP; k0 += 8) {
+    float xa[4], yb[2][2];
+    xa[0] = X[(r0 + g) * LD + k0 + q];
+    xa[1] = X[(r0 + g + 8) * LD + k0 + q];
+    xa[2] = X[(r0 + g) * LD + k0 + q + 4];
+    xa[3] = X[(r0 + g + 8) * LD + k0 + q + 4];
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      yb[j][0] = YT[(c0 + 8 * j + g) * LD + k0 + q];
+      yb[j][1] = YT[(c0 + 8 * j + g) * LD + k0 + q + 4];
+    }
+    unsigned ah[4], al[4], bh[2][2], bl[2][2];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      ah[e] = tf32_rna(xa[e]);
+      al[e] = tf32_rna(xa[e] - __uint_as_float(ah[e]));
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        bh[j][e] = tf32_rna(yb[j][e]);
+        bl[j][e] = tf32_rna(yb[j][e] - __uint_as_float(bh[j][e]));
+      }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      mma_tf32_m16n8k8(lo[j], al, bh[j]);
+      mma_tf32_m16n8k8(lo[j], ah, bl[j]);
+      mma_tf32_m16n8k8(hi[j], ah, bh[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = hi[j][e] + lo[j][e];
+}
+
+// The warp's output tile origin in a group of NP x NP products: one 16 x 16
+// tile per warp (one warp at NP = 16, four at NP = 32).
+template <class Gm>
+__device__ __forceinline__ void tc32_origin(int t, int& r0, int& c0) {
+  const int warp = t >> 5;
+  r0 = (Gm::NP == 32) ? 16 * (warp >> 1) : 0;
+  c0 = (Gm::NP == 32) ? 16 * (warp & 1) : 0;
+}
+
+// FP32 right-solve X = B A^{-1} without pivoting, one row of [A; B] per
+// thread (two threads per row, each half of the columns, at NP = 32).  The
+// matrices inverted are diagonally dominant (I - R R' with reflection
+// matrices R, R'), so elimination without pivoting is backward stable (see
+// gj_mma).  Columns are eliminated four at a time: the panel's pivot rows and
+// every row's panel entries are published, each thread forms its row's panel
+// entries times the 4 x 4 pivot block's inverse, x' = x P^{-1}, and updates
+// its other columns c by x' P[:, c].  A and B are row-major (pitch LD); the
+// result goes row-major to `out`, whose buffer is also the scratch of the
+// publication (2NP x 4 panel entries, then 4 pivot rows).  Returns nonzero if
+// a pivot was exactly 0.
+template <class Gm>
+struct UseGjRows {
+  static constexpr int NP = Gm::NP, G = Gm::G;
+  static constexpr bool value = sizeof(typename Gm::Real) == 4 && (NP == 16 || NP == 32) &&
+                                G % (2 * NP) == 0 && NP / (G / (2 * NP)) >= 4;
+};
+
+template <class Gm, int PART>
+__device__ __forceinline__ int gj_rows_part(const float* A, const float* B, float* out, int row,
+                                            int bar) {
+  constexpr int NP = Gm::NP, LD = Gm::LD, G = Gm::G;
+  constexpr int ROWS = 2 * NP, TPR = G / ROWS, CPT = NP / TPR, C0 = PART * CPT;
+  constexpr int RS = NP + 4;  // pivot-row pitch
+  float* lbuf = out;
+  float* rbuf = out + ROWS * 4;
+  float v[CPT];
+  const float* src = (row < NP) ? A + row * LD : B + (row - NP) * LD;
+  lds_vec<float, CPT>(v, src + C0);
+  int singular = 0;
+#pragma unroll
+  for (int j = 0; j < NP / 4; ++j) {
+    const int pc = 4 * j;
+    // 1. publish this row's panel entries and, on the pivot rows, the row
+    if (pc >= C0 && pc < C0 + CPT)
+      *reinterpret_cast<float4*>(lbuf + row * 4) =
+          make_float4(v[(pc - C0) & (CPT - 1)], v[(pc - C0 + 1) & (CPT - 1)],
+                      v[(pc - C0 + 2) & (CPT - 1)], v[(pc - C0 + 3) & (CPT - 1)]);
+    if (row >= pc && row < pc + 4) sts_vec<float, CPT>(rbuf + (row - pc) * RS + C0, v);
+    gsync<G>(bar);
+    // 2. x' = x P^{-1} (every thread factors the pivot block itself)
+    float P[4][4], x[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) lds_vec<float, 4>(P[a], rbuf + a * RS + pc);
+    lds_vec<float, 4>(x, lbuf + row * 4);
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const float piv = P[s][s];
+      singular |= (piv == 0.f);
+      const float inv = recip(piv);
+      const float fx = x[s] * inv;
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (c != s) x[c] = fmaf(-fx, P[s][c], x[c]);
+      x[s] = fx;
+#pragma unroll
+      for (int s2 = s + 1; s2 < 4; ++s2) {
+        const float f = P[s2][s] * inv;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c != s) P[s2][c] = fmaf(-f, P[s][c], P[s2][c]);
+        P[s2][s] = f;
+      }
+    }
+    if (row >= pc && row < pc + 4) {  // pivot rows take the exact unit rows
+#pragma unroll
+      for (int c = 0; c < 4; ++c) x[c] = (c == row - pc) ? 1.f : 0.f;
+    }
+    // 3. the row's columns: panel columns take x', the others lose x' P[:, c]
+#pragma unroll
+    for (int c4 = 0; c4 < CPT; c4 += 4) {
+      const int c = C0 + c4;
+      if (c == pc) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) v[c4 + e] = x[e];
+      } else {
+        float pr[4][4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) lds_vec<float, 4>(pr[s], rbuf + s * RS + c);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          float a = v[c4 + e];
+#pragma unroll
+          for (int s = 0; s < 4; ++s) a = fmaf(-x[s], pr[s][e], a);
+          v[c4 + e] = a;
+        }
+      }
+    }
+    gsync<G>(bar);  // the next panel (or the result) overwrites the publication
+  }
+  if (row >= NP) sts_vec<float, CPT>(out + (row - NP) * LD + C0, v);
+  return singular;
+}
+
+template <class Gm>
+__device__ __noinline__ int op_gj_rows(unsigned a_off, unsigned b_off, unsigned out_off, int t,
+                                       int bar) {
+  static_assert(UseGjRows<Gm>::value, "row-parallel Gauss-Jordan geometry");
+  constexpr int ROWS = 2 * Gm::NP;
+  const float* A = sp<float>(a_off);
+  const float* B = sp<float>(b_off);
+  float* out = sp<float>(out_off);
+  // warp-uniform halves at NP = 32 (rows t % 64, column half t / 64)
+  const int row = t % ROWS, part = t / ROWS;
+  if constexpr (Gm::G / ROWS == 1) {
+    return gj_rows_part<Gm, 0>(A, B, out, row, bar);
+  } else {
+    return part == 0 ? gj_rows_part<Gm, 0>(A, B, out, row, bar)
+                     : gj_rows_part<Gm, 1>(A, B, out, row, bar);
+  }
+}
+
 // Tile copies between the HBM scratch and smem.  The HBM side is in the tile
 // order of GO: the group's own (thread t owns TE contiguous Reals) or, for
 // records written by a kernel of another group size, that kernel's order.

@@ -173,6 +173,32 @@ def config2(W=100_000, L=100, seed=2, precision=_abi.PRECISION_FP64) -> Batch:
     return b
 
 
+def config2_scalar(W=100_000, L=100, seed=2, precision=_abi.PRECISION_FP64) -> Batch:
+    """Config 2's shape (W x 100 layers, N=16, 32 double-HG moments, thermal +
+    solar, the same optical-depth, albedo and temperature distributions) within
+    the reference GPU API's limits (src_cuda/cuda_solver.cuh:18-40, and the
+    per-layer phase tables of src_cuda/cuda_batched_solver.cu:112-180): moment
+    sets shared over wavenumbers (one per layer), one surface albedo (0.15),
+    solar cosine (0.55) and Planck band (1000-1000.025 cm^-1) per batch.  The
+    workload on which the engine and the reference's own GPU solver are timed
+    side by side."""
+    rng = np.random.default_rng(seed)
+    N, M = 16, 32
+    d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
+                       moment_layout=_abi.MOMENTS_SHARED, precision=precision,
+                       use_thermal_emission=1, use_delta_m=1, surface_temperature=300.0,
+                       solar_flux=1.0, solar_mu=0.55, surface_albedo=0.15,
+                       wavenumber_low=1000.0, wavenumber_high=1000.025)
+    b = Batch(d)
+    b.set("delta_tau", 10.0 ** rng.uniform(-4.0, 1.0, size=(W, L)))
+    b.set("single_scat_albedo", rng.uniform(0.0, 0.99, size=(W, L)))
+    f = rng.uniform(0.7, 0.95, size=L)
+    b.set("phase_moments", dhg_moments(f, rng.uniform(0.5, 0.9, size=L),
+                                       rng.uniform(-0.5, 0.0, size=L), M))
+    b.set("temperature", level_temperatures(rng, L))
+    return b
+
+
 def config3(W=20_000, L=60, seed=3, precision=_abi.PRECISION_FP64) -> Batch:
     """Precision stress: N=32, 1-omega = 10^U(-7,-1), tau = 10^U(-5,3), HG g~U(0,0.95),
     diffusion lower boundary, thermal + solar."""

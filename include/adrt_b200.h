@@ -249,18 +249,31 @@ int adrt_validate_batch(const adrt_batch_desc* desc, const adrt_inputs* host_in)
  * reference).  For callers that cannot call cudaMalloc -- inside a framework
  * whose caching allocator already holds the GPU's memory, on a latency-bound
  * path where an allocation's implicit synchronisation is not acceptable, or
- * in a plugin host that only hands over its own buffers.  Same arguments and
- * results as adrt_solve_batch, without an engine: the work memory is one
- * fixed 64 MiB array compiled into the library (present on every GPU that
- * loads it, until the process exits).  The first call on a device looks up
- * that array's device address; make it before any stream capture.  A batch
- * whose per-wavenumber work memory (about (L+1) x 25 KB at N=32 in FP64)
- * does not fit is rejected with ADRT_ERR_WORKSPACE.  All calls share the
- * array and it keeps the last call's contents; each call resets what must
- * start at zero, so calls that overlap on the GPU race and must not be
- * issued.  The device status word is not reported by this entry point. */
+ * in a plugin host that only hands over its own buffers.  Same arguments,
+ * argument checks and results as adrt_solve_batch, without an engine: the
+ * work memory is one fixed 64 MiB array compiled into the library (present
+ * on every GPU that loads it, until the process exits).  Arrays must be
+ * memory of the current device (or managed / mapped pinned memory); plain
+ * host arrays are refused with ADRT_ERR_INVALID_ARGUMENT.  The first call on
+ * a device looks up that array's device address, and the first call with
+ * each num_quadrature uploads that order's quadrature table (synchronously);
+ * make those calls before any stream capture (a capturing first call is
+ * refused with ADRT_ERR_WORKSPACE).  A batch of which one block of
+ * wavenumber slots (4 at N <= 16, 1 at N = 32; about (L+1) x 25 KB per
+ * wavenumber at N = 32 in FP64) does not fit is rejected with
+ * ADRT_ERR_WORKSPACE.  All calls share the array and it keeps the last
+ * call's contents; each call resets its work counter, so calls that overlap
+ * on the GPU race and must not be issued.  The device status word collects
+ * the flags of every call until adrt_noalloc_read_status reads and clears
+ * it. */
 int adrt_solve_batch_noalloc(const adrt_batch_desc* desc, const adrt_inputs* in,
                              const adrt_outputs* out, void* cuda_stream);
+
+/* Synchronise `cuda_stream` and read (and clear) the device status word of
+ * adrt_solve_batch_noalloc calls on the current device (enum adrt_device_flag
+ * bits), as adrt_engine_read_status does for an engine.  Allocates nothing
+ * (no counterpart in the reference). */
+int adrt_noalloc_read_status(void* cuda_stream, int* flags);
 
 /* ------------------------------------------------------------- adjoint */
 

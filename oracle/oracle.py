@@ -36,9 +36,9 @@ def reference_present() -> bool:
     return os.path.isdir(os.path.join(reference_dir(), "src"))
 
 
-def make(target: str, quiet: bool = True, **kw) -> subprocess.CompletedProcess:
+def make(target: str, quiet: bool = True, jobs: int = 1, **kw) -> subprocess.CompletedProcess:
     """`make -C oracle <target> REF=<reference_dir()>`."""
-    cmd = ["make", "-s", "-C", HERE, target, f"REF={reference_dir()}"]
+    cmd = ["make", "-s", f"-j{jobs}", "-C", HERE, target, f"REF={reference_dir()}"]
     if quiet:
         kw.setdefault("stdout", subprocess.DEVNULL)
     return subprocess.run(cmd, **kw)

@@ -245,14 +245,39 @@ def test_index_from_bottom_is_a_reversal(eng):
         assert np.array_equal(bot[k].reshape(8, L + 1)[:, ::-1], top[k].reshape(8, L + 1)), k
 
 
-def test_mixed_precision_accuracy_bound(eng):
-    """The mixed form's normalised error on config-2 samples (recorded bound)."""
-    b = workloads.config2(precision=_abi.PRECISION_MIXED).subset(np.arange(0, 100_000, 997))
+MIXED_CASES = [
+    # (name, batch, bound per wavenumber and output on the normalised error)
+    ("config1", lambda: workloads.config1(W=1000).subset(np.arange(0, 1000, 5)), 1e-6),
+    ("config2", lambda: workloads.config2(precision=_abi.PRECISION_MIXED).subset(
+        np.arange(0, 100_000, 97)), 1e-6),
+    ("config5", lambda: workloads.config5(precision=_abi.PRECISION_MIXED).subset(
+        np.arange(0, 10_000, 11)), 1e-6),
+    # the precision-stress workload (N = 32, 1 - omega down to 1e-7, tau up to
+    # 1e3): a stated bound, measured 2.2e-6 on 500 wavenumbers
+    ("config3", lambda: workloads.config3(precision=_abi.PRECISION_MIXED).subset(
+        np.arange(0, 20_000, 83)), 5e-6),
+]
+
+
+@pytest.mark.parametrize("name,make,bound", MIXED_CASES, ids=[c[0] for c in MIXED_CASES])
+def test_mixed_precision_accuracy(eng, name, make, bound):
+    """The mixed form against the FP64 oracle, per wavenumber and output
+    (F_up, F_down, F_dir, J), normalised by the wavenumber's largest value:
+    err <= bound + 30 sens, sens being the scheme's own FP64 round-off
+    sensitivity on that wavenumber (as in the FP64 parity tests)."""
+    b = make()
+    b.desc.precision = _abi.PRECISION_MIXED
     ref = oracle.solve_oracle(b, os.cpu_count() or 1)
+    sens_ref = oracle.solve_oracle(b, os.cpu_count() or 1, fma=True)
     res = run_device(eng, b)
-    for k in ("flux_up", "flux_down", "mean_intensity"):
-        e = oracle.norm_error(res[k], ref[k], b.L + 1)
-        assert e < 5e-3, (k, e)
+    per = b.L + 1
+    for k in ("flux_up", "flux_down", "flux_direct", "mean_intensity"):
+        e = per_wav_norm_err(res[k], ref[k], per)
+        s = per_wav_norm_err(sens_ref[k], ref[k], per)
+        lim = bound + 30.0 * s
+        bad = np.nonzero(e > lim)[0]
+        assert bad.size == 0, (name, k, int(bad[0]), float(e[bad[0]]), float(lim[bad[0]]))
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_BAD_INPUT) == 0
 
 
 def test_invalid_arguments_raise(eng):

@@ -1,4 +1,4 @@
-"""The allocation-free entry point adrt_solve_batch_noalloc (GPU).
+"""The allocation-free entry point adrt_solve_batch_noalloc.
 
 Callers that cannot allocate device memory -- code running under a
 framework's caching allocator that already holds the GPU, latency-bound
@@ -6,10 +6,12 @@ retrieval loops, plugin hosts that only lend their own buffers -- solve
 through adrt_solve_batch_noalloc, whose work memory is a fixed array inside
 the library.  This file checks, through the C ABI, that two calls in a row
 give the same fluxes as the engine's adrt_solve_batch on the same inputs,
-within the FP64 parity tolerance of the other GPU tests, and that a batch
-too large for the fixed work memory is refused with a clear error.  It is
-named to be collected last, and works alone in a fresh process or after the
-other tests.
+within the FP64 parity tolerance of the other GPU tests, and against the
+oracle; that a batch too large for the fixed work memory, plain host arrays
+and the batches adrt_solve_batch refuses are refused with a clear error; and
+that its device status word is read and cleared by adrt_noalloc_read_status.
+It is named to be collected last, and works alone in a fresh process or
+after the other tests.
 """
 import ctypes as C
 
@@ -19,18 +21,24 @@ import pytest
 from conftest import cuda_available
 from addingdoublingrt_b200 import _abi, _lib, workloads
 
-pytestmark = pytest.mark.gpu
 
-
-def _call_noalloc(lib, desc, di, do):
+def _call_noalloc(lib, desc, di, do, raw_ptrs=False):
     from addingdoublingrt_b200.engine import _ptr
+    ptr = (lambda a: None if a is None else a.ctypes.data) if raw_ptrs else _ptr
     ins = _abi.Inputs()
     for f in _abi.INPUT_FIELDS:
-        setattr(ins, f, _ptr(di.get(f)))
+        setattr(ins, f, ptr(di.get(f)))
     outs = _abi.Outputs()
     for f in _abi.OUTPUT_FIELDS:
-        setattr(outs, f, _ptr(do.get(f)))
+        setattr(outs, f, ptr(do.get(f)))
     return lib.adrt_solve_batch_noalloc(C.byref(desc), C.byref(ins), C.byref(outs), None)
+
+
+def _read_status(lib):
+    v = C.c_int(-1)
+    assert lib.adrt_noalloc_read_status(None, C.byref(v)) == 0, \
+        lib.adrt_last_status_detail().decode()
+    return v.value
 
 
 def _norm_err(x, ref, per):
@@ -41,6 +49,28 @@ def _norm_err(x, ref, per):
     return float(np.max(np.max(np.abs(x - ref), axis=1) / s))
 
 
+def test_noalloc_refuses_what_the_engine_refuses():
+    """The entry point runs adrt_solve_batch's own argument checks first (no
+    GPU is touched before they pass): a solar beam with solar_mu = 0, an
+    albedo outside [0, 1], a surface temperature without thermal emission."""
+    lib = _lib.load()
+    cases = []
+    b = workloads.config1(W=4)
+    b.desc.solar_mu = 0.0
+    cases.append((b, "solar_mu"))
+    b = workloads.config1(W=4)
+    b.desc.surface_albedo = 1.5
+    cases.append((b, "surface_albedo"))
+    b = workloads.config1(W=4)
+    b.desc.surface_temperature = 300.0
+    cases.append((b, "surface_temperature"))
+    for b, word in cases:
+        rc = _call_noalloc(lib, b.desc, b.arrays, b.alloc_outputs(("flux_up",)), raw_ptrs=True)
+        assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT
+        assert word in lib.adrt_last_status_detail().decode()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision", [_abi.PRECISION_FP64, _abi.PRECISION_MIXED])
 def test_noalloc_matches_engine_on_two_calls(precision):
     if not cuda_available():
@@ -67,8 +97,68 @@ def test_noalloc_matches_engine_on_two_calls(precision):
         for k in ("toa_flux_up", "toa_flux_down", "boa_flux_direct"):
             got = do[k].cpu().numpy()
             assert np.allclose(got, ref[k], rtol=1e-9, atol=1e-12 * np.max(np.abs(ref[k]))), (call, k)
+    assert _read_status(lib) == 0
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("N,L", [(16, 2000), (32, 1000)])
+def test_noalloc_few_slots_against_the_oracle(N, L):
+    """Batches so deep that the fixed work memory holds fewer wavenumber slots
+    than the GPU has resident thread groups (one or two blocks of slots, the
+    last wavenumbers taken by a partly idle grid), compared with the oracle."""
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    from oracle import oracle
+    lib = _lib.load()
+    b = workloads.random_small(11, N=N, L=L, W=9, use_thermal_emission=1)
+    di = to_device(b)
+    do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+    rc = _call_noalloc(lib, b.desc, di, do)
+    assert rc == 0, lib.adrt_last_status_detail().decode()
+    torch.cuda.synchronize()
+    ref = oracle.solve_oracle(b, which=_abi.INTERFACE_OUTPUTS)
+    reff = oracle.solve_oracle(b, which=_abi.INTERFACE_OUTPUTS, fma=True)
+    for k in _abi.INTERFACE_OUTPUTS:
+        sens = _norm_err(reff[k], ref[k], b.L + 1)
+        e = _norm_err(do[k].cpu().numpy(), ref[k], b.L + 1)
+        assert e <= 1e-6 + 1000 * sens, (k, e, sens)
+    assert _read_status(lib) & _abi.ADRT_FLAG_NONFINITE == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_status_word_is_read_and_cleared():
+    """A negative optical depth in the device arrays is flagged on the device
+    (as by the engine); adrt_noalloc_read_status reports it once, then 0."""
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    lib = _lib.load()
+    _read_status(lib)
+    b = workloads.config1(W=4)
+    b.arrays["delta_tau"].reshape(-1)[5] = -1.0
+    di = to_device(b)
+    do = alloc_device_outputs(b, ("flux_up",))
+    assert _call_noalloc(lib, b.desc, di, do) == 0, lib.adrt_last_status_detail().decode()
+    assert _read_status(lib) & _abi.ADRT_FLAG_BAD_INPUT
+    assert _read_status(lib) == 0
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_host_arrays():
+    """Plain host (numpy) arrays handed straight to the C entry point are
+    refused before any kernel sees a host address."""
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    lib = _lib.load()
+    b = workloads.config1(W=4)
+    rc = _call_noalloc(lib, b.desc, b.arrays, b.alloc_outputs(("flux_up",)), raw_ptrs=True)
+    assert rc == _abi.ADRT_ERR_INVALID_ARGUMENT
+    assert "not device memory" in lib.adrt_last_status_detail().decode()
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_a_batch_beyond_its_work_memory():
     if not cuda_available():
         pytest.skip("no CUDA device")
@@ -82,11 +172,13 @@ def test_noalloc_rejects_a_batch_beyond_its_work_memory():
     b.set("phase_moments", np.tile(b.arrays["phase_moments"].reshape(-1)[:b.desc.num_moments],
                                    4000))
     b.desc.use_thermal_emission = 0
+    b.desc.surface_temperature = -1.0
+    b.desc.top_temperature = -1.0
     b.arrays.pop("temperature", None)
     b.arrays.pop("planck_levels", None)
     b.desc.use_diffusion_lower_bc = 0
     di = to_device(b)
     do = alloc_device_outputs(b, ("flux_up",))
     rc = _call_noalloc(lib, b.desc, di, do)
-    assert rc == _abi.ADRT_ERR_WORKSPACE
+    assert rc == _abi.ADRT_ERR_WORKSPACE, lib.adrt_last_status_detail().decode()
     assert "work memory" in lib.adrt_last_status_detail().decode()
