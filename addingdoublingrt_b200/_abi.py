@@ -19,6 +19,7 @@ ADRT_ERR_NUMERICAL = -6
 ADRT_FLAG_SINGULAR_PIVOT = 1
 ADRT_FLAG_NONFINITE = 2
 ADRT_FLAG_BAD_INPUT = 4
+ADRT_FLAG_PIVOT_FALLBACK = 8
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
@@ -126,6 +127,26 @@ class Gradients(C.Structure):
 
 class ColumnDesc(C.Structure):
     _fields_ = [("desc", BatchDesc), ("inp", Inputs), ("out", Outputs)]
+
+
+MAPPING_WARP = 0
+MAPPING_THREAD = 1
+
+
+class UnevenPlan(C.Structure):
+    """adrt_uneven_plan: mapping per padded order 4 / 8 / 16, the warp launch's
+    blocks per SM (0 = occupancy limit), longest-first ordering, and the
+    autotuner's measured ns per wavenumber [order][warp, thread]."""
+    _fields_ = [("mapping", C.c_int * 3), ("warp_blocks_per_sm", C.c_int),
+                ("cost_order", C.c_int), ("ns_per_wavenumber", (C.c_double * 2) * 3)]
+
+    def as_dict(self) -> dict:
+        return {"mapping": {o: ("thread" if self.mapping[i] else "warp")
+                            for i, o in enumerate((4, 8, 16))},
+                "warp_blocks_per_sm": self.warp_blocks_per_sm, "cost_order": self.cost_order,
+                "ns_per_wavenumber": {o: {"warp": self.ns_per_wavenumber[i][0],
+                                          "thread": self.ns_per_wavenumber[i][1]}
+                                      for i, o in enumerate((4, 8, 16))}}
 
 
 def array_counts(d: BatchDesc) -> dict:

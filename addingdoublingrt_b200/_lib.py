@@ -41,6 +41,9 @@ EXPORTS = (
     "adrt_band_integrate",
     "adrt_engine_set_adjoint_mode",
     "adrt_engine_device",
+    "adrt_engine_autotune_uneven",
+    "adrt_engine_set_uneven_plan",
+    "adrt_engine_get_uneven_plan",
 )
 
 
@@ -91,6 +94,10 @@ def load(build_if_missing: bool = False) -> C.CDLL:
                                              P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
         lib.adrt_engine_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
         lib.adrt_engine_device.argtypes = [C.c_void_p, P(C.c_int)]
+        lib.adrt_engine_autotune_uneven.argtypes = [C.c_void_p, P(_abi.ColumnDesc), C.c_int,
+                                                    C.c_void_p, P(_abi.UnevenPlan)]
+        lib.adrt_engine_set_uneven_plan.argtypes = [C.c_void_p, P(_abi.UnevenPlan)]
+        lib.adrt_engine_get_uneven_plan.argtypes = [C.c_void_p, P(_abi.UnevenPlan)]
         lib.adrt_band_integrate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong,
                                             C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         lib.adrt_adjoint.argtypes = [C.c_void_p, P(_abi.BatchDesc), P(_abi.Inputs),

@@ -26,7 +26,8 @@ CUDA_CORE_LIB = os.path.join(PKG, "libadrt_b200_cudacore.so")
 CUDA_CORE_FLAGS = ["-DADRT_GEMM_MMA=0", "-DADRT_GJ_MMA=0", "-DADRT_PHASE_MMA=0"]
 
 SOURCES = ["adrt_engine.cu", "adrt_probe.cu", "adrt_noalloc.cu"]
-HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh"]
+HEADERS = ["adrt_types.cuh", "adrt_solver.cuh", "adrt_kernel.cuh", "adrt_adjoint.cuh",
+           "adrt_tpw.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

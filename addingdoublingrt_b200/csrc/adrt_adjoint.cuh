@@ -1493,7 +1493,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       AD.g_planck[wo + ul] = bB[l];
     }
   }
-  if (singular && t == 0) atomicOr(status, 1u);
+  if (singular && t == 0) atomicOr(status, status_bits(singular));
   X.sync();
 }
 

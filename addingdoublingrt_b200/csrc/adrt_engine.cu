@@ -18,6 +18,7 @@
 
 #include "../../include/adrt_b200.h"
 #include "adrt_adjoint.cuh"
+#include "adrt_tpw.cuh"
 
 using namespace adrt_dev;
 
@@ -184,6 +185,10 @@ struct adrt_engine {
   std::mutex hmu;  // one host-entry call at a time per engine
   std::mutex mu;
   int adjoint_mode = ADRT_ADJOINT_RECORD;
+  // uneven batches: warp mapping for every order, occupancy-limited grid,
+  // longest columns first (adrt_engine_autotune_uneven replaces it)
+  adrt_uneven_plan plan{{ADRT_MAPPING_WARP, ADRT_MAPPING_WARP, ADRT_MAPPING_WARP}, 0, 1,
+                        {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}}};
 };
 
 namespace {
@@ -463,6 +468,234 @@ int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   grid = std::min(grid, need_blocks);
   CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
   return k.launch(p, c0, grid, s);
+}
+
+// ------------------------------------------------------------- uneven batches
+// One column of an uneven launch: its description and the wavenumbers to
+// solve (all of them, or the autotuner's sample: the first W).
+struct UnevenColumn {
+  const adrt_column_desc* c;
+  int W;
+};
+
+int warp_blocks_per_sm_max() {
+  static int bps = -1;
+  if (bps < 0) {
+    const size_t smem = 4 * kMultiGroupBytes;
+    cudaFuncSetAttribute(solve_kernel_multi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, solve_kernel_multi<0>, 128, smem);
+    if (bps < 1) bps = 1;
+  }
+  return bps;
+}
+
+template <int NP>
+int tpw_blocks_per_sm() {
+  static int bps = -1;
+  if (bps < 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, tpw::solve_kernel_tpw<NP>, 128, 0);
+    if (bps < 1) bps = 1;
+  }
+  return bps;
+}
+
+// Thread-per-wavenumber work memory: every thread of the launch holds its
+// own records (about (L+1) x 3 NP^2 doubles, 0.97 MB at NP = 16, L = 150),
+// so the launch is capped by this budget (or the engine's workspace limit).
+constexpr size_t kThreadMappingBudget = size_t(16) << 30;
+
+size_t tpw_slot_bytes(int np, int lmax) {
+  const size_t d = np == 4 ? tpw::slot_doubles<4>(lmax)
+                   : np == 8 ? tpw::slot_doubles<8>(lmax) : tpw::slot_doubles<16>(lmax);
+  return d * sizeof(double);
+}
+
+long long tpw_slots(adrt_engine* e, int np, int lmax, long long ntasks) {
+  const int bps = np == 4 ? tpw_blocks_per_sm<4>() : np == 8 ? tpw_blocks_per_sm<8>()
+                                                             : tpw_blocks_per_sm<16>();
+  long long n = (long long)bps * e->num_sms * 128;
+  const size_t budget = e->max_ws ? e->max_ws : kThreadMappingBudget;
+  n = std::min<long long>(n, (long long)(budget / tpw_slot_bytes(np, lmax)));
+  return std::min<long long>(n, ntasks);
+}
+
+// Grow the engine's work buffer to `need` bytes (outside stream capture).
+int grow_scratch(adrt_engine* e, size_t need, cudaStreamCaptureStatus cap) {
+  if (need <= e->scratch_bytes) return ADRT_OK;
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(ADRT_ERR_WORKSPACE, "work buffer too small during stream capture");
+  CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(e->scratch);
+  e->scratch = nullptr;
+  e->scratch_bytes = 0;
+  if (cudaMalloc(&e->scratch, need) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "work buffer allocation of %zu B failed", need);
+  }
+  e->scratch_bytes = need;
+  return ADRT_OK;
+}
+
+// The uneven launch under `plan`, with e->mu held.  Columns are split into
+// the warp launch (N <= 16: every mixed column, and FP64 columns whose order
+// maps to warps), one thread-per-wavenumber launch per order (FP64 columns
+// whose order maps to threads) and the N = 32 launch; all run back to back on
+// the stream, each from its own work counter, over one column table.
+int uneven_locked(adrt_engine* e, std::vector<UnevenColumn>& cv, cudaStream_t s,
+                  const adrt_uneven_plan& plan) {
+  int rc;
+  if ((rc = set_device(e))) return rc;
+  e->last_stream = s;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  const int ncols = (int)cv.size();
+  for (auto& c : cv)
+    if ((rc = ensure_quad(e, c.c->desc.num_quadrature, c.c->desc.num_moments))) return rc;
+  // parts: 0 warp, 1..3 thread mapping at NP = 4, 8, 16, 4 the N = 32 kernel
+  std::vector<int> part[5];
+  int lmax[5] = {1, 1, 1, 1, 1};
+  int any_mixed_l = 0;
+  for (int i = 0; i < ncols; ++i) {
+    const adrt_batch_desc& d = cv[i].c->desc;
+    if (cv[i].W < 1) continue;
+    const int np = padded_order(d.num_quadrature);
+    const int oi = np == 4 ? 0 : np == 8 ? 1 : 2;
+    int k;
+    if (np == 32) {
+      k = 4;
+      any_mixed_l |= d.precision == ADRT_PRECISION_MIXED;
+    } else if (d.precision == ADRT_PRECISION_FP64 && plan.mapping[oi] == ADRT_MAPPING_THREAD) {
+      k = 1 + oi;
+    } else {
+      k = 0;
+    }
+    part[k].push_back(i);
+    lmax[k] = std::max(lmax[k], d.num_layers);
+  }
+  // longest columns first (cost ~ L NP^3 per wavenumber), so the persistent
+  // kernels' dynamic task queues end with short tasks
+  auto cost = [&](int i) {
+    const double np = padded_order(cv[i].c->desc.num_quadrature);
+    return (double)cv[i].c->desc.num_layers * np * np * np;
+  };
+  if (plan.cost_order)
+    for (auto& pv : part)
+      std::stable_sort(pv.begin(), pv.end(), [&](int a, int b) { return cost(a) > cost(b); });
+  int nused = 0;
+  for (auto& pv : part) nused += (int)pv.size();
+  if (nused == 0) return ADRT_OK;
+  if (e->d_cols_cap < (size_t)nused) {
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(ADRT_ERR_WORKSPACE, "column table too small during capture");
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->d_cols);
+    if (e->h_cols) cudaFreeHost(e->h_cols);
+    e->d_cols = nullptr;
+    e->h_cols = nullptr;
+    e->d_cols_cap = 0;
+    if (cudaMalloc(&e->d_cols, sizeof(ColumnDev) * nused) != cudaSuccess ||
+        cudaMallocHost(&e->h_cols, sizeof(ColumnDev) * nused) != cudaSuccess)
+      return fail(ADRT_ERR_OUT_OF_MEMORY, "column table allocation failed");
+    e->d_cols_cap = nused;
+    if (!e->cols_copied) CUDA_TRY(cudaEventCreateWithFlags(&e->cols_copied, cudaEventDisableTiming));
+  }
+  // the previous upload must have left the pinned staging before it is rewritten
+  if (cap == cudaStreamCaptureStatusNone && e->cols_copied) CUDA_TRY(cudaEventSynchronize(e->cols_copied));
+  long long totals[5] = {0, 0, 0, 0, 0};
+  int first[5];
+  int nt = 0;
+  for (int k = 0; k < 5; ++k) {
+    first[k] = nt;
+    for (int i : part[k]) {
+      const adrt_column_desc* c = cv[i].c;
+      ColumnDev col = make_column(e, &c->desc, &c->in, &c->out);
+      col.W = cv[i].W;
+      col.task_begin = totals[k];
+      totals[k] += cv[i].W;
+      e->h_cols[nt++] = col;
+    }
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_cols, e->h_cols, sizeof(ColumnDev) * nused, cudaMemcpyHostToDevice, s));
+  // (in a capture the copy runs at each replay, from the staging as it is
+  // then; recording the event there would leave it a captured event)
+  if (e->cols_copied && cap == cudaStreamCaptureStatusNone)
+    CUDA_TRY(cudaEventRecord(e->cols_copied, s));
+  // the warp launch: one wavenumber per warp, all orders <= 16, one launch
+  if (!part[0].empty()) {
+    const size_t smem = 4 * kMultiGroupBytes;
+    const int bmax = warp_blocks_per_sm_max();
+    const int bps = plan.warp_blocks_per_sm ? std::min(plan.warp_blocks_per_sm, bmax) : bmax;
+    const size_t sb = (SlotLayout<Geo<16, double>>::bytes(lmax[0]) + 255) & ~size_t(255);
+    long long blocks = (long long)bps * e->num_sms;
+    if (e->max_ws) {
+      blocks = std::min<long long>(blocks, (long long)(e->max_ws / (4 * sb)));
+      if (blocks < 1) return fail(ADRT_ERR_WORKSPACE, "workspace limit below one slot (%zu B)", sb);
+    }
+    if ((rc = grow_scratch(e, (size_t)blocks * 4 * sb, cap))) return rc;
+    blocks = std::min<long long>(blocks, (totals[0] + 3) / 4);
+    SolveParams p{};
+    p.cols = e->d_cols + first[0];
+    p.ncols = (int)part[0].size();
+    p.ntasks = totals[0];
+    p.counter = e->counter;
+    p.status = e->status;
+    p.scratch = e->scratch;
+    p.slot_bytes = sb;
+    p.nslots = (int)blocks * 4;
+    p.max_layers = lmax[0];
+    CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+    solve_kernel_multi<0><<<(int)blocks, 128, smem, s>>>(p);
+    CUDA_TRY(cudaGetLastError());
+  }
+  // the thread-per-wavenumber launches, one per order
+  for (int k = 1; k <= 3; ++k) {
+    if (part[k].empty()) continue;
+    const int np = k == 1 ? 4 : k == 2 ? 8 : 16;
+    const long long nslots = tpw_slots(e, np, lmax[k], totals[k]);
+    if (nslots < 1)
+      return fail(ADRT_ERR_WORKSPACE, "workspace below one thread-mapping slot (%zu B)",
+                  tpw_slot_bytes(np, lmax[k]));
+    if ((rc = grow_scratch(e, (size_t)nslots * tpw_slot_bytes(np, lmax[k]), cap))) return rc;
+    SolveParams p{};
+    p.cols = e->d_cols + first[k];
+    p.ncols = (int)part[k].size();
+    p.ntasks = totals[k];
+    p.counter = e->counter + 1 + k;
+    p.status = e->status;
+    p.scratch = e->scratch;
+    p.slot_bytes = tpw_slot_bytes(np, lmax[k]);
+    p.nslots = (int)nslots;
+    p.max_layers = lmax[k];
+    CUDA_TRY(cudaMemsetAsync(e->counter + 1 + k, 0, sizeof(unsigned long long), s));
+    const int grid = (int)((nslots + 127) / 128);
+    if (np == 4) tpw::solve_kernel_tpw<4><<<grid, 128, 0, s>>>(p);
+    else if (np == 8) tpw::solve_kernel_tpw<8><<<grid, 128, 0, s>>>(p);
+    else tpw::solve_kernel_tpw<16><<<grid, 128, 0, s>>>(p);
+    CUDA_TRY(cudaGetLastError());
+  }
+  // columns of N > 16: one launch of the N = 32 kernel (per-column precision)
+  if (!part[4].empty()) {
+    KernInfo k = pick(32, any_mixed_l ? ADRT_PRECISION_MIXED : ADRT_PRECISION_FP64);
+    int grid;
+    size_t sb;
+    if ((rc = ensure_scratch(e, k, lmax[4], &grid, &sb))) return rc;
+    SolveParams p{};
+    p.cols = e->d_cols + first[4];
+    p.ncols = (int)part[4].size();  // 1: the kernel takes the column from c0
+    p.ntasks = totals[4];
+    p.counter = e->counter + 1;  // its own work counter
+    p.status = e->status;
+    p.scratch = e->scratch;
+    p.slot_bytes = sb;
+    p.nslots = grid * k.groups;
+    p.max_layers = lmax[4];
+    grid = (int)std::min<long long>(grid, totals[4]);
+    CUDA_TRY(cudaMemsetAsync(e->counter + 1, 0, sizeof(unsigned long long), s));
+    ColumnDev c0 = e->h_cols[first[4]];
+    if ((rc = k.launch(p, c0, grid, s))) return rc;
+  }
+  return ADRT_OK;
 }
 
 }  // namespace
@@ -1024,137 +1257,148 @@ int adrt_solve_batch_uneven(adrt_engine* e, const adrt_column_desc* cols, int nc
                             void* stream_ptr) {
   if (!e || !cols || ncols < 1) return fail(ADRT_ERR_INVALID_ARGUMENT, "bad uneven-batch arguments");
   int rc;
-  int lmax_s = 0, lmax_l = 0, any_mixed_l = 0;
-  std::vector<int> small, large;
   for (int i = 0; i < ncols; ++i) {
     if ((rc = check_desc(&cols[i].desc))) return rc;
     if ((rc = check_inputs(&cols[i].desc, &cols[i].in))) return rc;
-    if (padded_order(cols[i].desc.num_quadrature) <= 16) {
-      small.push_back(i);
-      lmax_s = std::max(lmax_s, cols[i].desc.num_layers);
-    } else {
-      large.push_back(i);
-      lmax_l = std::max(lmax_l, cols[i].desc.num_layers);
-      any_mixed_l |= cols[i].desc.precision == ADRT_PRECISION_MIXED;
-    }
   }
-  // longest columns first (cost ~ L NP^3 per wavenumber), so the persistent
-  // kernel's dynamic task queue ends with short tasks
-  auto cost = [&](int i) {
-    const double np = padded_order(cols[i].desc.num_quadrature);
-    return (double)cols[i].desc.num_layers * np * np * np;
-  };
-  auto by_cost = [&](int a, int b) { return cost(a) > cost(b); };
-  std::stable_sort(small.begin(), small.end(), by_cost);
-  std::stable_sort(large.begin(), large.end(), by_cost);
+  std::lock_guard<std::mutex> lk(e->mu);
+  std::vector<UnevenColumn> cv(ncols);
+  for (int i = 0; i < ncols; ++i) cv[i] = UnevenColumn{&cols[i], cols[i].desc.num_wavenumbers};
+  return uneven_locked(e, cv, static_cast<cudaStream_t>(stream_ptr), e->plan);
+}
+
+int adrt_engine_set_uneven_plan(adrt_engine* e, const adrt_uneven_plan* plan) {
+  if (!e || !plan) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
+  for (int m : plan->mapping)
+    if (m != ADRT_MAPPING_WARP && m != ADRT_MAPPING_THREAD)
+      return fail(ADRT_ERR_INVALID_ARGUMENT, "unknown mapping %d", m);
+  if (plan->warp_blocks_per_sm < 0)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "warp_blocks_per_sm must be >= 0");
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->plan = *plan;
+  return ADRT_OK;
+}
+
+int adrt_engine_get_uneven_plan(const adrt_engine* e, adrt_uneven_plan* plan) {
+  if (!e || !plan) return fail(ADRT_ERR_INVALID_ARGUMENT, "null argument");
+  *plan = e->plan;
+  return ADRT_OK;
+}
+
+int adrt_engine_autotune_uneven(adrt_engine* e, const adrt_column_desc* cols, int ncols,
+                                void* stream_ptr, adrt_uneven_plan* out) {
+  if (!e || !cols || ncols < 1) return fail(ADRT_ERR_INVALID_ARGUMENT, "bad uneven-batch arguments");
+  int rc;
+  for (int i = 0; i < ncols; ++i) {
+    if ((rc = check_desc(&cols[i].desc))) return rc;
+    if ((rc = check_inputs(&cols[i].desc, &cols[i].in))) return rc;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
   std::lock_guard<std::mutex> lk(e->mu);
   if ((rc = set_device(e))) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);
-  e->last_stream = s;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
-  for (int i = 0; i < ncols; ++i)
-    if ((rc = ensure_quad(e, cols[i].desc.num_quadrature, cols[i].desc.num_moments))) return rc;
-  if (e->d_cols_cap < (size_t)ncols) {
-    if (cap != cudaStreamCaptureStatusNone)
-      return fail(ADRT_ERR_WORKSPACE, "column table too small during capture");
-    CUDA_TRY(cudaDeviceSynchronize());
-    cudaFree(e->d_cols);
-    if (e->h_cols) cudaFreeHost(e->h_cols);
-    e->d_cols = nullptr;
-    e->h_cols = nullptr;
-    e->d_cols_cap = 0;
-    if (cudaMalloc(&e->d_cols, sizeof(ColumnDev) * ncols) != cudaSuccess ||
-        cudaMallocHost(&e->h_cols, sizeof(ColumnDev) * ncols) != cudaSuccess)
-      return fail(ADRT_ERR_OUT_OF_MEMORY, "column table allocation failed");
-    e->d_cols_cap = ncols;
-    if (!e->cols_copied) CUDA_TRY(cudaEventCreateWithFlags(&e->cols_copied, cudaEventDisableTiming));
-  }
-  // the previous upload must have left the pinned staging before it is rewritten
-  if (cap == cudaStreamCaptureStatusNone && e->cols_copied) CUDA_TRY(cudaEventSynchronize(e->cols_copied));
-  long long totals[2] = {0, 0};
-  int nsm = 0;
-  for (int part = 0; part < 2; ++part) {
-    const std::vector<int>& ids = part == 0 ? small : large;
-    for (int i : ids) {
-      ColumnDev c = make_column(e, &cols[i].desc, &cols[i].in, &cols[i].out);
-      c.task_begin = totals[part];
-      totals[part] += cols[i].desc.num_wavenumbers;
-      e->h_cols[nsm++] = c;
-    }
-  }
-  CUDA_TRY(cudaMemcpyAsync(e->d_cols, e->h_cols, sizeof(ColumnDev) * ncols, cudaMemcpyHostToDevice, s));
-  // (in a capture the copy runs at each replay, from the staging as it is
-  // then; recording the event there would leave it a captured event)
-  if (e->cols_copied && cap == cudaStreamCaptureStatusNone)
-    CUDA_TRY(cudaEventRecord(e->cols_copied, s));
-  // columns of N <= 16: one launch of the multi-order kernel
-  if (!small.empty()) {
-    const size_t smem = 4 * kMultiGroupBytes;
-    static int bps = -1;
-    if (bps < 0) {
-      cudaFuncSetAttribute(solve_kernel_multi<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, solve_kernel_multi<0>, 128, smem);
-      if (bps < 1) bps = 1;
-    }
-    const size_t sb = (SlotLayout<Geo<16, double>>::bytes(lmax_s) + 255) & ~size_t(255);
-    int blocks = bps * e->num_sms;
-    size_t need = (size_t)blocks * 4 * sb;
-    if (e->max_ws && need > e->max_ws) {
-      blocks = (int)(e->max_ws / (4 * sb));
-      if (blocks < 1) return fail(ADRT_ERR_WORKSPACE, "workspace limit below one slot (%zu B)", sb);
-      need = (size_t)blocks * 4 * sb;
-    }
-    if (need > e->scratch_bytes) {
-      if (cap != cudaStreamCaptureStatusNone)
-        return fail(ADRT_ERR_WORKSPACE, "work buffer too small during stream capture");
-      CUDA_TRY(cudaDeviceSynchronize());
-      cudaFree(e->scratch);
-      e->scratch = nullptr;
-      e->scratch_bytes = 0;
-      if (cudaMalloc(&e->scratch, need) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(ADRT_ERR_OUT_OF_MEMORY, "work buffer allocation of %zu B failed", need);
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "the autotuner times launches: not during a capture");
+  adrt_uneven_plan plan = e->plan;
+  for (auto& r : plan.ns_per_wavenumber) r[0] = r[1] = 0.0;
+  cudaEvent_t ev0, ev1;
+  CUDA_TRY(cudaEventCreate(&ev0));
+  CUDA_TRY(cudaEventCreate(&ev1));
+  // ns per wavenumber of `cv` under `p` (one untimed run, then one timed)
+  auto time_plan = [&](std::vector<UnevenColumn>& cv, const adrt_uneven_plan& p,
+                       double* ns) -> int {
+    long long n = 0;
+    for (auto& c : cv) n += c.W;
+    if (n == 0) return ADRT_OK;
+    int r = uneven_locked(e, cv, s, p);
+    if (r) return r;
+    CUDA_TRY(cudaEventRecord(ev0, s));
+    if ((r = uneven_locked(e, cv, s, p))) return r;
+    CUDA_TRY(cudaEventRecord(ev1, s));
+    CUDA_TRY(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+    *ns = ms * 1e6 / (double)n;
+    return ADRT_OK;
+  };
+  // 1. per padded order: the two mappings on a sample of that order's FP64
+  //    wavenumbers, large enough for several waves of either launch
+  const int orders[3] = {4, 8, 16};
+  for (int oi = 0; oi < 3 && !rc; ++oi) {
+    std::vector<int> ids;
+    int lmax = 1;
+    for (int i = 0; i < ncols; ++i)
+      if (padded_order(cols[i].desc.num_quadrature) == orders[oi] &&
+          cols[i].desc.precision == ADRT_PRECISION_FP64) {
+        ids.push_back(i);
+        lmax = std::max(lmax, cols[i].desc.num_layers);
       }
-      e->scratch_bytes = need;
+    if (ids.empty()) continue;
+    const long long warp_slots = (long long)warp_blocks_per_sm_max() * e->num_sms * 4;
+    const long long thread_slots = tpw_slots(e, orders[oi], lmax, 1ll << 40);
+    const long long want = 3 * std::max(warp_slots, thread_slots);
+    std::vector<UnevenColumn> cv;
+    long long taken = 0;
+    // the same share of every column (columns differ in L and W)
+    long long total = 0;
+    for (int i : ids) total += cols[i].desc.num_wavenumbers;
+    const double frac = std::min(1.0, (double)want / (double)total);
+    for (int i : ids) {
+      const int w = std::max(1, (int)std::ceil(frac * cols[i].desc.num_wavenumbers));
+      cv.push_back(UnevenColumn{&cols[i], std::min(w, cols[i].desc.num_wavenumbers)});
+      taken += cv.back().W;
     }
-    blocks = std::min<long long>(blocks, (long long)(e->scratch_bytes / (4 * sb)));
-    blocks = (int)std::min<long long>(blocks, (totals[0] + 3) / 4);
-    SolveParams p{};
-    p.cols = e->d_cols;
-    p.ncols = (int)small.size();
-    p.ntasks = totals[0];
-    p.counter = e->counter;
-    p.status = e->status;
-    p.scratch = e->scratch;
-    p.slot_bytes = sb;
-    p.nslots = blocks * 4;
-    p.max_layers = lmax_s;
-    CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
-    solve_kernel_multi<0><<<blocks, 128, smem, s>>>(p);
-    CUDA_TRY(cudaGetLastError());
+    (void)taken;
+    adrt_uneven_plan p = plan;
+    double ns[2] = {0.0, 0.0};
+    for (int m = 0; m < 2 && !rc; ++m) {
+      p.mapping[oi] = m;
+      rc = time_plan(cv, p, &ns[m]);
+    }
+    if (rc) break;
+    plan.ns_per_wavenumber[oi][0] = ns[0];
+    plan.ns_per_wavenumber[oi][1] = ns[1];
+    plan.mapping[oi] = (ns[1] > 0.0 && ns[1] < ns[0]) ? ADRT_MAPPING_THREAD : ADRT_MAPPING_WARP;
   }
-  // columns of N > 16: one launch of the N = 32 kernel (per-column precision)
-  if (!large.empty()) {
-    KernInfo k = pick(32, any_mixed_l ? ADRT_PRECISION_MIXED : ADRT_PRECISION_FP64);
-    int grid;
-    size_t sb;
-    if ((rc = ensure_scratch(e, k, lmax_l, &grid, &sb))) return rc;
-    SolveParams p{};
-    p.cols = e->d_cols + small.size();
-    p.ncols = (int)large.size();  // 1: the kernel takes the column from c0
-    p.ntasks = totals[1];
-    p.counter = e->counter + 1;  // its own work counter
-    p.status = e->status;
-    p.scratch = e->scratch;
-    p.slot_bytes = sb;
-    p.nslots = grid * k.groups;
-    p.max_layers = lmax_l;
-    grid = (int)std::min<long long>(grid, totals[1]);
-    CUDA_TRY(cudaMemsetAsync(e->counter + 1, 0, sizeof(unsigned long long), s));
-    ColumnDev c0 = make_column(e, &cols[large[0]].desc, &cols[large[0]].in, &cols[large[0]].out);
-    if ((rc = k.launch(p, c0, grid, s))) return rc;
+  // 2. the warp launch's grid cap, on a sample of everything it runs
+  if (!rc) {
+    std::vector<UnevenColumn> cv;
+    long long total = 0;
+    for (int i = 0; i < ncols; ++i) {
+      const int np = padded_order(cols[i].desc.num_quadrature);
+      const bool warp = np <= 16 && (cols[i].desc.precision != ADRT_PRECISION_FP64 ||
+                                     plan.mapping[np == 4 ? 0 : np == 8 ? 1 : 2] ==
+                                         ADRT_MAPPING_WARP);
+      if (warp) total += cols[i].desc.num_wavenumbers;
+    }
+    const long long want = 3ll * warp_blocks_per_sm_max() * e->num_sms * 4;
+    const double frac = total ? std::min(1.0, (double)want / (double)total) : 0.0;
+    for (int i = 0; i < ncols && total; ++i) {
+      const int np = padded_order(cols[i].desc.num_quadrature);
+      if (np > 16) continue;
+      const int w = std::max(1, (int)std::ceil(frac * cols[i].desc.num_wavenumbers));
+      cv.push_back(UnevenColumn{&cols[i], std::min(w, cols[i].desc.num_wavenumbers)});
+    }
+    double best = 0.0;
+    int best_b = 0;
+    for (int b = warp_blocks_per_sm_max(); b >= 1 && !rc && !cv.empty(); --b) {
+      adrt_uneven_plan p = plan;
+      p.warp_blocks_per_sm = b;
+      double ns = 0.0;
+      rc = time_plan(cv, p, &ns);
+      if (!rc && (best_b == 0 || ns < best)) {
+        best = ns;
+        best_b = b;
+      }
+    }
+    plan.warp_blocks_per_sm = (best_b == warp_blocks_per_sm_max()) ? 0 : best_b;
   }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (rc) return rc;
+  e->plan = plan;
+  if (out) *out = plan;
   return ADRT_OK;
 }
 

@@ -451,6 +451,11 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   const unsigned oR = X.mo(0), oA = X.mo(3), oTG = X.mo(4);
   const unsigned oT[2] = {X.mo(1), X.mo(2)};
   constexpr bool taping = TAPE;
+  // An unstable first-order start (tau0 beyond half the smallest quadrature
+  // cosine: T = I - tau0 Gpp with large negative diagonal entries) leaves
+  // I - R^2 outside the diagonally dominant class the pivot-free solve is
+  // argued for; its solves use the reference's partial pivoting.
+  const int pivot = tau0 > 0.5 * mu[0];
   using GC = Geo<NP, Real>;  // record order
   using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);
@@ -531,11 +536,12 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
       // (I - R^2)^{-1} into the free T buffer and the record, then TG = T (I - R^2)^{-1}
       Real* tk = tape + (size_t)k * Tp::STEP;
       *singular |= op_gj<Gm, GC, true>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t,
-                                       X.bar, oT[cur ^ 1], tk + Tp::OFF_AI);
+                                       X.bar, oT[cur ^ 1], tk + Tp::OFF_AI, pivot);
       X.sync();
       op_gemm<Gm, true>(oTc, oT[cur ^ 1], kNoMat, 0, kNoMat, oTG, t);
     } else {
-      *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar);  // TG = T (I-R^2)^-1
+      *singular |= op_gj<Gm>(oA, oTc, kNoMat, oTG, X.gjo(), X.redo(), t, X.bar, kNoMat, nullptr,
+                             pivot);  // TG = T (I-R^2)^-1
     }
     X.sync();
     if constexpr (taping) {  // the adjoint's record of this step
@@ -1018,15 +1024,22 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
   else
     tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp,
                            Ppm, singular, src64);
+  (void)tF;
   const Ctx<GmF> XF(goff, tbF, t_, bar);
   const Ctx<GmD> XD(goff, tbD, t_, bar);
   XD.sync();
   const Tile<GmF> tf(XF.t);
   const Tile<GmD> td(XD.t);
+  // T = Lambda + T' is widened as its two parts: the diffuse T' (FP32, the
+  // buffer 6 + (nn & 1) of both FP32 doublings) plus the direct diagonal
+  // Lambda kept in FP64, so that 1 - T of a thin layer keeps FP64 accuracy
+  // in the adding (T rounded to FP32 as a whole loses it: 6e-8 of 1 per layer)
+  const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
+  const double* lam = XF.DV(D_LAM0 + (nn & 1));
   float Rf[TR][TC], Tf[TR][TC];
   if (tf.valid()) {
     tf.load_rm(Rf, XF.m(0));
-    tf.load_rm(Tf, XF.m(tF));
+    tf.load_rm(Tf, XF.m(6 + (nn & 1)));
   }
   XD.sync();  // the FP64 buffers overlay the FP32 region
   if (td.valid()) {
@@ -1036,7 +1049,7 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
 #pragma unroll
       for (int b = 0; b < TC; ++b) {
         Rd[a][b] = Rf[a][b];
-        Td[a][b] = Tf[a][b];
+        Td[a][b] = (double)Tf[a][b] + ((td.row(a) == td.col(b)) ? lam[td.row(a)] : 0.0);
       }
     td.store_rm(Rd, XD.m(0));
     td.store_rm(Td, XD.m(1));
@@ -1572,7 +1585,7 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
         emit_interface<Gm>(X, C, w, l + 1, N, solar, F0, mu0, lv, status);
     }
   }
-  if (singular && t == 0) atomicOr(status, 1u);
+  if (singular && t == 0) atomicOr(status, status_bits(singular));
   X.sync();
 }
 

@@ -513,6 +513,20 @@ struct UseGjMMA {
                                 ((2 * NP / 8) * (NP / 8)) % NW == 0;
 };
 
+// The pivot-free solve's safety net: a pivot below kGjMinPivot in magnitude
+// (or not finite) means the matrix is not the diagonally dominant one the
+// argument above covers; gj_mma then returns kGjWeakPivot and op_gj solves
+// again with partial pivoting.  Every such matrix here is I minus a product
+// of reflection matrices with O(1) entries, so the bound is absolute.
+constexpr double kGjMinPivot = 1e-10;
+constexpr int kGjWeakPivot = 2;  // op_gj result bit: solved again with pivoting
+
+// Device status bits of op_gj results (adrt_device_flag): an exactly zero
+// pivot (1), a pivoted re-solve (8).
+__device__ __forceinline__ unsigned status_bits(int gj) {
+  return ((gj & 1) ? 1u : 0u) | ((gj & kGjWeakPivot) ? 8u : 0u);
+}
+
 template <class Gm, class GO = Gm, bool OUTG = false>
 __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, const double* bvec,
                                       double* out_cm, double* out_rm, double* lbuf, double* rbuf,
@@ -540,7 +554,7 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
     acc[u][0] = v.x;
     acc[u][1] = v.y;
   }
-  int singular = 0;
+  int singular = 0, weak = 0;
 #pragma unroll
   for (int j = 0; j < NP / 4; ++j) {
     const int pt = j >> 1, half = j & 1;  // tile row/column holding the panel, and which half
@@ -583,6 +597,7 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
       for (int s = 0; s < 4; ++s) {
         const double piv = P[s][s];
         singular |= (piv == 0.0);
+        weak |= !(fabs(piv) >= kGjMinPivot);  // tiny or non-finite
         const double inv = recip(piv);
         const double fx = x[s] * inv;
 #pragma unroll
@@ -640,7 +655,7 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
       }
     }
   }
-  return singular;
+  return singular | (weak ? kGjWeakPivot : 0);
 }
 
 // X = B A^{-1} by Gauss-Jordan column elimination, with column pivoting on
@@ -650,13 +665,15 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
 // the right-hand side is the single row `bvec` (a vector solve), when it is
 // kIdentity the result is A^{-1}.  The result is written column-major to
 // out_cm and/or row-major to out_rm.  FP64 orders >= 8 take gj_mma (above).
-// Returns nonzero if a pivot was exactly 0.
+// Returns bit 0 if a pivot was exactly 0, and kGjWeakPivot when the
+// tensor-core solve met a weak pivot and the pivoted elimination was used
+// instead; `pivot` requests the pivoted elimination from the start.
 // OUTG: the result also into HBM (out_g), in the tile order of GO.
 template <class Gm, class GO = Gm, bool OUTG = false>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
                                   int bar, unsigned orm_off = 0xffffffffu,
-                                  typename Gm::Real* out_g = nullptr) {
+                                  typename Gm::Real* out_g = nullptr, int pivot = 0) {
   using Real = typename Gm::Real;
   const Real* A_rm = sp<Real>(a_off);
   const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
@@ -666,13 +683,21 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
   unsigned* red = sp<unsigned>(red_off);
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP, DIM = Gm::DIM;
   constexpr int G = Gm::G;
+  int fell_back = 0;
   if constexpr (UseGjMMA<Gm>::value) {
     static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
-    Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
-    Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
-    // scratch: the output buffer, or the one matrix buffer the call names
-    Real* lbuf = o_cm ? o_cm : out_rm;
-    return gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
+    if (!pivot) {
+      Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+      Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
+      // scratch: the output buffer, or the one matrix buffer the call names
+      Real* lbuf = o_cm ? o_cm : out_rm;
+      const int r = gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
+      if (!(r & kGjWeakPivot)) return r;
+      // A and B are intact: solve again below with partial pivoting, once
+      // every thread is done with the scratch
+      fell_back = kGjWeakPivot;
+      gsync<G>(bar);
+    }
   }
   const Tile<Gm> tl(t);
   const bool tv = tl.valid();
@@ -805,7 +830,7 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
       }
     }
   }
-  return singular;
+  return singular | fell_back;
 }
 
 // ============================================================== FP32 on the tensor cores

@@ -153,8 +153,7 @@ class Engine:
                                                 self._dev(out), s))
         return out
 
-    def solve_uneven(self, columns: list, stream=None) -> None:
-        """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
+    def _columns(self, columns: list):
         arr = (_abi.ColumnDesc * len(columns))()
         for i, (desc, di, do) in enumerate(columns):
             self._sizes(desc, [("in", di), ("out", do)])
@@ -163,6 +162,31 @@ class Engine:
                 setattr(arr[i].inp, f, self._dev(di.get(f)))
             for f in _abi.OUTPUT_FIELDS:
                 setattr(arr[i].out, f, self._dev(do.get(f)))
+        return arr
+
+    def autotune_uneven(self, columns: list, stream=None) -> _abi.UnevenPlan:
+        """adrt_engine_autotune_uneven: time both mappings per order on samples of
+        `columns` and keep the faster (the engine's plan from then on)."""
+        arr = self._columns(columns)
+        plan = _abi.UnevenPlan()
+        s = None
+        if stream is not None:
+            s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        _lib.check(self.lib.adrt_engine_autotune_uneven(self.handle, arr, len(columns), s,
+                                                        C.byref(plan)))
+        return plan
+
+    def uneven_plan(self) -> _abi.UnevenPlan:
+        plan = _abi.UnevenPlan()
+        _lib.check(self.lib.adrt_engine_get_uneven_plan(self.handle, C.byref(plan)))
+        return plan
+
+    def set_uneven_plan(self, plan: _abi.UnevenPlan) -> None:
+        _lib.check(self.lib.adrt_engine_set_uneven_plan(self.handle, C.byref(plan)))
+
+    def solve_uneven(self, columns: list, stream=None) -> None:
+        """adrt_solve_batch_uneven: columns = [(desc, dev_inputs, dev_outputs), ...]."""
+        arr = self._columns(columns)
         s = None
         if stream is not None:
             s = C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))

@@ -12,7 +12,8 @@ scheme (first-order thin-layer start, per-layer doubling counts, delta-M
 scaled beam), so results agree with adrt::solve; the solve runs on the B200
 engine in FP64 (or the mixed form); and gradients come from the engine's
 hand-written adjoint (adrt_adjoint) through a torch.autograd.Function, not
-from automatic differentiation of the forward.  Tensors are moved to the
+from automatic differentiation of the forward.  The adjoint is that of the
+FP64 form, so a mixed-form solve whose inputs require gradients is refused.  Tensors are moved to the
 current CUDA device and computed in float64; gradients are returned in the
 inputs' dtypes.
 """
@@ -115,5 +116,11 @@ def solve_batch(config: BatchConfig, delta_tau, ssa, phase_moments, planck_level
     """(flux_up_toa, flux_down_boa) of every wavenumber; differentiable in all four
     array arguments (src_jax/batch_solver.py:501-574)."""
     as_t = lambda x: x if torch.is_tensor(x) else torch.as_tensor(x, dtype=torch.float64)
-    return _SolveBatch.apply(config, as_t(delta_tau), as_t(ssa), as_t(phase_moments),
-                             as_t(planck_levels))
+    args = [as_t(delta_tau), as_t(ssa), as_t(phase_moments), as_t(planck_levels)]
+    if config.precision == "mixed" and torch.is_grad_enabled() and any(
+            a.requires_grad for a in args):
+        # the adjoint differentiates the FP64 form; the mixed form's gradients
+        # would belong to a different forward
+        raise ValueError("gradients are available for precision='fp64' only; solve the mixed "
+                         "form under torch.no_grad() or with inputs that do not require grad")
+    return _SolveBatch.apply(config, *args)

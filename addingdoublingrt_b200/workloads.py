@@ -283,6 +283,80 @@ def config4_columns(ncols=4096, seed=4, max_total=None):
     return cols
 
 
+def config4_shapes(ncols=4096, seed=4):
+    """The column shapes of config 4 (L, N, W, source type per column), drawn as
+    config4_columns draws them."""
+    rng = np.random.default_rng(seed)
+    shapes = []
+    for _ in range(ncols):
+        L = int(rng.integers(20, 151))
+        N = int(rng.choice([4, 8, 16]))
+        W = int(np.floor(np.exp(rng.uniform(np.log(256.0), np.log(8192.0)))))
+        src = int(rng.integers(0, 3))  # 0 solar, 1 thermal, 2 both
+        shapes.append((L, N, W, src))
+    return shapes
+
+
+def config4_device(ncols=4096, seed=4, precision=_abi.PRECISION_MIXED, device="cuda",
+                   fraction=1.0):
+    """Config 4 generated on the device (the full batch, about 9.3e6
+    wavenumber-columns and 40 GB of inputs and outputs, is too large to build
+    on the host): the column shapes of config4_columns, per-wavenumber values
+    from a seeded torch generator with config 4's distributions.  `fraction`
+    keeps the first ceil(fraction W) wavenumbers of every column.  Returns
+    [(desc, device inputs, device outputs)] for Engine.solve_uneven."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    f64 = dict(dtype=torch.float64, device=device)
+
+    def U(lo, hi, *shape):
+        return lo + (hi - lo) * torch.rand(*shape, generator=g, **f64)
+
+    cols = []
+    crng = np.random.default_rng(seed + 1000)
+    for L, N, W, src in config4_shapes(ncols, seed):
+        W = max(1, int(np.ceil(fraction * W)))
+        M = 2 * N
+        thermal, solar = src in (1, 2), src in (0, 2)
+        d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
+                           moment_layout=_abi.MOMENTS_PER_WAVENUMBER, precision=precision,
+                           use_thermal_emission=int(thermal), use_delta_m=1,
+                           surface_temperature=300.0 if thermal else -1.0,
+                           solar_flux=1.0 if solar else 0.0)
+        m = torch.arange(M, **f64)
+        f, g1, g2 = U(0.7, 0.95, W, 1), U(0.5, 0.9, W, 1), U(-0.5, 0.0, W, 1)
+        ins = {"delta_tau": (10.0 ** U(-4.0, 1.0, W * L)).contiguous(),
+               "single_scat_albedo": U(0.0, 0.99, W * L),
+               "phase_moments": (f * g1 ** m + (1.0 - f) * g2 ** m).reshape(-1).contiguous(),
+               "surface_albedo": U(0.0, 0.3, W), "solar_mu": U(0.1, 1.0, W)}
+        if thermal:
+            ins["temperature"] = torch.as_tensor(level_temperatures(crng, L), **f64)
+            lo, hi = _band(W)
+            ins["wavenumber_low"] = torch.as_tensor(lo, **f64)
+            ins["wavenumber_high"] = torch.as_tensor(hi, **f64)
+        outs = {k: torch.zeros(W * (L + 1), **f64) for k in _abi.INTERFACE_OUTPUTS}
+        cols.append((d, ins, outs))
+    return cols
+
+
+def column_to_host(desc, ins, w) -> Batch:
+    """Wavenumber w of a device column as a host batch of one (oracle checks)."""
+    d = _abi.BatchDesc.from_buffer_copy(desc)
+    d.num_wavenumbers = 1
+    W, L, M = desc.num_wavenumbers, desc.num_layers, desc.num_moments
+    b = Batch(d)
+    for k, v in ins.items():
+        if k in ("delta_tau", "single_scat_albedo"):
+            b.set(k, v[w * L:(w + 1) * L].cpu().numpy().reshape(1, L))
+        elif k == "phase_moments":
+            b.set(k, v[w * M:(w + 1) * M].cpu().numpy().reshape(1, M))
+        elif k == "temperature":
+            b.set(k, v.cpu().numpy())
+        else:
+            b.set(k, v[w:w + 1].cpu().numpy())
+    return b
+
+
 def random_small(seed, N=None, L=None, W=None, **flags) -> Batch:
     """Small randomized batch exercising every option (parity tests)."""
     rng = np.random.default_rng(seed)

@@ -49,16 +49,19 @@ def parse():
     p.add_argument("--adjoint-wavenumbers", type=int, default=10_000,
                    help="wavenumbers of the config-5 adjoint timing")
     p.add_argument("--workload", default="config2",
-                   choices=["config2", "config4", "adjoint", "band"],
+                   choices=["config2", "config4", "adjoint", "band", "table"],
                    help="config2: the headline line; config4: uneven batch; adjoint: config 5; "
                         "band: band integration of a spectrum (--wavenumbers x 1000)")
     p.add_argument("--no-adjoint", action="store_true",
                    help="skip the adjoint/forward timing of the headline line")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-entry (e2e) timing")
+    p.add_argument("--no-config4", action="store_true",
+                   help="skip the full config-4 uneven batch of the headline line")
     p.add_argument("--no-cuda-core", action="store_true",
                    help="skip the CUDA-core FP64 form (the mixed form's denominator)")
     p.add_argument("--no-reference-gpu", action="store_true",
-                   help="skip the reference's own GPU solver (oracle/_ref/libadrt_ref_gpu.so)")
+                   help="reference arm: skip the reference's own GPU solver "
+                        "(oracle/_ref/libadrt_ref_gpu.so)")
     return p.parse_args()
 
 
@@ -180,6 +183,14 @@ def run_reference(args):
         "e2e": {"value": rate, "unit": "wavenumber-solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_gpu and args.gpus == 1:
+        try:
+            line["reference_gpu"] = reference_gpu(workloads.config2_scalar(W=args.wavenumbers))
+            c1 = reference_gpu(workloads.config1(), steps=10, warmup=2)
+            c1["workload"] = "config1 (W=1000 x 20 layers, N=8: the reference's solveKernel<8>)"
+            line["reference_gpu_config1"] = c1
+        except Exception as ex:  # the CPU line stands on its own
+            line["reference_gpu"] = {"unavailable": str(ex)[:200]}
     print(json.dumps(line), flush=True)
 
 
@@ -222,45 +233,182 @@ def time_adjoint(eng, W=10_000, reps=3, mode=_abi.ADJOINT_RECORD):
     return statistics.median(fw), statistics.median(ad)
 
 
-def run_config4(args, eng):
-    """Uneven batch (config 4 columns: L ~ U{20..150}, N in {4, 8, 16}, W log-uniform
-    256..8192, solar / thermal / both, mixed precision), the first columns up to
-    --wavenumbers wavenumber-columns: one launch of the persistent multi-order
-    kernel against one launch per column (the reference's pattern of a
-    solveBatch call per column)."""
+def _time_uneven(eng, cols, reps=1, warmup=1):
     import torch
-    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
-    cols = workloads.config4_columns(ncols=4096, seed=4, max_total=args.wavenumbers)
-    dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in cols]
-    total = sum(c.W for c in cols)
-    for _ in range(args.warmup):
-        eng.solve_uneven(dev)
-    torch.cuda.synchronize()
+    for _ in range(warmup):
+        eng.solve_uneven(cols)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        eng.solve_uneven(dev)
-    e1.record()
-    torch.cuda.synchronize()
-    one = e0.elapsed_time(e1) / args.steps
-    for d, di, do in dev:
-        eng.solve_device(d, di, do)
     torch.cuda.synchronize()
     e0.record()
-    for d, di, do in dev:
-        eng.solve_device(d, di, do)
+    for _ in range(reps):
+        eng.solve_uneven(cols)
     e1.record()
     torch.cuda.synchronize()
-    per_col = e0.elapsed_time(e1)
-    line = {"metric": "wavenumber-solves/s, uneven batch (config 4)", "value": total / (one * 1e-3),
-            "unit": "wavenumber-solves/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": one, "higher_is_better": True,
-            "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"config4: first {len(cols)} columns, {total} wavenumber-"
-                                   "columns, N in {4,8,16}, L 20..150, mixed precision"},
-            "one_launch_ms": one, "launch_per_column_ms": per_col,
-            "speedup_vs_launch_per_column": per_col / one, "status": eng.read_status()}
-    print(json.dumps(line), flush=True)
+    return e0.elapsed_time(e1) / reps
+
+
+def _prefix(cols, fraction):
+    """Every column's first ceil(fraction W) wavenumbers (views of the same tensors)."""
+    out = []
+    for d, ins, outs in cols:
+        W, L, M = d.num_wavenumbers, d.num_layers, d.num_moments
+        w = max(1, int(np.ceil(fraction * W)))
+        dd = _abi.BatchDesc.from_buffer_copy(d)
+        dd.num_wavenumbers = w
+        per = {"delta_tau": L, "single_scat_albedo": L, "phase_moments": M}
+        ii = {k: (v if k == "temperature" else v[:w * per.get(k, 1)]) for k, v in ins.items()}
+        oo = {k: v[:w * (L + 1)] for k, v in outs.items()}
+        out.append((dd, ii, oo))
+    return out
+
+
+def run_config4(args, eng, line=True):
+    """Config 4 in full: 4096 columns, L ~ U{20..150}, N in {4, 8, 16}, W log-uniform
+    256..8192 (9.37e6 wavenumber-columns, generated on the device), solar /
+    thermal / both.  The uneven plan is autotuned on the FP64 batch (mapping per
+    order, warp-launch grid), the whole batch is solved in FP64 under it, and on
+    a 5 % prefix of every column the autotuned plan is compared with the fixed
+    thread-per-wavenumber mapping (the reference's solveKernel mapping) and with
+    the warp mapping alone; the mixed form runs on the same prefix.  One
+    wavenumber per column is checked against the oracle."""
+    import torch
+    from oracle import oracle
+    t0 = time.perf_counter()
+    cols = workloads.config4_device(ncols=4096, seed=4, precision=_abi.PRECISION_FP64)
+    gen_s = time.perf_counter() - t0
+    total = sum(d.num_wavenumbers for d, _, _ in cols)
+    saved = _abi.UnevenPlan.from_buffer_copy(eng.uneven_plan())
+    t0 = time.perf_counter()
+    plan = eng.autotune_uneven(cols)
+    tune_s = time.perf_counter() - t0
+    full_ms = _time_uneven(eng, cols, reps=1, warmup=1)
+    status = eng.read_status()
+    # one wavenumber per column against the oracle (FP64, autotuned plan)
+    import concurrent.futures as cf
+    checks = []
+    for d, ins, outs in cols:
+        w = d.num_wavenumbers // 2
+        L = d.num_layers
+        got = {k: outs[k][w * (L + 1):(w + 1) * (L + 1)].cpu().numpy()
+               for k in ("flux_up", "flux_down", "mean_intensity")}
+        checks.append((workloads.column_to_host(d, ins, w), got))
+
+    def check(item):
+        b, got = item
+        ref = oracle.solve_oracle(b, 1, which=_abi.INTERFACE_OUTPUTS)
+        return max(oracle.norm_error(got[k], ref[k], b.L + 1) for k in got)
+
+    with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        err = max(ex.map(check, checks))
+    sub = _prefix(cols, 0.05)
+    nsub = sum(d.num_wavenumbers for d, _, _ in sub)
+    tuned_ms = _time_uneven(eng, sub)
+    fixed = _abi.UnevenPlan.from_buffer_copy(plan)
+    for i in range(3):
+        fixed.mapping[i] = _abi.MAPPING_THREAD
+    fixed.warp_blocks_per_sm = 0
+    eng.set_uneven_plan(fixed)
+    thread_ms = _time_uneven(eng, sub)
+    warp = _abi.UnevenPlan.from_buffer_copy(plan)
+    for i in range(3):
+        warp.mapping[i] = _abi.MAPPING_WARP
+    warp.warp_blocks_per_sm = 0
+    eng.set_uneven_plan(warp)
+    warp_ms = _time_uneven(eng, sub)
+    eng.set_uneven_plan(plan)
+    for d, _, _ in sub:
+        d.precision = _abi.PRECISION_MIXED
+    mixed_ms = _time_uneven(eng, sub)
+    eng.set_uneven_plan(saved)
+    res = {
+        "metric": "wavenumber-solves/s, uneven batch (config 4)", "value": total / (full_ms * 1e-3),
+        "unit": "wavenumber-solves/s", "ms_per_step": full_ms, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic (generated on the device)",
+        "config": {"workload": f"config4: 4096 columns, {total} wavenumber-columns, N in "
+                               "{4,8,16}, L 20..150, FP64, autotuned plan"},
+        "plan": plan.as_dict(), "autotune_s": tune_s, "generate_s": gen_s,
+        "prefix_5pct": {"wavenumbers": nsub,
+                        "autotuned_solves_per_s": nsub / (tuned_ms * 1e-3),
+                        "thread_per_wavenumber_solves_per_s": nsub / (thread_ms * 1e-3),
+                        "warp_per_wavenumber_solves_per_s": nsub / (warp_ms * 1e-3),
+                        "autotuned_over_thread_per_wavenumber": thread_ms / tuned_ms,
+                        "mixed_solves_per_s": nsub / (mixed_ms * 1e-3)},
+        "oracle_max_normalized_error_one_wavenumber_per_column": err,
+        "status": status}
+    if line:
+        print(json.dumps(res), flush=True)
+    return res
+
+
+def run_table(args, eng):
+    """One line per configuration (1, 2, 3, 5) with the figures of the results
+    table: FP64 and mixed solves/s of the whole batch (device arrays, CUDA
+    events), their normalised error against the FP64 oracle on a sample (per
+    output), the FP64 form's roofline fraction, and the reference's own CPU
+    solver (oracle/_ref, else the C restatement) on one core and on all host
+    cores, each a bounded sample."""
+    import torch
+    from oracle import oracle
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    from addingdoublingrt_b200 import _lib
+    peaks = measured_peaks(_lib.load())
+    kind = "reference" if oracle.ref_available() else "port"
+    cpu_solve = (lambda b, n: oracle.solve_reference(b, n)) if kind == "reference" else \
+        (lambda b, n: oracle.solve_oracle(b, n))
+    cases = [("config1", lambda p: workloads.config1(), 1000),
+             ("config2", lambda p: workloads.config2(precision=p), 2000),
+             ("config3", lambda p: workloads.config3(precision=p), 500),
+             ("config5", lambda p: workloads.config5(precision=p), 1000)]
+    for name, make, nsample in cases:
+        row = {"metric": f"table row: {name}", "unit": "wavenumber-solves/s"}
+        outs = {}
+        for pname, prec in (("fp64", _abi.PRECISION_FP64), ("mixed", _abi.PRECISION_MIXED)):
+            b = make(prec)
+            b.desc.precision = prec
+            di = to_device(b)
+            do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+            eng.reserve(b.desc)
+            for _ in range(2):
+                eng.solve_device(b.desc, di, do)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(3):
+                eng.solve_device(b.desc, di, do)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / 3
+            row[f"{pname}_solves_per_s"] = b.W / (ms * 1e-3)
+            row[f"{pname}_ms"] = ms
+            outs[pname] = (b, do)
+            if pname == "fp64":
+                fl = oracle.flops(b)
+                row["fp64_roofline_frac"] = fl / (ms * 1e-3) / 1e12 / peaks["fp64_tflops"]
+                row["W"], row["L"], row["N"] = b.W, b.L, b.N
+        b = outs["fp64"][0]
+        idx = np.linspace(0, b.W - 1, min(b.W, nsample)).astype(np.int64)
+        sub = b.subset(idx)
+        ref = oracle.solve_oracle(sub, os.cpu_count() or 1, which=_abi.INTERFACE_OUTPUTS)
+        t = torch.as_tensor(idx, device="cuda")
+        for pname, (bb, do) in outs.items():
+            row[f"{pname}_normalized_error"] = {
+                k: oracle.norm_error(do[k].view(-1, b.L + 1)[t].cpu().numpy().ravel(), ref[k],
+                                     b.L + 1)
+                for k in ("flux_up", "flux_down", "flux_direct", "mean_intensity")}
+        # the reference's CPU solver: one core, and every host core
+        for cores in (1, os.cpu_count() or 1):
+            n = 8 * cores
+            while True:
+                sb = b.subset(np.arange(min(n, b.W)))
+                t0 = time.perf_counter()
+                cpu_solve(sb, cores)
+                dt = time.perf_counter() - t0
+                if dt > 3.0 or n >= b.W:
+                    break
+                n = int(min(b.W, n * max(2.0, 4.0 / max(dt, 1e-3))))
+            row[f"cpu_{cores}_cores_solves_per_s"] = sb.W / dt
+        row["cpu_kind"] = kind
+        print(json.dumps(row), flush=True)
 
 
 def run_band(args, eng):
@@ -320,7 +468,6 @@ def cuda_core_rate(args):
         env.pop(k, None)
     cmd = [sys.executable, os.path.abspath(__file__), "--only", "fp64", "--no-check",
            "--no-adjoint", "--no-cpu-baseline", "--no-cuda-core", "--no-e2e",
-           "--no-reference-gpu",
            "--wavenumbers", str(args.wavenumbers), "--steps", str(max(1, min(args.steps, 3))),
            "--warmup", str(max(1, min(args.warmup, 2)))]
     r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
@@ -334,16 +481,15 @@ def cuda_core_rate(args):
     return {"value": None, "error": (r.stderr or r.stdout)[-300:]}
 
 
-def reference_gpu(batch, eng, steps=3, warmup=1):
+def reference_gpu(batch, steps=3, warmup=1):
     """The reference's own GPU solver (adrt::cuda::solveBatch, src_cuda,
     compiled unmodified with --use_fast_math into oracle/_ref/libadrt_ref_gpu.so)
-    timed on `batch` between CUDA events, beside this engine's FP64 form on the
-    same batch.  The reference computes TOA F_up / F_down and BOA F_dir in FP32;
-    its TOA F_up error is measured against the engine's FP64 result (which
-    matches the FP64 oracle to 1e-9)."""
+    timed on `batch` between CUDA events (part of the reference arm).  The
+    reference computes TOA F_up / F_down and BOA F_dir in FP32 with its own
+    second-order layer start; its TOA F_up error is measured against the FP64
+    oracle on a sample of 256 wavenumbers."""
     import ctypes as C
-    import torch
-    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    from oracle import oracle
     path = os.path.join(ROOT, "oracle", "_ref", "libadrt_ref_gpu.so")
     if not os.path.exists(path):
         return {"unavailable": "oracle/_ref/libadrt_ref_gpu.so not built"}
@@ -358,8 +504,25 @@ def reference_gpu(batch, eng, steps=3, warmup=1):
                                 warmup, C.byref(ms), fu.ctypes.data, None, None)
     if rc != 0:
         return {"unavailable": lib.ref_gpu_last_error().decode()}
+    idx = np.linspace(0, W - 1, min(W, 256)).astype(np.int64)
+    ref = oracle.solve_oracle(batch.subset(idx), os.cpu_count() or 1,
+                              which=("toa_flux_up",))["toa_flux_up"]
+    return {"solves_per_s": W / (ms.value * 1e-3), "ms_per_call": ms.value,
+            "toa_flux_up_max_rel_err_vs_oracle": oracle_rel(fu[idx], ref),
+            "library": "oracle/_ref/libadrt_ref_gpu.so (src_cuda, --use_fast_math, sm_100a)",
+            "workload": REF_GPU_WORKLOAD}
+
+
+REF_GPU_WORKLOAD = ("config2 shape within the reference GPU API (workloads.config2_scalar): "
+                    "W x 100 layers, N=16, 32 moments shared per layer, scalar albedo / mu0 / band")
+
+
+def engine_rate(eng, batch, steps=3, warmup=1):
+    """The engine's FP64 solves/s on `batch` (device arrays, CUDA events)."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
     di = to_device(batch)
-    do = alloc_device_outputs(batch, ("toa_flux_up",))
+    do = alloc_device_outputs(batch, _abi.INTERFACE_OUTPUTS)
     eng.reserve(batch.desc)
     for _ in range(warmup):
         eng.solve_device(batch.desc, di, do)
@@ -370,13 +533,7 @@ def reference_gpu(batch, eng, steps=3, warmup=1):
         eng.solve_device(batch.desc, di, do)
     e1.record()
     torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1) / steps
-    ref = do["toa_flux_up"].cpu().numpy()
-    return {"solves_per_s": W / (ms.value * 1e-3), "ms_per_call": ms.value,
-            "engine_fp64_solves_per_s": W / (ems * 1e-3),
-            "engine_over_reference": ms.value / ems,
-            "toa_flux_up_max_rel_err_vs_fp64": oracle_rel(fu, ref),
-            "library": "oracle/_ref/libadrt_ref_gpu.so (src_cuda, --use_fast_math, sm_100a)"}
+    return batch.W / (e0.elapsed_time(e1) / steps * 1e-3)
 
 
 def oracle_rel(x, ref):
@@ -431,6 +588,8 @@ def main():
         return run_config4(args, eng)
     if args.workload == "band":
         return run_band(args, eng)
+    if args.workload == "table":
+        return run_table(args, eng)
     if args.workload == "adjoint":
         W = args.adjoint_wavenumbers
         fw, ad = time_adjoint(eng, W=W)
@@ -519,11 +678,10 @@ def main():
     cc = None
     if world == 1 and not args.no_cuda_core and not args.only:
         cc = cuda_core_rate(args)
-    refgpu = None
-    if world == 1 and not args.no_reference_gpu and not args.only:
-        refgpu = reference_gpu(workloads.config2_scalar(W=args.wavenumbers), eng)
-        refgpu["workload"] = ("config2 shape within the reference GPU API: W x 100 layers, "
-                              "N=16, moments shared per layer, scalar albedo / mu0 / band")
+    scalar_rate = None
+    if world == 1 and not args.only:
+        # the workload the reference arm times the reference's GPU solver on
+        scalar_rate = engine_rate(eng, workloads.config2_scalar(W=args.wavenumbers))
 
     adj = {}
     if not args.no_adjoint:
@@ -531,6 +689,17 @@ def main():
         fw2, ad2 = time_adjoint(eng, mode=_abi.ADJOINT_RECOMPUTE)
         adj = {"adjoint_over_forward": ad / fw, "adjoint_config5_ms": ad, "forward_config5_ms": fw,
                "adjoint_recompute_over_forward": ad2 / fw2, "adjoint_recompute_config5_ms": ad2}
+    c4 = None
+    if world == 1 and not args.only and not args.no_config4:
+        # free the headline batches first (config 4 holds 40 GB on the device)
+        for r in results.values():
+            r["out"] = {k: v.cpu() for k, v in r["out"].items()} if rank == 0 else None
+        torch.cuda.empty_cache()
+        try:
+            c4 = run_config4(args, eng, line=False)
+        except Exception as ex:
+            c4 = {"error": str(ex)[:300]}
+        torch.cuda.empty_cache()
     if rank == 0:
         from oracle import oracle
         fl = oracle.flops(b)  # algorithmic flops of the whole batch
@@ -567,7 +736,7 @@ def main():
             "mixed_over_fp64": (results["fp64"]["ms"] / results["mixed"]["ms"]
                                 if len(precisions) == 2 else None),
             "fp64_cuda_core_solves_per_s": cc["value"] if cc else None,
-            "reference_gpu": refgpu,
+            "fp64_solves_per_s_reference_gpu_workload": scalar_rate,
             "mixed_over_fp64_cuda_core": (job_rate(args.wavenumbers, world, results["mixed"]["ms"] * 1e-3)
                                           / cc["value"] if cc and cc.get("value") and
                                           "mixed" in results else None),
@@ -578,6 +747,7 @@ def main():
                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h} if e2e_s else None),
             "gpu_launches": args.steps,
             **adj,
+            "config4": c4,
             "clocks": results[pname]["clocks"],
             "device_status": {p: results[p]["status"] for p in precisions},
         }

@@ -59,8 +59,10 @@ enum adrt_status {
 enum adrt_device_flag {
   ADRT_FLAG_SINGULAR_PIVOT = 1, /* an LU pivot was exactly zero (reference: silent inv=0) */
   ADRT_FLAG_NONFINITE = 2,      /* a non-finite flux was produced */
-  ADRT_FLAG_BAD_INPUT = 4       /* tau < 0, omega outside [0,1], T < 0 seen on the device, or
+  ADRT_FLAG_BAD_INPUT = 4,      /* tau < 0, omega outside [0,1], T < 0 seen on the device, or
                                    a channel range outside the spectrum (band integration) */
+  ADRT_FLAG_PIVOT_FALLBACK = 8  /* a pivot-free tensor-core right-solve met a pivot below 1e-10
+                                   and was solved again with partial pivoting (results valid) */
 };
 
 /* ---------------------------------------------------------------- config */
@@ -352,9 +354,48 @@ typedef struct adrt_column_desc {
 } adrt_column_desc;
 
 /* Solve many columns of different W, L, N in ONE launch of the persistent
- * solver kernel.  The column table is copied to the device by the engine. */
+ * solver kernel per mapping (the engine's uneven plan, below; by default one
+ * launch of the warp-per-wavenumber kernel for every N <= 16 and one of the
+ * N = 32 kernel).  Replaces one adrt::cuda::solveBatch call per column
+ * (src_cuda/cuda_solver.cuh:77-80).  The column table is copied to the device
+ * by the engine; the call neither allocates nor synchronises the host once a
+ * call of the same size has been made, so it can be captured in a graph. */
 int adrt_solve_batch_uneven(adrt_engine* engine, const adrt_column_desc* cols, int ncols,
                             void* cuda_stream);
+
+/* How an uneven batch is mapped onto the GPU (no counterpart in the
+ * reference).  For padded orders 4, 8 and 16, the FP64 columns either run
+ * one wavenumber per warp in the persistent multi-order kernel
+ * (ADRT_MAPPING_WARP, the default) or one wavenumber per thread
+ * (ADRT_MAPPING_THREAD: the reference's solveKernel mapping,
+ * src_cuda/cuda_solver.cu:131-493, on this engine's scheme and outputs);
+ * mixed-precision columns always take the warp mapping.  warp_blocks_per_sm
+ * caps the warp launch's grid (0 = the occupancy limit); cost_order sorts the
+ * columns longest first (L N^3 per wavenumber) so that the dynamic task
+ * queue ends with short tasks.  ns_per_wavenumber holds what the autotuner
+ * measured for [order 4, 8, 16][warp, thread] (0 = not measured). */
+enum adrt_mapping { ADRT_MAPPING_WARP = 0, ADRT_MAPPING_THREAD = 1 };
+typedef struct adrt_uneven_plan {
+  int mapping[3];
+  int warp_blocks_per_sm;
+  int cost_order;
+  double ns_per_wavenumber[3][2];
+} adrt_uneven_plan;
+
+/* Autotune the uneven plan for this batch's shape: for every padded order
+ * present with FP64 columns, both mappings solve a sample of that order's
+ * wavenumbers (at least a few waves of the GPU's resident slots), and the
+ * faster one per wavenumber is kept; then the warp launch's grid cap is
+ * chosen the same way.  Results (including the measured times) go to `out`
+ * (may be NULL) and become the engine's plan.  Synchronises the stream; do
+ * not call it during a stream capture.  The sample solves write the sampled
+ * wavenumbers' outputs, which the next solve of the batch overwrites. */
+int adrt_engine_autotune_uneven(adrt_engine* engine, const adrt_column_desc* cols, int ncols,
+                                void* cuda_stream, adrt_uneven_plan* out);
+
+/* Set (e.g. a fixed mapping to compare against) or read the engine's plan. */
+int adrt_engine_set_uneven_plan(adrt_engine* engine, const adrt_uneven_plan* plan);
+int adrt_engine_get_uneven_plan(const adrt_engine* engine, adrt_uneven_plan* plan);
 
 /* ---------------------------------------------------------- utilities */
 

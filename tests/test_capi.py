@@ -178,3 +178,18 @@ def test_short_device_arrays_are_refused_before_the_launch():
         assert eng.read_status() == 0
     finally:
         eng.close()
+
+
+def test_mixed_form_refuses_gradients():
+    """The adjoint differentiates the FP64 form, so a mixed-form solve whose
+    inputs require gradients is refused before anything runs (no GPU needed)."""
+    import torch
+    from addingdoublingrt_b200 import torch_api
+    cfg = torch_api.BatchConfig()
+    cfg.precision = "mixed"
+    rng = np.random.default_rng(3)
+    tau, ssa, mom, planck = (torch.as_tensor(rng.uniform(0.1, 0.9, size=sh))
+                             for sh in ((3, 2), (3, 2), (2, 16), (3, 3)))
+    tau.requires_grad_(True)
+    with pytest.raises(ValueError, match="fp64"):
+        torch_api.solve_batch(cfg, tau, ssa, mom, planck)

@@ -245,6 +245,40 @@ def test_index_from_bottom_is_a_reversal(eng):
         assert np.array_equal(bot[k].reshape(8, L + 1)[:, ::-1], top[k].reshape(8, L + 1)), k
 
 
+@pytest.mark.parametrize("N", [8, 16, 32])
+def test_fp64_extremes_of_the_pivot_free_solve(eng, N):
+    """Inputs at the edges of the argument for the pivot-free tensor-core
+    solve: near-conservative thick layers (1 - omega = 1e-7, tau = 1e3, where
+    I - R^2 is nearly singular), unstable thin-layer starts (omega < 0.01 with
+    tau up to 1e3, where T = I - tau0 Gpp has large negative diagonal entries
+    and the solves use partial pivoting) and ordinary layers, mixed in every
+    column, against the oracle with the tiered FP64 tolerance."""
+    rng = np.random.default_rng(900 + N)
+    W, L, M = 24, 12, 2 * N
+    d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
+                       moment_layout=_abi.MOMENTS_PER_WAVENUMBER, use_thermal_emission=1,
+                       use_delta_m=1, use_diffusion_lower_bc=int(N == 32), solar_flux=1.0,
+                       solar_mu=0.5, surface_albedo=0.0 if N == 32 else 0.2)
+    b = workloads.Batch(d)
+    kind = rng.integers(0, 3, size=(W, L))
+    tau = np.where(kind == 0, 1e3, np.where(kind == 1, 10.0 ** rng.uniform(1, 3, size=(W, L)),
+                                            10.0 ** rng.uniform(-3, 0, size=(W, L))))
+    om = np.where(kind == 0, 1.0 - 1e-7, np.where(kind == 1, rng.uniform(0.001, 0.009, size=(W, L)),
+                                                  rng.uniform(0.1, 0.95, size=(W, L))))
+    b.set("delta_tau", tau)
+    b.set("single_scat_albedo", om)
+    b.set("phase_moments", workloads.hg_moments(rng.uniform(0.0, 0.95, size=W), M))
+    b.set("temperature", workloads.level_temperatures(rng, L))
+    lo = rng.uniform(500.0, 2000.0, size=W)
+    b.set("wavenumber_low", lo)
+    b.set("wavenumber_high", lo + 0.025)
+    ref = oracle.solve_oracle(b, 4)
+    sens = oracle.solve_oracle(b, 4, fma=True)
+    res = run_device(eng, b)
+    assert_fp64_parity(b, res, ref, sens, f"extremes N={N}")
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_SINGULAR_PIVOT) == 0
+
+
 MIXED_CASES = [
     # (name, batch, bound per wavenumber and output on the normalised error)
     ("config1", lambda: workloads.config1(W=1000).subset(np.arange(0, 1000, 5)), 1e-6),
@@ -298,6 +332,85 @@ def test_bad_values_set_the_device_status_flag(eng):
     run_device(eng, b)
     assert eng.read_status() & _abi.ADRT_FLAG_BAD_INPUT
     assert eng.read_status() == 0  # read clears
+
+
+def _uneven_cols(seed=4, ncols=12, per=200):
+    cols = [c.subset(np.arange(min(c.W, per)))
+            for c in workloads.config4_columns(ncols=ncols, seed=seed)]
+    cols.append(workloads.random_small(77, N=32, L=5, W=3, use_delta_m=0))
+    return cols
+
+
+def test_thread_mapping_matches_the_oracle(eng):
+    """The thread-per-wavenumber mapping (one thread solves a wavenumber, the
+    reference's solveKernel mapping) on FP64 columns of N 4, 8 and 16 -- one
+    wavenumber per column, plus every wavenumber of the small columns --
+    against the oracle with the tiered FP64 tolerance; mixed columns of the
+    same call keep the warp mapping and equal their separate solves."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    cols = _uneven_cols(seed=14, ncols=9, per=24)
+    for i, c in enumerate(cols):
+        c.desc.precision = _abi.PRECISION_MIXED if i % 4 == 3 else _abi.PRECISION_FP64
+    plan = eng.uneven_plan()
+    saved = _abi.UnevenPlan.from_buffer_copy(plan)
+    for i in range(3):
+        plan.mapping[i] = _abi.MAPPING_THREAD
+    eng.set_uneven_plan(plan)
+    try:
+        dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS))
+               for c in cols]
+        eng.solve_uneven(dev)
+        torch.cuda.synchronize()
+    finally:
+        eng.set_uneven_plan(saved)
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_BAD_INPUT) == 0
+    for c, (_, _, do) in zip(cols, dev):
+        res = {k: v.cpu().numpy() for k, v in do.items()}
+        if c.desc.precision == _abi.PRECISION_MIXED:
+            single = run_device(eng, c, _abi.INTERFACE_OUTPUTS)
+            for k in _abi.INTERFACE_OUTPUTS:
+                assert np.array_equal(res[k], single[k]), (c.N, k)
+            continue
+        ref = oracle.solve_oracle(c, 4, which=_abi.INTERFACE_OUTPUTS)
+        sens = oracle.solve_oracle(c, 4, which=_abi.INTERFACE_OUTPUTS, fma=True)
+        assert_fp64_parity(c, res, ref, sens, f"thread mapping N={c.N}")
+
+
+def test_autotuned_uneven_plan(eng):
+    """The autotuner measures both mappings for every order present and keeps
+    the faster; a solve under its plan equals the separate solves of each
+    column (FP64 columns to the FP64 tolerance of the oracle, since the thread
+    mapping sums in another order)."""
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    cols = _uneven_cols(seed=24, ncols=12, per=300)
+    for c in cols:
+        c.desc.precision = _abi.PRECISION_FP64
+    dev = [(c.desc, to_device(c), alloc_device_outputs(c, _abi.INTERFACE_OUTPUTS)) for c in cols]
+    saved = _abi.UnevenPlan.from_buffer_copy(eng.uneven_plan())
+    try:
+        plan = eng.autotune_uneven(dev)
+        d = plan.as_dict()
+        padded = {4 if c.N <= 4 else 8 if c.N <= 8 else 16 if c.N <= 16 else 32 for c in cols}
+        for o in (4, 8, 16):
+            if o in padded:
+                assert d["ns_per_wavenumber"][o]["warp"] > 0 and \
+                    d["ns_per_wavenumber"][o]["thread"] > 0, d
+                best = min(d["ns_per_wavenumber"][o], key=d["ns_per_wavenumber"][o].get)
+                assert d["mapping"][o] == best, d
+        eng.solve_uneven(dev)
+        torch.cuda.synchronize()
+    finally:
+        eng.set_uneven_plan(saved)
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_BAD_INPUT) == 0
+    for c, (_, _, do) in zip(cols, dev):
+        res = {k: v.cpu().numpy() for k, v in do.items()}
+        single = run_device(eng, c, _abi.INTERFACE_OUTPUTS)
+        sens = oracle.solve_oracle(c, 4, which=_abi.INTERFACE_OUTPUTS, fma=True)
+        ref = oracle.solve_oracle(c, 4, which=_abi.INTERFACE_OUTPUTS)
+        assert_fp64_parity(c, res, ref, sens, f"autotuned N={c.N}")
+        assert_fp64_parity(c, single, ref, sens, f"single N={c.N}")
 
 
 def test_uneven_batch_equals_separate_solves(eng):

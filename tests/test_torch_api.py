@@ -86,3 +86,4 @@ def test_solve_batch_forward_and_gradients():
             args_p[k], args_m[k] = ap, am
             fdv = (L(*args_p) - L(*args_m)) / (2 * h)
             assert abs(grad[idx] - fdv) <= 2e-6 * max(1.0, abs(fdv)), (k, idx, grad[idx], fdv)
+
