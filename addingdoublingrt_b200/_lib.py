@@ -29,6 +29,7 @@ EXPORTS = (
     "adrt_last_status_detail",
     "adrt_version",
     "adrt_probe_fma_tflops",
+    "adrt_probe_mma_tflops",
     "adrt_solve_batch_f32",
     "adrt_gauss_legendre",
     "adrt_planck_band",
@@ -79,6 +80,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         lib.adrt_last_status_detail.restype = C.c_char_p
         lib.adrt_version.restype = C.c_char_p
         lib.adrt_probe_fma_tflops.argtypes = [P(C.c_double), P(C.c_double)]
+        lib.adrt_probe_mma_tflops.argtypes = [P(C.c_double), P(C.c_double), P(C.c_double)]
         lib.adrt_gauss_legendre.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         lib.adrt_planck_band.argtypes = [C.c_double, C.c_double, C.c_double, P(C.c_double)]
         lib.adrt_planck_band_deriv.argtypes = [C.c_double, C.c_double, C.c_double,

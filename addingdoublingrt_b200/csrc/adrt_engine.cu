@@ -181,6 +181,9 @@ struct adrt_engine {
   char* hstage = nullptr;
   size_t hstage_bytes = 0;
   cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
+  // shared-moment phase tables of a batch (layout ADRT_MOMENTS_SHARED)
+  double* ptab = nullptr;
+  size_t ptab_bytes = 0;
   cudaEvent_t hev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::mutex hmu;  // one host-entry call at a time per engine
   std::mutex mu;
@@ -434,6 +437,60 @@ int cast_grid(size_t n, int num_sms) {
   return (int)(b < cap ? (b > 0 ? b : 1) : cap);
 }
 
+// Phase matrices of the moment sets every wavenumber shares (one per layer),
+// once per call: phase_table_kernel forms set u's normalised P++ / P+- into
+// table[u], which the solve reads instead of rebuilding them per wavenumber
+// and layer.  The table grows outside stream capture only.
+int ensure_ptab(adrt_engine* e, int np, int layers, cudaStreamCaptureStatus cap) {
+  const size_t need = (size_t)layers * 2 * np * np * sizeof(double);
+  if (need <= e->ptab_bytes) return ADRT_OK;
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(ADRT_ERR_WORKSPACE,
+                "phase table too small during stream capture; call adrt_engine_reserve first");
+  if (e->ptab) {
+    CUDA_TRY(cudaDeviceSynchronize());
+    cudaFree(e->ptab);
+    e->ptab = nullptr;
+    e->ptab_bytes = 0;
+  }
+  if (cudaMalloc(&e->ptab, need) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ADRT_ERR_OUT_OF_MEMORY, "phase table allocation failed");
+  }
+  e->ptab_bytes = need;
+  return ADRT_OK;
+}
+
+template <int NP>
+int launch_ptab(const ColumnDev& c, double* tab, int sets, cudaStream_t s) {
+  static bool ready = false;
+  if (!ready) {
+    CUDA_TRY(cudaFuncSetAttribute(phase_table_kernel<NP>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)AdjGroup<NP>::bytes));
+    ready = true;
+  }
+  phase_table_kernel<NP><<<sets, AdjGeo<NP>::G, AdjGroup<NP>::bytes, s>>>(c, tab);
+  CUDA_TRY(cudaGetLastError());
+  return ADRT_OK;
+}
+
+int phase_table(adrt_engine* e, ColumnDev& c, cudaStream_t s) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  int rc = ensure_ptab(e, c.NP, c.L, cap);
+  if (rc) return rc;
+  switch (c.NP) {
+    case 4: rc = launch_ptab<4>(c, e->ptab, c.L, s); break;
+    case 8: rc = launch_ptab<8>(c, e->ptab, c.L, s); break;
+    case 16: rc = launch_ptab<16>(c, e->ptab, c.L, s); break;
+    default: rc = launch_ptab<32>(c, e->ptab, c.L, s); break;
+  }
+  if (rc) return rc;
+  c.ptab = e->ptab;
+  return ADRT_OK;
+}
+
 // adrt_solve_batch after argument checks, with e->mu held.
 int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
                  const adrt_outputs* out, cudaStream_t s, const adrt_raw_inputs* raw = nullptr) {
@@ -466,6 +523,7 @@ int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   p.max_layers = d->num_layers;
   const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
   grid = std::min(grid, need_blocks);
+  if (!raw && d->moment_layout == ADRT_MOMENTS_SHARED && (rc = phase_table(e, c0, s))) return rc;
   CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
   return k.launch(p, c0, grid, s);
 }
@@ -791,6 +849,7 @@ int adrt_engine_destroy(adrt_engine* e) {
     if (ev) cudaEventDestroy(ev);
   cudaFree(e->stage);
   cudaFree(e->adj_scratch);
+  cudaFree(e->ptab);
   delete e;
   return ADRT_OK;
 }
@@ -805,6 +864,10 @@ int adrt_engine_reserve(adrt_engine* e, const adrt_batch_desc* d) {
   KernInfo k = pick(d->num_quadrature, d->precision);
   int grid;
   size_t sb;
+  if (d->moment_layout == ADRT_MOMENTS_SHARED &&
+      (rc = ensure_ptab(e, padded_order(d->num_quadrature), d->num_layers,
+                        cudaStreamCaptureStatusNone)))
+    return rc;
   return ensure_scratch(e, k, d->num_layers, &grid, &sb);
 }
 
@@ -1227,6 +1290,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   if (ptab_bytes) {
     k.tlaunch(c0, const_cast<double*>(a.ptab), L, k.gsmem, s);
     CUDA_TRY(cudaGetLastError());
+    c0.ptab = a.ptab;  // the taping forward reads the table too
   }
   if (psum_bytes) CUDA_TRY(cudaMemsetAsync(a.pacc, 0, psum_bytes, s));
   for (long long w0 = 0; w0 < W; w0 += wc) {

@@ -300,20 +300,24 @@ __device__ __forceinline__ void phase_products(const double* chi, int nuse, doub
 // and, with `solar`, the solar phase vectors into D_PP / D_PM.  With PL0,
 // plm0[l] = P_l(mu0) for l < nuse (formed once per wavenumber by the same
 // recurrence) and the un-normalised solar vectors also go to D_LAM0 / D_LAM1.
+// With mats = false only the solar vectors are formed (the matrices come from
+// a table).
 template <class Gm, bool PL0 = false>
 __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
                                          const double* chi, int nuse, double f, int N,
                                          const double* pl, bool solar, double mu0, double* Ppp,
-                                         double* Ppm, const double* plm0 = nullptr) {
+                                         double* Ppm, const double* plm0 = nullptr,
+                                         bool mats = true) {
   constexpr int NP = Gm::NP, G = Gm::G;
   const Ctx<Gm> X(goff, tb, t_, bar);
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
-  if constexpr (UsePhaseMMA<Gm>::value)
+  if (!mats) {
+  } else if constexpr (UsePhaseMMA<Gm>::value) {
     // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
     phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
-  else
+  } else {
   for (int e = t; e < NP * NP; e += G) {
     const int r = e / NP, c = e % NP;
     double spp = 0.0, spm = 0.0;
@@ -332,8 +336,9 @@ __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int
     Ppp[e] = spp;
     Ppm[e] = spm;
   }
+  }
   X.sync();
-  if (!UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
+  if (mats && !UsePhaseMMA<Gm>::value && t < N) {  // Hansen renormalisation (scalar path)
     const int c = t;
     double sum = 0.0;
     for (int i = 0; i < N; ++i) sum += (Ppp[i * NP + c] + Ppm[i * NP + c]) * wt[i];
@@ -1254,8 +1259,9 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
   const double F0 = C->solar_flux;
   const bool solar = (F0 > 0.0 && mu0 > 0.0);
   const Levels lv(slot, lmax);
-  double* Ppp = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
-  double* Ppm = Ppp + NP * NP;
+  double* Pslot = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
+  const double* Ppp = Pslot;
+  const double* Ppm = Pslot + NP * NP;
   Real* recs = reinterpret_cast<Real*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
   const double* chi_base = C->moments;
   const double Bs = X.sc[S_BS], Btop = X.sc[S_BTOP];
@@ -1284,8 +1290,8 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
     int nuse;
     double f;
     const double* chi = moments(0, nuse, f);
-    build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
-                    Ppm);
+    build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Pslot,
+                    Pslot + NP * NP);
   }
 
   // ---------------- bottom composite: surface, or the lower boundary intensity
@@ -1380,12 +1386,25 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
           }
       }
     } else {
-      if (layout != 1) {
+      if (layout == 0 && C->ptab) {
+        // the shared set's matrices from the call's table; the solar vectors
+        // depend on this wavenumber's mu0
+        const int u = from_bottom ? nL - 1 - l : l;
+        Ppp = C->ptab + (size_t)u * 2 * NP * NP;
+        Ppm = Ppp + NP * NP;
+        if (solar) {
+          int nuse;
+          double f;
+          const double* chi = moments(l, nuse, f);
+          build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0,
+                          nullptr, nullptr, nullptr, false);
+        }
+      } else if (layout != 1) {
         int nuse;
         double f;
         const double* chi = moments(l, nuse, f);
-        build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
-                    Ppm);
+        build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Pslot,
+                        Pslot + NP * NP);
       }
       if constexpr (MODE == MODE_FP64) {
         Real* tape_l = nullptr;

@@ -39,6 +39,9 @@ struct ColumnDev {
   const double* raw_wn;
   QuadDev quad;
   long long task_begin;  // first flattened task index of this column
+  // normalised P++ / P+- of the moment sets shared by every wavenumber (one
+  // per layer, [L][2][NP][NP]), formed once per call; null: built per layer
+  const double* ptab;
 };
 
 // Kernel parameters (passed by value).

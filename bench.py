@@ -706,6 +706,7 @@ def main():
         ms = results[pname]["ms"]
         peaks = measured_peaks(_lib.load())
         pk = peaks["fp64_tflops"] if pname == "fp64" else peaks["fp32_tflops"]
+        tpk = tensor_peaks(_lib.load())
         achieved = fl / (ms * 1e-3) / 1e12
         traffic = None
         try:
@@ -742,6 +743,9 @@ def main():
                                           "mixed" in results else None),
             "accuracy_vs_oracle": acc,
             "roofline": roof,
+            "peaks": {"fp64_fma_tflops": peaks["fp64_tflops"],
+                      "fp32_fma_tflops": peaks["fp32_tflops"], **(tpk or {}),
+                      "source": "probe kernels on this GPU (csrc/adrt_probe.cu)"},
             "e2e": ({"value": job_rate(args.wavenumbers, world, e2e_s),
                      "unit": "wavenumber-solves/s",
                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h} if e2e_s else None),
@@ -757,6 +761,17 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def tensor_peaks(lib):
+    """Warp-level tensor-core throughput of this GPU (adrt_probe_mma_tflops)."""
+    import ctypes as C
+    v = [C.c_double() for _ in range(3)]
+    if hasattr(lib, "adrt_probe_mma_tflops") and \
+            lib.adrt_probe_mma_tflops(*(C.byref(x) for x in v)) == 0:
+        return {"fp64_dmma_tflops": v[0].value, "tf32_mma_tflops": v[1].value,
+                "bf16_mma_tflops": v[2].value}
+    return None
 
 
 def measured_peaks(lib):

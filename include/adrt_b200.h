@@ -405,6 +405,12 @@ int adrt_engine_get_uneven_plan(const adrt_engine* engine, adrt_uneven_plan* pla
  * has no counterpart. */
 int adrt_probe_fma_tflops(double* fp64_tflops, double* fp32_tflops);
 
+/* Measured warp-level tensor-core throughput (TFLOP/s) of the current device:
+ * mma.sync m8n8k4 f64 (the FP64 products and right-solves), m16n8k8 tf32 (the
+ * mixed form's FP32 products, three per product) and m16n8k16 bf16.  Engine
+ * utility; the reference has no counterpart. */
+int adrt_probe_mma_tflops(double* fp64_dmma_tflops, double* tf32_tflops, double* bf16_tflops);
+
 /* Gauss-Legendre nodes and weights on [0,1], the engine's own quadrature
  * (replaces adrt::gaussLegendre, src/quadrature.cpp:11-51). */
 int adrt_gauss_legendre(int n, double* nodes, double* weights);
