@@ -723,11 +723,15 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
 // SOL the solar vectors' (which depend on each wavenumber's mu0; plm0[l] =
 // P_l(mu0) for l < nuse, the un-normalised vectors in D_LAM0 / D_LAM1 as
 // build_phase<Gm, true> leaves them).
+//
+// With delta-M truncation (f >= 0: the forward used chi*_l = (chi_l - f) /
+// (1 - f) for l < nuse = 2N, f = chi_2N, src/solver.cpp:441-501) the cotangent
+// of chi*_l reaches chi_l as 1 / (1 - f) and chi_2N as (chi_l - 1) / (1 - f)^2.
 template <class Gm, bool MAT = true, bool SOL = true>
 __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, int bar,
                                            const double* chi, int nuse, int N, const double* pl,
                                            bool solar, double mu0, double* dchi,
-                                           const double* plm0) {
+                                           const double* plm0, double f = -1.0) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   constexpr int NP = Gm::NP, G = Gm::G, LD = Gm::LD;
@@ -744,10 +748,20 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
   Real* qp = vb + A_H * NP;
   Real* qm = vb + A_RU * NP;
   solar = SOL && solar;
+  const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
+  // the cotangent v of the effective moment l, into the inputs' moments
+  auto add_moment = [&](int l, double v) {
+    if (f >= 0.0) {
+      atomicAdd(&dchi[l], v * inv_1mf);
+      atomicAdd(&dchi[nuse], v * (chi[l] - 1.0) * inv_1mf * inv_1mf);
+    } else {
+      atomicAdd(&dchi[l], v);
+    }
+  };
   if constexpr (MAT) {
     // un-normalised Q
     if constexpr (UsePhaseMMA<Gm>::value)
-      phase_products<Gm>(chi, nuse, -1.0, N, pl, Qpp, Qpm, LD, t);
+      phase_products<Gm>(chi, nuse, f, N, pl, Qpp, Qpm, LD, t);
     else
     for (int e = t; e < NP * NP; e += G) {
       const int r = e / NP, c = e % NP;
@@ -755,7 +769,8 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
       if (r < N && c < N) {
         double sign = 1.0;
         for (int l = 0; l < nuse; ++l) {
-          const double term = (2 * l + 1) * chi[l] * pl[l * N + r] * pl[l * N + c];
+          const double cl = (f >= 0.0) ? (chi[l] - f) * inv_1mf : chi[l];
+          const double term = (2 * l + 1) * cl * pl[l * N + r] * pl[l * N + c];
           spp += term;
           spm += sign * term;
           sign = -sign;
@@ -837,8 +852,8 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
         s1 += __shfl_xor_sync(0xffffffffu, s1, o);
       }
       if (g == 0) {
-        if (l0 < nuse) atomicAdd(&dchi[l0], (2 * l0 + 1) * s0 / (2.0 * kPi));
-        if (l1 < nuse) atomicAdd(&dchi[l1], (2 * l1 + 1) * s1 / (2.0 * kPi));
+        if (l0 < nuse) add_moment(l0, (2 * l0 + 1) * s0 / (2.0 * kPi));
+        if (l1 < nuse) add_moment(l1, (2 * l1 + 1) * s1 / (2.0 * kPi));
       }
     }
     forms_done = true;
@@ -863,7 +878,7 @@ __device__ __noinline__ void phase_adjoint(unsigned goff, unsigned tb, int t_, i
           if (i < N) sv += pl[l * N + i] * (qp[i] + sg * qm[i]);
         acc += plm * sv;
       }
-      atomicAdd(&dchi[l], (2 * l + 1) * acc / (2.0 * kPi));
+      add_moment(l, (2 * l + 1) * acc / (2.0 * kPi));
     }
   }
   X.sync();
@@ -1145,11 +1160,13 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     }
   }
   int nuse_l1 = M;
+  double f_l1 = -1.0;
   if (layout == 1) {  // one moment set per wavenumber: the solar phase vectors once
     int nuse;
     double f;
     const double* chi = moments(0, nuse, f);
     nuse_l1 = nuse;
+    f_l1 = f;
     build_phase<Gm, true>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Ppp,
                           Ppm, plm0);
   }
@@ -1365,10 +1382,10 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
           }
           if (solar)
             phase_adjoint<Gm, false, true>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl,
-                                           solar, mu0, dchi, plm0);
+                                           solar, mu0, dchi, plm0, f);
         } else if (dchi) {
           phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, N, C->quad.pl, solar, mu0, dchi,
-                            plm0);
+                            plm0, f);
         }
       } else {  // one moment set per wavenumber: accumulate the phase cotangents
         if (tl.valid()) {
@@ -1432,7 +1449,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     X.sync();
     const double* chi = C->moments + (size_t)w * M;
     phase_adjoint<Gm>(X.goff, X.tb, t, X.bar, chi, nuse_l1, N, C->quad.pl, solar, mu0,
-                      AD.g_mom + (size_t)w * M, plm0);
+                      AD.g_mom + (size_t)w * M, plm0, f_l1);
   }
   // ======== 3. lower boundary, beam and Planck chain rules
   double pub = 0.0, pubmu = 0.0;
@@ -1481,8 +1498,28 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
   for (int l = t; l < nL; l += G) {
     const int ul = fb ? nL - 1 - l : l;
     const double om = lv.om[l];
-    if (AD.g_tau) AD.g_tau[(size_t)w * nL + ul] = gtau[l];
-    if (AD.g_ssa) AD.g_ssa[(size_t)w * nL + ul] = (om > 0.0 && om <= 1.0) ? gom[l] : 0.0;
+    double gt = gtau[l], go = (om > 0.0 && om <= 1.0) ? gom[l] : 0.0;
+    // delta-M scaling (src/solver.cpp:441-501): tau' = (1 - omega f) tau,
+    // omega' = omega (1 - f) / (1 - omega f), f = chi_2N of the layer's set;
+    // the cotangents above are those of tau' and omega'
+    const double om_u = lv.omu[l];
+    const double tau_u = C->dtau[(size_t)w * nL + ul];
+    if (C->delta_m && M > 2 * N && om_u > 0.0 && tau_u > 0.0) {
+      int nuse;
+      double f;
+      const double* chi = moments(l, nuse, f);
+      if (f >= 0.0) {
+        const double d = 1.0 - om_u * f;
+        const double gtu = gt * d;
+        const double gou = -gt * f * tau_u + go * (1.0 - f) / (d * d);
+        const double gf = -gt * om_u * tau_u + go * om_u * (om_u - 1.0) / (d * d);
+        if (AD.g_mom) atomicAdd(&AD.g_mom[(size_t)(chi - C->moments) + 2 * N], gf);
+        gt = gtu;
+        go = gou;
+      }
+    }
+    if (AD.g_tau) AD.g_tau[(size_t)w * nL + ul] = gt;
+    if (AD.g_ssa) AD.g_ssa[(size_t)w * nL + ul] = (om_u > 0.0 && om_u <= 1.0) ? go : 0.0;
   }
   for (int l = t; l <= nL; l += G) {
     const int ul = fb ? nL - l : l;
@@ -1691,7 +1728,7 @@ __global__ void __launch_bounds__(AdjGeo<NP>::G) phase_finish_kernel(ColumnDev c
   double f;
   moment_use(&col0, chi, nuse, f);
   phase_adjoint<Gm, true, false>(X.goff, X.tb, t, X.bar, chi, nuse, col0.N, col0.quad.pl, false,
-                                 1.0, AD.g_mom + u * col0.M, nullptr);
+                                 1.0, AD.g_mom + u * col0.M, nullptr, f);
 }
 
 }  // namespace adrt_dev

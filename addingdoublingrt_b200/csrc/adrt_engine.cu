@@ -1135,13 +1135,6 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   int rc = check_desc(d);
   if (rc) return rc;
   if ((rc = check_inputs(d, in))) return rc;
-  // with delta-M truncation the source gradients stand, but those with respect
-  // to the unscaled optical properties and moments are not formed
-  if (d->use_delta_m && d->num_moments > 2 * d->num_quadrature &&
-      (gr->delta_tau || gr->single_scat_albedo || gr->phase_moments))
-    return fail(ADRT_ERR_UNSUPPORTED,
-                "adjoint: with delta-M truncation (use_delta_m, num_moments > 2N) only "
-                "temperature, planck_levels and surface_emission gradients are formed");
   std::lock_guard<std::mutex> lk(e->mu);
   if ((rc = set_device(e))) return rc;
   cudaStream_t s = static_cast<cudaStream_t>(stream_ptr);

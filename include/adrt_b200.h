@@ -328,8 +328,10 @@ int adrt_engine_set_adjoint_mode(adrt_engine* engine, int mode);
  * wavenumbers; chains beyond the record pool are recomputed), or, in
  * ADRT_ADJOINT_RECOMPUTE mode, the backward pass recomputes them all.  `out` may be
  * NULL or receive the forward outputs.  With delta-M truncation in effect
- * (use_delta_m with num_moments > 2N) only the temperature, planck_levels and
- * surface_emission gradients are formed. */
+ * (use_delta_m with num_moments > 2N) the gradients are those of the
+ * unscaled inputs: tau' = (1 - omega f) tau, omega' = omega (1 - f) /
+ * (1 - omega f) and chi*_l = (chi_l - f) / (1 - f), f = chi_2N, are
+ * differentiated through (src/solver.cpp:441-501), f included. */
 int adrt_adjoint(adrt_engine* engine, const adrt_batch_desc* desc, const adrt_inputs* in,
                  const adrt_outputs* out, const adrt_cotangents* cot,
                  const adrt_gradients* grads, void* cuda_stream);

@@ -329,6 +329,44 @@ def test_delta_m_truncated_temperature_gradient_matches_finite_differences(eng):
     assert e < 1e-4, ("temperature", e)
 
 
+@pytest.mark.parametrize("layout", [_abi.MOMENTS_SHARED, _abi.MOMENTS_PER_WAVENUMBER,
+                                    _abi.MOMENTS_PER_LAYER])
+def test_delta_m_truncated_gradients_match_finite_differences(eng, layout):
+    """With delta-M truncation (3N moments, f = chi_2N) the gradients in tau,
+    omega and every moment -- through the scaled tau', omega' and chi* of
+    src/solver.cpp:441-501, f included -- against central differences of the
+    oracle, for the three moment layouts."""
+    N = 8
+    b = small_batch(61 + layout, N, W=3, L=5, layout=layout)
+    M = 3 * N
+    g = b.arrays["phase_moments"].reshape(-1, 2 * N)[:, 1]
+    b.desc.num_moments = M
+    b.set("phase_moments", workloads.hg_moments(g, M))
+    assert np.all(g ** (2 * N) > 1e-12)  # truncation active in every set
+    rng = np.random.default_rng(61)
+    cot = {k: rng.normal(size=b.W * (b.L + 1)) for k in COT}
+    ad = run_adjoint(eng, b, cot)
+    for name in ("delta_tau", "single_scat_albedo"):
+        fd = fd_layer_param(b, cot, name)
+        e = rel_err(ad[name].reshape(b.W, b.L), fd)
+        assert e < 2e-5, (name, layout, e)
+    chi = b.arrays["phase_moments"].reshape(-1, M)
+    fd = np.zeros_like(chi)
+    h = 1e-6
+    for s_ in range(chi.shape[0]):
+        for m in range(M):
+            vals = []
+            for sgn in (1.0, -1.0):
+                c = chi.copy()
+                c[s_, m] += sgn * h
+                bb = workloads.Batch(_abi.BatchDesc.from_buffer_copy(b.desc), dict(b.arrays))
+                bb.set("phase_moments", c)
+                vals.append(loss_per_wav(bb, cot).sum())
+            fd[s_, m] = (vals[0] - vals[1]) / (2 * h)
+    e = rel_err(ad["phase_moments"].reshape(-1, M), fd)
+    assert e < 1e-4, ("phase_moments", layout, e)
+
+
 def test_shared_moments_without_block_sums_match_per_layer_sets(eng):
     """Shared per-layer moments whose per-block cotangent sums would pass
     1 GB (here 1800 layers at N = 16) take the per-layer moment adjoint beside
