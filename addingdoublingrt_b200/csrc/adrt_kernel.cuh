@@ -790,13 +790,18 @@ __device__ __noinline__ int doubling_lam(unsigned goff, unsigned tb, int t_, int
 // row-major.  Returns 8 (the buffer of the row-major T); the layer sources
 // are left as by doubling_lam.
 template <class Gm>
-__device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int bar, double tau,
-                                        double om, double Bt, double Bb, double tcum, int N,
-                                        bool solar, double F0, double mu0, const double* Ppp,
-                                        const double* Ppm, int* singular, double* src64) {
+__device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, unsigned tbD, int t_,
+                                        int bar, double tau, double om, double Bt, double Bb,
+                                        double tcum, int N, bool solar, double F0, double mu0,
+                                        const double* Ppp, const double* Ppm, int* singular,
+                                        double* src64) {
   static_assert(UseTC32<Gm>::value && UseGjRows<Gm>::value, "tensor-core FP32 geometry");
   using Real = float;
   const Ctx<Gm> X(goff, tb, t_, bar);
+  // the source vectors (a, b, s_up, s_dn and the solar ru, rd) in FP64, in
+  // the class-D group's FP64 vector slots (idle while a layer doubles in
+  // FP32; V_UB, the composite's source, is not touched)
+  const Ctx<Geo<Gm::NP, double, Gm::G>> XV(goff, tbD, t_, bar);
   constexpr int NP = Gm::NP, TR = Gm::TR, TC = Gm::TC, LD = Gm::LD;
   const int t = X.t;
   const double* mu = X.DV(D_MU);
@@ -852,10 +857,10 @@ __device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int 
       }
     }
     X.DV(D_LAM0)[i] = lam;
-    X.V(V_Y0)[i] = static_cast<Real>(a);
-    X.V(V_Z0)[i] = static_cast<Real>(-a);
-    X.V(V_SU0)[i] = static_cast<Real>(su);
-    X.V(V_SD0)[i] = static_cast<Real>(sd);
+    XV.V(V_Y0)[i] = a;
+    XV.V(V_Z0)[i] = -a;
+    XV.V(V_SU0)[i] = su;
+    XV.V(V_SD0)[i] = sd;
   }
   int r0, c0;
   tc32_origin<Gm>(t, r0, c0);
@@ -864,20 +869,19 @@ __device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int 
   int cur = 0;
   for (int k = 0; k < nn; ++k) {
     const int par = k & 1;
-    Real* av = X.V(V_Y0 + par);
-    Real* bv = X.V(V_Z0 + par);
-    Real* su = X.V(V_SU0 + par);
-    Real* sd = X.V(V_SD0 + par);
+    double* av = XV.V(V_Y0 + par);
+    double* bv = XV.V(V_Z0 + par);
+    double* su = XV.V(V_SU0 + par);
+    double* sd = XV.V(V_SD0 + par);
     const double* lam = X.DV(D_LAM0 + par);
-    const Real gmv = static_cast<Real>(gam);
     X.sync();  // R, T, T', Lambda and the vectors of the previous step are complete
     if (solar && X.warp == 0) {  // ru = R sd + gam su, rd = gam R su + sd (old R)
-      const Real* vv[2] = {sd, su};
-      Real yv[2];
-      matvec<Gm, true, 2>(Rc, vv, yv, X.lane);
+      const double* vv[2] = {sd, su};
+      double yv[2];
+      matvec_fd<Gm, true, 2>(Rc, vv, yv, X.lane);
       if (X.lane < NP) {
-        X.V(V_RU)[X.lane] = yv[0] + gmv * su[X.lane];
-        X.V(V_RD)[X.lane] = gmv * yv[1] + sd[X.lane];
+        XV.V(V_RU)[X.lane] = yv[0] + gam * su[X.lane];
+        XV.V(V_RD)[X.lane] = gam * yv[1] + sd[X.lane];
       }
     }
     {  // A = I - R^2, RHS = Lambda R^2 + T'
@@ -942,33 +946,33 @@ __device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int 
         }
     }
     if (X.warp == 0) {
-      Real* an = X.V(V_Y0 + 1 - par);
-      Real* bn = X.V(V_Z0 + 1 - par);
-      Real* sun = X.V(V_SU0 + 1 - par);
-      Real* sdn = X.V(V_SD0 + 1 - par);
-      if (X.lane < NP) X.V(V_TMP)[X.lane] = Real(2) * av[X.lane] - bv[X.lane];
+      double* an = XV.V(V_Y0 + 1 - par);
+      double* bn = XV.V(V_Z0 + 1 - par);
+      double* sun = XV.V(V_SU0 + 1 - par);
+      double* sdn = XV.V(V_SD0 + 1 - par);
+      if (X.lane < NP) XV.V(V_TMP)[X.lane] = 2.0 * av[X.lane] - bv[X.lane];
       __syncwarp();
-      const Real* vc[2] = {X.V(V_TMP), bv};
-      Real gv[2], rv[2];
-      matvec<Gm, false, 2>(Gp, vc, gv, X.lane);  // G' c, G' b
-      matvec<Gm, false, 2>(Am, vc, rv, X.lane);  // TGR c, TGR b
-      Real gs[2] = {Real(0), Real(0)};
+      const double* vc[2] = {XV.V(V_TMP), bv};
+      double gv[2], rv[2];
+      matvec_fd<Gm, false, 2>(Gp, vc, gv, X.lane);  // G' c, G' b
+      matvec_fd<Gm, false, 2>(Am, vc, rv, X.lane);  // TGR c, TGR b
+      double gs[2] = {0.0, 0.0};
       if (solar) {
-        const Real* vs[2] = {X.V(V_RU), X.V(V_RD)};
-        matvec<Gm, false, 2>(Gp, vs, gs, X.lane);
+        const double* vs[2] = {XV.V(V_RU), XV.V(V_RD)};
+        matvec_fd<Gm, false, 2>(Gp, vs, gs, X.lane);
       }
       if (X.lane < NP) {
         const int i = X.lane;
-        const Real l = static_cast<Real>(lam[i]);
-        const Real c = X.V(V_TMP)[i], a = av[i], b = bv[i];
+        const double l = lam[i];
+        const double c = XV.V(V_TMP)[i], a = av[i], b = bv[i];
         an[i] = ((l * c + gv[0]) - rv[1]) + a;
-        bn[i] = ((l * b + gv[1]) - rv[0]) + (Real(2) * b - a);
+        bn[i] = ((l * b + gv[1]) - rv[0]) + (2.0 * b - a);
         if (solar) {
-          sun[i] = (l * X.V(V_RU)[i] + gs[0]) + su[i];
-          sdn[i] = (l * X.V(V_RD)[i] + gs[1]) + gmv * sd[i];
+          sun[i] = (l * XV.V(V_RU)[i] + gs[0]) + su[i];
+          sdn[i] = (l * XV.V(V_RD)[i] + gs[1]) + gam * sd[i];
         } else {
-          sun[i] = Real(0);
-          sdn[i] = Real(0);
+          sun[i] = 0.0;
+          sdn[i] = 0.0;
         }
         X.DV(D_LAM0 + 1 - par)[i] = lam[i] * lam[i];
       }
@@ -990,8 +994,8 @@ __device__ __noinline__ int doubling_tc(unsigned goff, unsigned tb, int t_, int 
   }
   if (X.warp == 0 && X.lane < NP) {
     const int i = X.lane, par = nn & 1;
-    const double a = X.V(V_Y0 + par)[i], b = X.V(V_Z0 + par)[i];
-    const double su = X.V(V_SU0 + par)[i], sd = X.V(V_SD0 + par)[i];
+    const double a = XV.V(V_Y0 + par)[i], b = XV.V(V_Z0 + par)[i];
+    const double su = XV.V(V_SU0 + par)[i], sd = XV.V(V_SD0 + par)[i];
     double up = 0.0, dn = 0.0;
     if (i < N) {
       up = (a * Bb - b * Bt) / tau + su;
@@ -1024,8 +1028,8 @@ __device__ __noinline__ int doubling_lam_wide(unsigned goff, unsigned tbD, unsig
   static_assert(GmF::TR == TR && GmF::TC == TC && GmF::G == GmD::G, "tile maps must agree");
   int tF;
   if constexpr (UseTC32<GmF>::value && UseGjRows<GmF>::value)
-    tF = doubling_tc<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
-                          singular, src64);
+    tF = doubling_tc<GmF>(goff, tbF, tbD, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp,
+                          Ppm, singular, src64);
   else
     tF = doubling_lam<GmF>(goff, tbF, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp,
                            Ppm, singular, src64);

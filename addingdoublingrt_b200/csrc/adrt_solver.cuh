@@ -1158,6 +1158,31 @@ __device__ __forceinline__ void matvec(const typename Gm::Real* S,
     for (int n = 0; n < NV; ++n) y[n] += __shfl_xor_sync(0xffffffffu, y[n], off);
 }
 
+// y = X v with X an FP32 smem matrix and the vectors in FP64 (accumulated in
+// FP64): the source recurrences of the FP32 doubling, whose vectors are
+// carried in FP64.  Lane layout as matvec.
+template <class Gm, bool CM, int NV>
+__device__ __forceinline__ void matvec_fd(const float* S, const double* const (&v)[NV],
+                                          double (&y)[NV], int lane) {
+  constexpr int NP = Gm::NP, LPR = Gm::LPR, KCH = Gm::KCH, LD = Gm::LD;
+  const int i = lane % NP, part = lane / NP;
+#pragma unroll
+  for (int n = 0; n < NV; ++n) y[n] = 0.0;
+  if (part < LPR) {
+#pragma unroll
+    for (int kk = 0; kk < KCH; ++kk) {
+      const int k = part * KCH + kk;
+      const double x = CM ? S[k * LD + i] : S[i * LD + k];
+#pragma unroll
+      for (int n = 0; n < NV; ++n) y[n] = fma(x, v[n][k], y[n]);
+    }
+  }
+#pragma unroll
+  for (int off = NP; off < NP * LPR; off <<= 1)
+#pragma unroll
+    for (int n = 0; n < NV; ++n) y[n] += __shfl_xor_sync(0xffffffffu, y[n], off);
+}
+
 // ============================================================== Planck (device)
 // Band-integrated Planck function, DisORT method: Simpson refinement for
 // narrow bands, small-v polynomial / large-v exponential series otherwise.

@@ -507,8 +507,11 @@ def reference_gpu(batch, steps=3, warmup=1):
     idx = np.linspace(0, W - 1, min(W, 256)).astype(np.int64)
     ref = oracle.solve_oracle(batch.subset(idx), os.cpu_count() or 1,
                               which=("toa_flux_up",))["toa_flux_up"]
+    scale = float(np.max(np.abs(ref))) or 1.0
     return {"solves_per_s": W / (ms.value * 1e-3), "ms_per_call": ms.value,
             "toa_flux_up_max_rel_err_vs_oracle": oracle_rel(fu[idx], ref),
+            "toa_flux_up_median_rel_err_vs_oracle":
+                float(np.median(np.abs(fu[idx] - ref) / np.maximum(np.abs(ref), 1e-12 * scale))),
             "library": "oracle/_ref/libadrt_ref_gpu.so (src_cuda, --use_fast_math, sm_100a)",
             "workload": REF_GPU_WORKLOAD}
 

@@ -96,14 +96,20 @@ def unstable_start(b):
     return out
 
 
-def assert_fp64_parity(b, res, ref, sens_ref, tag):
+def assert_fp64_parity(b, res, ref, sens_ref, tag, other_ref=None):
+    """other_ref: a second FP64 evaluation of the scheme (the reference's own
+    build: pivoted LU, FMA contraction); near-conservative wavenumbers are then
+    held to 1e-6 + 30 times its spread from the oracle instead of 1e-6."""
     per = b.L + 1
     nc = near_conservative(b)
     us = unstable_start(b)
     for k in OUTS:
         e = per_wav_norm_err(res[k], ref[k], per)
         s = per_wav_norm_err(sens_ref[k], ref[k], per)
-        bound = np.where(nc, 1e-6, 1e-9 + np.where(us, 1000.0, 30.0) * s)
+        nc_bound = 1e-6
+        if other_ref is not None:
+            nc_bound = 1e-6 + 30.0 * np.maximum(s, per_wav_norm_err(other_ref[k], ref[k], per))
+        bound = np.where(nc, nc_bound, 1e-9 + np.where(us, 1000.0, 30.0) * s)
         bad = np.nonzero(e > bound)[0]
         assert bad.size == 0, (tag, k, int(bad[0]), float(e[bad[0]]), float(bound[bad[0]]))
     for k, idx in (("toa_flux_down", 0),):
@@ -252,7 +258,10 @@ def test_fp64_extremes_of_the_pivot_free_solve(eng, N):
     I - R^2 is nearly singular), unstable thin-layer starts (omega < 0.01 with
     tau up to 1e3, where T = I - tau0 Gpp has large negative diagonal entries
     and the solves use partial pivoting) and ordinary layers, mixed in every
-    column, against the oracle with the tiered FP64 tolerance."""
+    column, against the oracle with the tiered FP64 tolerance; the near-
+    conservative columns, whose scheme amplifies round-off beyond what the FMA
+    probe samples, are bounded by the spread of the reference's own FP64 build
+    from the oracle."""
     rng = np.random.default_rng(900 + N)
     W, L, M = 24, 12, 2 * N
     d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
@@ -274,8 +283,9 @@ def test_fp64_extremes_of_the_pivot_free_solve(eng, N):
     b.set("wavenumber_high", lo + 0.025)
     ref = oracle.solve_oracle(b, 4)
     sens = oracle.solve_oracle(b, 4, fma=True)
+    other = oracle.solve_reference(b, 4) if oracle.ref_available() else None
     res = run_device(eng, b)
-    assert_fp64_parity(b, res, ref, sens, f"extremes N={N}")
+    assert_fp64_parity(b, res, ref, sens, f"extremes N={N}", other_ref=other)
     assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_SINGULAR_PIVOT) == 0
 
 
