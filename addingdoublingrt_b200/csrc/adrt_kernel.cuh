@@ -193,6 +193,9 @@ struct Levels {
 #ifndef ADRT_PHASE_MMA
 #define ADRT_PHASE_MMA 1
 #endif
+#ifndef ADRT_PHASE_TABLE
+#define ADRT_PHASE_TABLE 1  // tuning: 0 rebuilds shared phase matrices per wavenumber
+#endif
 
 template <class Gm>
 struct UsePhaseMMA {
@@ -535,9 +538,42 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
         }
       }
     }
-    op_gemm<Gm, true>(oR, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2 (X = R row-major)
-    X.sync();
-    if constexpr (taping) {
+    int steps = -1;  // product-form steps of (I - R^2)^{-1}, or -1: Gauss-Jordan
+    if constexpr (UseNS<Gm>::value) {
+      op_gemm<Gm, true>(oR, oR, kNoMat, 0, oA, kNoMat, t);  // S = R^2 (X = R row-major)
+      X.sync();
+      steps = pivot ? -1 : ns_steps(ns_norm_inf<Gm>(Am, t));
+      if (steps < 0) {
+        op_id_plus<Gm>(oA, oA, -1.0, t);  // A = I - S (each thread its own tile)
+        X.sync();
+      }
+    } else {
+      op_gemm<Gm, true>(oR, oR, kNoMat, 1, oA, kNoMat, t);  // I - R^2 (X = R row-major)
+      X.sync();
+    }
+    if (steps == 0 && !taping) {
+      // (I - S)^{-1} = I + S to round-off: TG = T + T S
+      op_gemm<Gm, true>(oTc, oA, oTc, 0, kNoMat, oTG, t);
+    } else if (steps >= 0) {
+      // X = (I + S)(I + S^2)...: S, E and X rotate through the S buffer, the
+      // free T buffer and the TG buffer, ending outside the TG buffer
+      const bool odd = (steps & 1) || steps == 0;
+      unsigned e = oA, x = odd ? oT[cur ^ 1] : oTG, f = odd ? oTG : oT[cur ^ 1];
+      op_id_plus<Gm>(oA, x, 1.0, t);  // X_0 = I + S
+      X.sync();
+      for (int j = 0; j < steps; ++j) {
+        op_gemm<Gm, true>(e, e, kNoMat, 0, f, kNoMat, t);  // E <- E^2
+        X.sync();
+        op_gemm<Gm, true>(x, f, x, 0, e, kNoMat, t);  // X <- X + X E (into the old E)
+        X.sync();
+        const unsigned ne = f, nx = e;
+        f = x;
+        e = ne;
+        x = nx;
+      }
+      if constexpr (taping) op_s2g<Gm, GC>(x, tape + (size_t)k * Tp::STEP + Tp::OFF_AI, t);
+      op_gemm<Gm, true>(oTc, x, kNoMat, 0, kNoMat, oTG, t);  // TG = T X (column-major)
+    } else if constexpr (taping) {
       // (I - R^2)^{-1} into the free T buffer and the record, then TG = T (I - R^2)^{-1}
       Real* tk = tape + (size_t)k * Tp::STEP;
       *singular |= op_gj<Gm, GC, true>(oA, kIdentity, kNoMat, kNoMat, X.gjo(), X.redo(), t,
@@ -1390,7 +1426,7 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
           }
       }
     } else {
-      if (layout == 0 && C->ptab) {
+      if (ADRT_PHASE_TABLE && layout == 0 && C->ptab) {
         // the shared set's matrices from the call's table; the solar vectors
         // depend on this wavenumber's mu0
         const int u = from_bottom ? nL - 1 - l : l;

@@ -483,6 +483,83 @@ __device__ __noinline__ void op_gemm_lam(unsigned xt_off, unsigned y_off, unsign
   }
 }
 
+// ============================================================== (I - S)^{-1} by products
+// For the doubling's A = I - R^2 with S = R^2 small, the inverse is the
+// product form of the Neumann series, (I - S)^{-1} = (I + S)(I + S^2)(I + S^4)
+// ..., i.e. X_0 = I + S, E_0 = S^2, X_{j+1} = X_j + X_j E_{j+1} with E_{j+1} =
+// E_j^2 (the Newton-Schulz iteration X <- X (2I - A X) from X_0 = 2I - A):
+// after k steps the residual is I - A X_k = S^(2^(k+1)), of norm at most
+// ||S||^(2^(k+1)).  With ||S||_inf <= 1e-8 / 1e-4 / 1e-2 / 0.1, k = 0 / 1 / 2 /
+// 3 steps bring it below 1e-16: 1 + 2k FP64 tensor-core products against the
+// ~950 instructions of the blocked Gauss-Jordan.  Beyond 0.1 the solve stays
+// the Gauss-Jordan.  One-warp groups only (the products' buffers rotate, never
+// in place).
+#ifndef ADRT_NS_INVERSE
+#define ADRT_NS_INVERSE 1
+#endif
+template <class Gm>
+struct UseNS {
+  static constexpr bool value = ADRT_NS_INVERSE && UseMMA<Gm>::value && Gm::G == 32;
+};
+
+// ||S||_inf (the largest row sum of |S|) of a row-major smem matrix over the
+// one-warp group, every lane ending with it.
+template <class Gm>
+__device__ __forceinline__ double ns_norm_inf(const double* S, int t) {
+  static_assert(Gm::G == 32, "one-warp groups");
+  constexpr int TR = Gm::TR, TC = Gm::TC, CB = Gm::CB;
+  const Tile<Gm> tl(t);
+  double X[TR][TC];
+  if (tl.valid()) {
+    tl.load_rm(X, S);
+  } else {
+#pragma unroll
+    for (int a = 0; a < TR; ++a)
+#pragma unroll
+      for (int b = 0; b < TC; ++b) X[a][b] = 0.0;
+  }
+  double m = 0.0;
+#pragma unroll
+  for (int a = 0; a < TR; ++a) {
+    double r = 0.0;
+#pragma unroll
+    for (int b = 0; b < TC; ++b) r += fabs(X[a][b]);
+#pragma unroll
+    for (int o = 1; o < CB; o <<= 1) r += __shfl_xor_sync(0xffffffffu, r, o);  // the row's sum
+    m = fmax(m, r);
+  }
+#pragma unroll
+  for (int o = CB; o < 32; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  return m;
+}
+
+// Product-form steps for ||S||_inf = nrm, or -1 when the Gauss-Jordan serves
+// (at most ADRT_NS_MAX_STEPS: a longer chain of dependent products is no
+// shorter than the elimination).
+#ifndef ADRT_NS_MAX_STEPS
+#define ADRT_NS_MAX_STEPS 3
+#endif
+__device__ __forceinline__ int ns_steps(double nrm) {
+  const int k = !(nrm <= 0.1) ? -1 : nrm <= 1e-8 ? 0 : nrm <= 1e-4 ? 1 : nrm <= 1e-2 ? 2 : 3;
+  return k > ADRT_NS_MAX_STEPS ? -1 : k;
+}
+
+// dst = I + sign * src (row-major, tile order).
+template <class Gm>
+__device__ __noinline__ void op_id_plus(unsigned src_off, unsigned dst_off, double sign, int t) {
+  constexpr int TR = Gm::TR, TC = Gm::TC;
+  const Tile<Gm> tl(t);
+  if (!tl.valid()) return;
+  double X[TR][TC];
+  tl.load_rm(X, sp<double>(src_off));
+#pragma unroll
+  for (int a = 0; a < TR; ++a)
+#pragma unroll
+    for (int b = 0; b < TC; ++b)
+      X[a][b] = ((tl.row(a) == tl.col(b)) ? 1.0 : 0.0) + sign * X[a][b];
+  tl.store_rm(X, sp<double>(dst_off));
+}
+
 // FP64 right-solve X = B A^{-1} on the tensor cores, without pivoting.
 //
 // Every matrix the solver inverts is I - R R' with R, R' reflection matrices
@@ -518,6 +595,9 @@ struct UseGjMMA {
 // argument above covers; gj_mma then returns kGjWeakPivot and op_gj solves
 // again with partial pivoting.  Every such matrix here is I minus a product
 // of reflection matrices with O(1) entries, so the bound is absolute.
+#ifndef ADRT_GJ_FALLBACK
+#define ADRT_GJ_FALLBACK 1  // tuning: 0 leaves out the pivoted re-solve
+#endif
 constexpr double kGjMinPivot = 1e-10;
 constexpr int kGjWeakPivot = 2;  // op_gj result bit: solved again with pivoting
 
@@ -670,10 +750,9 @@ __device__ __forceinline__ int gj_mma(const double* A_rm, const double* B_rm, co
 // instead; `pivot` requests the pivoted elimination from the start.
 // OUTG: the result also into HBM (out_g), in the tile order of GO.
 template <class Gm, class GO = Gm, bool OUTG = false>
-__device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
-                                  unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
-                                  int bar, unsigned orm_off = 0xffffffffu,
-                                  typename Gm::Real* out_g = nullptr, int pivot = 0) {
+__device__ __noinline__ int gj_pivoted(unsigned a_off, unsigned b_off, unsigned bvec_off,
+                                       unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
+                                       int bar, unsigned orm_off, typename Gm::Real* out_g) {
   using Real = typename Gm::Real;
   const Real* A_rm = sp<Real>(a_off);
   const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
@@ -683,22 +762,6 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
   unsigned* red = sp<unsigned>(red_off);
   constexpr int TR = Gm::TR, TC = Gm::TC, LD = Gm::LD, NP = Gm::NP, DIM = Gm::DIM;
   constexpr int G = Gm::G;
-  int fell_back = 0;
-  if constexpr (UseGjMMA<Gm>::value) {
-    static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
-    if (!pivot) {
-      Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
-      Real* o_cm = (ocm_off == kNoMat) ? nullptr : out_cm;
-      // scratch: the output buffer, or the one matrix buffer the call names
-      Real* lbuf = o_cm ? o_cm : out_rm;
-      const int r = gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, gjbuf, t, bar, out_g);
-      if (!(r & kGjWeakPivot)) return r;
-      // A and B are intact: solve again below with partial pivoting, once
-      // every thread is done with the scratch
-      fell_back = kGjWeakPivot;
-      gsync<G>(bar);
-    }
-  }
   const Tile<Gm> tl(t);
   const bool tv = tl.valid();
   Real A[TR][TC], B[TR][TC];
@@ -830,7 +893,7 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
       }
     }
   }
-  return singular | fell_back;
+  return singular;
 }
 
 // ============================================================== FP32 on the tensor cores
@@ -1032,6 +1095,45 @@ __device__ __noinline__ int op_gj_rows(unsigned a_off, unsigned b_off, unsigned 
     return part == 0 ? gj_rows_part<Gm, 0>(A, B, out, row, bar)
                      : gj_rows_part<Gm, 1>(A, B, out, row, bar);
   }
+}
+
+// The right-solve X = B A^{-1} (arguments as gj_pivoted): FP64 orders >= 8
+// on the tensor cores without pivoting (gj_mma), and the pivoted
+// elimination (a function of its own, so that the tensor-core path keeps its
+// registers) when `pivot` asks for it, when gj_mma met a weak pivot, or for
+// the other orders and FP32.  Returns bit 0 if a pivot was exactly 0, and
+// kGjWeakPivot when the tensor-core solve met a weak pivot and the pivoted
+// elimination was used instead.
+template <class Gm, class GO = Gm, bool OUTG = false>
+__device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
+                                  unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
+                                  int bar, unsigned orm_off = 0xffffffffu,
+                                  typename Gm::Real* out_g = nullptr, int pivot = 0) {
+  using Real = typename Gm::Real;
+  if constexpr (UseGjMMA<Gm>::value) {
+    constexpr int NP = Gm::NP, LD = Gm::LD, DIM = Gm::DIM;
+    static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
+    if (!pivot || !ADRT_GJ_FALLBACK) {
+      const Real* A_rm = sp<Real>(a_off);
+      const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
+      const Real* bvec = (bvec_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(bvec_off);
+      Real* out_rm = (orm_off == kNoMat) ? nullptr : sp<Real>(orm_off);
+      Real* o_cm = (ocm_off == kNoMat) ? nullptr : sp<Real>(ocm_off);
+      // scratch: the output buffer, or the one matrix buffer the call names
+      Real* lbuf = o_cm ? o_cm : out_rm;
+      const int r = gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, sp<Real>(gj_off),
+                                         t, bar, out_g);
+      if (!ADRT_GJ_FALLBACK) return r & 1;
+      if (!(r & kGjWeakPivot)) return r;
+      // A and B are intact: solve again with partial pivoting, once every
+      // thread is done with the scratch
+      gsync<Gm::G>(bar);
+      return gj_pivoted<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar,
+                                      orm_off, out_g) | kGjWeakPivot;
+    }
+  }
+  return gj_pivoted<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar,
+                                  orm_off, out_g);
 }
 
 // Tile copies between the HBM scratch and smem.  The HBM side is in the tile

@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true", help="skip the host-entry (e2e) timing")
     p.add_argument("--no-config4", action="store_true",
                    help="skip the full config-4 uneven batch of the headline line")
+    p.add_argument("--config4-fraction", type=float, default=1.0,
+                   help="config 4 with the first ceil(f W) wavenumbers of every column "
+                        "(profiling runs; the measured workload is f = 1)")
     p.add_argument("--no-cuda-core", action="store_true",
                    help="skip the CUDA-core FP64 form (the mixed form's denominator)")
     p.add_argument("--no-reference-gpu", action="store_true",
@@ -274,7 +277,8 @@ def run_config4(args, eng, line=True):
     import torch
     from oracle import oracle
     t0 = time.perf_counter()
-    cols = workloads.config4_device(ncols=4096, seed=4, precision=_abi.PRECISION_FP64)
+    cols = workloads.config4_device(ncols=4096, seed=4, precision=_abi.PRECISION_FP64,
+                                    fraction=args.config4_fraction)
     gen_s = time.perf_counter() - t0
     total = sum(d.num_wavenumbers for d, _, _ in cols)
     saved = _abi.UnevenPlan.from_buffer_copy(eng.uneven_plan())
@@ -296,10 +300,16 @@ def run_config4(args, eng, line=True):
     def check(item):
         b, got = item
         ref = oracle.solve_oracle(b, 1, which=_abi.INTERFACE_OUTPUTS)
-        return max(oracle.norm_error(got[k], ref[k], b.L + 1) for k in got)
+        sens = oracle.solve_oracle(b, 1, which=_abi.INTERFACE_OUTPUTS, fma=True)
+        return (max(oracle.norm_error(got[k], ref[k], b.L + 1) for k in got),
+                max(oracle.norm_error(sens[k], ref[k], b.L + 1) for k in got))
 
     with cf.ThreadPoolExecutor(os.cpu_count() or 1) as ex:
-        err = max(ex.map(check, checks))
+        checked = list(ex.map(check, checks))
+    err = max(e for e, _ in checked)
+    sens_max = max(s_ for _, s_ in checked)
+    # beyond the FP64 parity tests' tolerance (1e-9 + 1000 x the FMA sensitivity)
+    beyond = sum(1 for e, s_ in checked if e > 1e-9 + 1000.0 * s_)
     sub = _prefix(cols, 0.05)
     nsub = sum(d.num_wavenumbers for d, _, _ in sub)
     tuned_ms = _time_uneven(eng, sub)
@@ -333,7 +343,9 @@ def run_config4(args, eng, line=True):
                         "warp_per_wavenumber_solves_per_s": nsub / (warp_ms * 1e-3),
                         "autotuned_over_thread_per_wavenumber": thread_ms / tuned_ms,
                         "mixed_solves_per_s": nsub / (mixed_ms * 1e-3)},
-        "oracle_max_normalized_error_one_wavenumber_per_column": err,
+        "oracle_check_one_wavenumber_per_column": {
+            "max_normalized_error": err, "max_fp64_fma_sensitivity": sens_max,
+            "beyond_1e-9_plus_1000x_sensitivity": beyond, "checked": len(checked)},
         "status": status}
     if line:
         print(json.dumps(res), flush=True)
