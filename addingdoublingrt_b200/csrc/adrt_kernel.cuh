@@ -303,20 +303,26 @@ __device__ __forceinline__ void phase_products(const double* chi, int nuse, doub
 // and, with `solar`, the solar phase vectors into D_PP / D_PM.  With PL0,
 // plm0[l] = P_l(mu0) for l < nuse (formed once per wavenumber by the same
 // recurrence) and the un-normalised solar vectors also go to D_LAM0 / D_LAM1.
-// With mats = false only the solar vectors are formed (the matrices come from
-// a table).
+// With a table (the call's shared-moment phase table row of this layer: the
+// normalised P++ then P+-) the matrices are copied from it and only the solar
+// vectors are formed.
 template <class Gm, bool PL0 = false>
 __device__ __noinline__ void build_phase(unsigned goff, unsigned tb, int t_, int bar,
                                          const double* chi, int nuse, double f, int N,
                                          const double* pl, bool solar, double mu0, double* Ppp,
                                          double* Ppm, const double* plm0 = nullptr,
-                                         bool mats = true) {
+                                         const double* table = nullptr) {
   constexpr int NP = Gm::NP, G = Gm::G;
   const Ctx<Gm> X(goff, tb, t_, bar);
   const int t = X.t;
   const double inv_1mf = (f >= 0.0) ? 1.0 / (1.0 - f) : 1.0;
   const double* wt = X.DV(D_WT);
+  const bool mats = table == nullptr;
   if (!mats) {
+    for (int e = t; e < NP * NP; e += G) {
+      Ppp[e] = __ldg(table + e);
+      Ppm[e] = __ldg(table + NP * NP + e);
+    }
   } else if constexpr (UsePhaseMMA<Gm>::value) {
     // scratch: D_PP .. D_LAM1 (4 NP doubles; the solar vectors are built below)
     phase_products<Gm, true>(chi, nuse, f, N, pl, Ppp, Ppm, NP, t, wt, X.DV(D_PP), bar);
@@ -1299,9 +1305,9 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
   const double F0 = C->solar_flux;
   const bool solar = (F0 > 0.0 && mu0 > 0.0);
   const Levels lv(slot, lmax);
-  double* Pslot = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
-  const double* Ppp = Pslot;
-  const double* Ppm = Pslot + NP * NP;
+  double* const Pslot = reinterpret_cast<double*>(slot + SLay::level_bytes(lmax));
+  const double* const Ppp = Pslot;
+  const double* const Ppm = Pslot + NP * NP;
   Real* recs = reinterpret_cast<Real*>(slot + SLay::level_bytes(lmax) + SLay::phase_bytes());
   const double* chi_base = C->moments;
   const double Bs = X.sc[S_BS], Btop = X.sc[S_BTOP];
@@ -1426,25 +1432,20 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
           }
       }
     } else {
-      if (ADRT_PHASE_TABLE && layout == 0 && C->ptab) {
-        // the shared set's matrices from the call's table; the solar vectors
-        // depend on this wavenumber's mu0
-        const int u = from_bottom ? nL - 1 - l : l;
-        Ppp = C->ptab + (size_t)u * 2 * NP * NP;
-        Ppm = Ppp + NP * NP;
-        if (solar) {
-          int nuse;
-          double f;
-          const double* chi = moments(l, nuse, f);
-          build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0,
-                          nullptr, nullptr, nullptr, false);
-        }
-      } else if (layout != 1) {
+      if (layout != 1) {
+        // moments per layer; a set shared by every wavenumber (layout 0) has
+        // its matrices in the call's table, copied into the slot (the doubling
+        // reads them at a fixed place), and only the solar vectors, which
+        // depend on this wavenumber's mu0, are formed here
         int nuse;
         double f;
         const double* chi = moments(l, nuse, f);
+        const double* table =
+            (ADRT_PHASE_TABLE && layout == 0 && C->ptab)
+                ? C->ptab + (size_t)(from_bottom ? nL - 1 - l : l) * 2 * NP * NP
+                : nullptr;
         build_phase<Gm>(X.goff, X.tb, t, X.bar, chi, nuse, f, N, C->quad.pl, solar, mu0, Pslot,
-                        Pslot + NP * NP);
+                        Pslot + NP * NP, nullptr, table);
       }
       if constexpr (MODE == MODE_FP64) {
         Real* tape_l = nullptr;

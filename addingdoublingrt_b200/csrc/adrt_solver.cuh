@@ -493,9 +493,12 @@ __device__ __noinline__ void op_gemm_lam(unsigned xt_off, unsigned y_off, unsign
 // 3 steps bring it below 1e-16: 1 + 2k FP64 tensor-core products against the
 // ~950 instructions of the blocked Gauss-Jordan.  Beyond 0.1 the solve stays
 // the Gauss-Jordan.  One-warp groups only (the products' buffers rotate, never
-// in place).
+// in place).  Off by default: on config 2 (N = 16) and config 5 the solve
+// takes the same time with it as without (3 steps at most) and longer with
+// fewer steps allowed, since the norm and the extra products cost what the
+// shorter elimination saves; it is kept as a tuning option.
 #ifndef ADRT_NS_INVERSE
-#define ADRT_NS_INVERSE 1
+#define ADRT_NS_INVERSE 0
 #endif
 template <class Gm>
 struct UseNS {
