@@ -193,6 +193,9 @@ struct Levels {
 #ifndef ADRT_PHASE_MMA
 #define ADRT_PHASE_MMA 1
 #endif
+#ifndef ADRT_UNSTABLE_PIVOT
+#define ADRT_UNSTABLE_PIVOT 1  // tuning: 0 leaves unstable starts to the weak-pivot check
+#endif
 #ifndef ADRT_PHASE_TABLE
 #define ADRT_PHASE_TABLE 1  // tuning: 0 rebuilds shared phase matrices per wavenumber
 #endif
@@ -469,7 +472,7 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   // cosine: T = I - tau0 Gpp with large negative diagonal entries) leaves
   // I - R^2 outside the diagonally dominant class the pivot-free solve is
   // argued for; its solves use the reference's partial pivoting.
-  const int pivot = tau0 > 0.5 * mu[0];
+  const int pivot = ADRT_UNSTABLE_PIVOT && tau0 > 0.5 * mu[0];
   using GC = Geo<NP, Real>;  // record order
   using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);

@@ -573,9 +573,15 @@ def job_rate(units_per_rank: int, world: int, seconds: float) -> float:
     return units_per_rank * world / seconds
 
 
-def rank_seed(rank: int) -> int:
-    """Each rank solves its own shard of synthetic wavenumbers."""
-    return 2 + rank
+def rank_batch(W: int, rank: int, world: int, precision):
+    """This rank's config-2 wavenumbers: with one rank the W-wavenumber batch;
+    with several, a cost-balanced contiguous range of one W x world batch
+    (weak scaling: about W wavenumbers of work per rank, no exchange)."""
+    if world == 1:
+        return workloads.config2(W=W, precision=precision)
+    from addingdoublingrt_b200 import shard
+    whole = workloads.config2(W=W * world, precision=precision)
+    return shard.shard(whole, rank, world)[2]
 
 
 # ---------------------------------------------------------------- engine arm
@@ -620,8 +626,7 @@ def main():
     precisions = [args.only] if args.only else ["fp64", "mixed"]
     for pname in precisions:
         prec = _abi.PRECISION_FP64 if pname == "fp64" else _abi.PRECISION_MIXED
-        # weak scaling: every rank solves its own batch of the full size
-        b = workloads.config2(W=args.wavenumbers, seed=rank_seed(rank), precision=prec)
+        b = rank_batch(args.wavenumbers, rank, world, prec)
         di = to_device(b)
         do = alloc_device_outputs(b, which=_abi.INTERFACE_OUTPUTS)
         eng.reserve(b.desc)
@@ -649,8 +654,8 @@ def main():
     acc = {}
     if rank == 0 and not args.no_check:
         from oracle import oracle
-        idx = np.arange(0, args.wavenumbers, max(1, args.wavenumbers // 200))
         b0 = results[precisions[0]]["batch"]
+        idx = np.arange(0, b0.W, max(1, b0.W // 200))
         ref = oracle.solve_oracle(b0.subset(idx), os.cpu_count() or 1,
                                   which=_abi.INTERFACE_OUTPUTS)
         L = b0.L
@@ -746,7 +751,9 @@ def main():
             "config": {"workload": WORKLOAD, "precision": pname,
                        "wavenumbers_per_gpu": args.wavenumbers,
                        "l2": "inputs 190 MB > 126 MB L2, no flush",
-                       "parallelism": f"replicas x{world} (wavenumber shards)"},
+                       "parallelism": (f"wavenumber shards x{world}: cost-balanced contiguous "
+                                       "ranges of one batch, no exchange") if world > 1
+                                      else "one GPU"},
             **{f"{p}_solves_per_s": job_rate(args.wavenumbers, world, results[p]["ms"] * 1e-3)
                for p in precisions},
             "mixed_over_fp64": (results["fp64"]["ms"] / results["mixed"]["ms"]
