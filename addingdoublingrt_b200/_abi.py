@@ -20,6 +20,9 @@ ADRT_FLAG_SINGULAR_PIVOT = 1
 ADRT_FLAG_NONFINITE = 2
 ADRT_FLAG_BAD_INPUT = 4
 ADRT_FLAG_PIVOT_FALLBACK = 8
+ADRT_FLAG_PIVOT_UNRESOLVED = 16
+PIVOTING_TENSOR_CORE = 0
+PIVOTING_PARTIAL = 1
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1

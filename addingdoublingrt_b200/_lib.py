@@ -41,6 +41,7 @@ EXPORTS = (
     "adrt_planck_band_deriv",
     "adrt_band_integrate",
     "adrt_engine_set_adjoint_mode",
+    "adrt_engine_set_pivoting",
     "adrt_engine_device",
     "adrt_engine_autotune_uneven",
     "adrt_engine_set_uneven_plan",
@@ -95,6 +96,7 @@ def load(build_if_missing: bool = False) -> C.CDLL:
         lib.adrt_solve_batch_raw.argtypes = [C.c_void_p, P(_abi.BatchDesc),
                                              P(_abi.RawInputs), P(_abi.OutputsF32), C.c_void_p]
         lib.adrt_engine_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
+        lib.adrt_engine_set_pivoting.argtypes = [C.c_void_p, C.c_int]
         lib.adrt_engine_device.argtypes = [C.c_void_p, P(C.c_int)]
         lib.adrt_engine_autotune_uneven.argtypes = [C.c_void_p, P(_abi.ColumnDesc), C.c_int,
                                                     C.c_void_p, P(_abi.UnevenPlan)]

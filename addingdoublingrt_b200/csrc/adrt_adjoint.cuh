@@ -426,9 +426,21 @@ __device__ __noinline__ void doubling_adjoint(unsigned goff, unsigned tb, int t_
   // 1. the record of this layer's chain: taped by the forward pass, or the
   //    chain again now (buffers 0..5 and V_*)
   const int nn = num_doublings(tau, om > 1.0 ? 1.0 : om);
-  if (recompute)
+  if (recompute) {
+    int fl = 0;
     doubling<Gm, true>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
-                       singular, tape);
+                       &fl, tape);
+    if (ADRT_GJ_FALLBACK && (fl & kGjWeakPivot)) {  // the chain again, pivoted
+      if (t == 0) X.sc[S_PIVALL] = 1.0;
+      X.sync();
+      fl = kGjWeakPivot;
+      doubling<Gm, true>(goff, tb, t_, bar, tau, om, Bt, Bb, tcum, N, solar, F0, mu0, Ppp, Ppm,
+                         &fl, tape);
+      X.sync();
+      if (t == 0) X.sc[S_PIVALL] = 0.0;
+    }
+    *singular |= fl;
+  }
   X.sync();
   const double* mu = X.DV(D_MU);
   const double* wt = X.DV(D_WT);
@@ -1094,7 +1106,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
     if (scat && cb) {  // b_rhs = M^{-T} bx with M = I - R Rb, as b_rhs^T = bx^T M^{-1}
       op_gemm<Gm>(X.mo(J_Rc), X.mo(J_TGR), kNoMat, 1, X.mo(J_T1), kNoMat, t);
       X.sync();
-      singular |= op_gj<Gm>(X.mo(J_T1), kNoMat, vo(A_Y), X.mo(J_T2), X.gjo(), X.redo(), t, X.bar);
+      singular |= op_gj_safe<Gm>(X.mo(J_T1), kNoMat, vo(A_Y), X.mo(J_T2), X.gjo(), X.redo(), t, X.bar);
       X.sync();
       brhs = X.m(J_T2);
       bstride = LD;
@@ -1200,7 +1212,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
       // ---- general: A1 = I - Rb R, D1 = T A1^{-1}
       op_gemm<Gm>(X.mo(J_TGc), X.mo(J_R), kNoMat, 1, X.mo(J_bR1), X.mo(J_bR1c), t);
       X.sync();
-      singular |= op_gj<Gm>(X.mo(J_bR1), X.mo(J_TG), kNoMat, X.mo(J_bT1c), X.gjo(), X.redo(), t,
+      singular |= op_gj_safe<Gm>(X.mo(J_bR1), X.mo(J_TG), kNoMat, X.mo(J_bT1c), X.gjo(), X.redo(), t,
                             X.bar, X.mo(J_bT1));
       X.sync();
       op_gemm<Gm>(X.mo(J_TGc), X.mo(J_TG), kNoMat, 0, X.mo(J_W), X.mo(J_Ac), t);   // Q = Rb T
@@ -1231,7 +1243,7 @@ __device__ __noinline__ void wav_adjoint(unsigned goff, unsigned tb, int t_, int
                   kNoMat, 0.0, kNoMat, kNoMat, 0.0, t);
       X.sync();
       // W = dD1 A1^{-T}
-      singular |= op_gj<Gm>(X.mo(J_bR1c), X.mo(J_bTG), kNoMat, kNoMat, X.gjo(), X.redo(), t,
+      singular |= op_gj_safe<Gm>(X.mo(J_bR1c), X.mo(J_bTG), kNoMat, kNoMat, X.gjo(), X.redo(), t,
                             X.bar, X.mo(J_T2));
       X.sync();
       // G1 = D1^T W (= -dA1);  dT = F^T dRb + W + b_rhs Id^T
@@ -1602,12 +1614,14 @@ __global__ void __launch_bounds__(128, 3) tape_kernel(SolveParams P, ColumnDev c
       const unsigned long long base = atomicAdd(AD.pool_used, n);
       toff[nL] = (base + n <= (unsigned long long)AD.pool_cap) ? (long long)base : -1ll;
     }
+    if (P.pivot_all && t == 0)
+      sp<double>(goff + (unsigned)CommonLayout<NP>::misc + 48)[S_PIVALL] = 1.0;
     gsync<G>(bar);
     const long long base = toff[nL];
-    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, st, lmax, P.status,
-                            reinterpret_cast<double*>(st + WS::fwd(lmax)),
-                            base >= 0 ? AD.pool + base : nullptr, base >= 0 ? (long long)need : 0,
-                            toff);
+    wav_body_checked<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, st, lmax, P.status,
+                                    reinterpret_cast<double*>(st + WS::fwd(lmax)),
+                                    base >= 0 ? AD.pool + base : nullptr,
+                                    base >= 0 ? (long long)need : 0, toff);
   }
 }
 

@@ -105,9 +105,23 @@ struct Kern {
     }
     return cached;
   }
+  // Both passes: the solve, then the re-solve of the wavenumbers it listed
+  // (a launch whose groups find an empty list and return at once when none
+  // met a weak pivot).
+  // (p.redo_pass already set: the re-solve pass alone, over the list as it is)
   static int launch(const SolveParams& p, const ColumnDev& c0, int grid, cudaStream_t s) {
-    solve_kernel<NP, KIND><<<grid, kThreads, smem(), s>>>(p, c0);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = cudaSuccess;
+    if (p.redo && !p.redo_pass) e = cudaMemsetAsync(p.redo, 0, 2 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess && !p.redo_pass) {
+      solve_kernel<NP, KIND><<<grid, kThreads, smem(), s>>>(p, c0);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && p.redo) {
+      SolveParams q = p;
+      q.redo_pass = 1;
+      solve_kernel<NP, KIND><<<grid, kThreads, smem(), s>>>(q, c0);
+      e = cudaGetLastError();
+    }
     if (e != cudaSuccess) return fail(ADRT_ERR_CUDA, "solve kernel launch: %s", cudaGetErrorString(e));
     return ADRT_OK;
   }
@@ -152,6 +166,9 @@ KernInfo pick(int n, int precision) {
 // up to four chunks so that the copies overlap the solves; a chunk then keeps
 // every resident thread group busy for several wavenumbers.
 constexpr size_t kHostChunkMin = 8192;
+// Room of the re-solve list: wavenumbers of one launch whose pivot-free solve
+// met a weak pivot (none on physical inputs; beyond it ADRT_FLAG_PIVOT_UNRESOLVED).
+constexpr long long kRedoCap = 65536;
 
 struct adrt_engine {
   int device = 0;
@@ -164,6 +181,7 @@ struct adrt_engine {
   size_t scratch_bytes = 0;
   unsigned long long* counter = nullptr;
   unsigned int* status = nullptr;
+  unsigned long long* redo = nullptr;  // re-solve list (SolveParams::redo), kRedoCap entries
   ColumnDev* d_cols = nullptr;
   size_t d_cols_cap = 0;
   ColumnDev* h_cols = nullptr;       // pinned staging of the column table
@@ -188,6 +206,7 @@ struct adrt_engine {
   std::mutex hmu;  // one host-entry call at a time per engine
   std::mutex mu;
   int adjoint_mode = ADRT_ADJOINT_RECORD;
+  int pivoting = ADRT_PIVOTING_TENSOR_CORE;
   // uneven batches: warp mapping for every order, occupancy-limited grid,
   // longest columns first (adrt_engine_autotune_uneven replaces it)
   adrt_uneven_plan plan{{ADRT_MAPPING_WARP, ADRT_MAPPING_WARP, ADRT_MAPPING_WARP}, 0, 1,
@@ -491,9 +510,11 @@ int phase_table(adrt_engine* e, ColumnDev& c, cudaStream_t s) {
   return ADRT_OK;
 }
 
-// adrt_solve_batch after argument checks, with e->mu held.
+// adrt_solve_batch after argument checks, with e->mu held.  With `relist`,
+// only the re-solve pass runs, over those wavenumbers.
 int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in,
-                 const adrt_outputs* out, cudaStream_t s, const adrt_raw_inputs* raw = nullptr) {
+                 const adrt_outputs* out, cudaStream_t s, const adrt_raw_inputs* raw = nullptr,
+                 const std::vector<unsigned long long>* relist = nullptr) {
   int rc;
   if ((rc = set_device(e))) return rc;
   e->last_stream = s;
@@ -521,10 +542,19 @@ int solve_locked(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   p.slot_bytes = sb;
   p.nslots = grid * k.groups;
   p.max_layers = d->num_layers;
+  p.redo = e->redo;
+  p.redo_cap = kRedoCap;
+  p.pivot_all = e->pivoting == ADRT_PIVOTING_PARTIAL;
   const int need_blocks = (d->num_wavenumbers + k.groups - 1) / k.groups;
   grid = std::min(grid, need_blocks);
   if (!raw && d->moment_layout == ADRT_MOMENTS_SHARED && (rc = phase_table(e, c0, s))) return rc;
   CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+  if (relist) {
+    CUDA_TRY(cudaStreamSynchronize(s));
+    CUDA_TRY(cudaMemcpy(e->redo, relist->data(), relist->size() * sizeof(unsigned long long),
+                        cudaMemcpyHostToDevice));
+    p.redo_pass = 1;
+  }
   return k.launch(p, c0, grid, s);
 }
 
@@ -702,7 +732,14 @@ int uneven_locked(adrt_engine* e, std::vector<UnevenColumn>& cv, cudaStream_t s,
     p.slot_bytes = sb;
     p.nslots = (int)blocks * 4;
     p.max_layers = lmax[0];
+    p.redo = e->redo;
+    p.redo_cap = kRedoCap;
+    p.pivot_all = e->pivoting == ADRT_PIVOTING_PARTIAL;
     CUDA_TRY(cudaMemsetAsync(e->counter, 0, sizeof(unsigned long long), s));
+    CUDA_TRY(cudaMemsetAsync(e->redo, 0, 2 * sizeof(unsigned long long), s));
+    solve_kernel_multi<0><<<(int)blocks, 128, smem, s>>>(p);
+    CUDA_TRY(cudaGetLastError());
+    p.redo_pass = 1;  // the listed wavenumbers again, pivoted
     solve_kernel_multi<0><<<(int)blocks, 128, smem, s>>>(p);
     CUDA_TRY(cudaGetLastError());
   }
@@ -748,6 +785,9 @@ int uneven_locked(adrt_engine* e, std::vector<UnevenColumn>& cv, cudaStream_t s,
     p.slot_bytes = sb;
     p.nslots = grid * k.groups;
     p.max_layers = lmax[4];
+    p.redo = e->redo;
+    p.redo_cap = kRedoCap;
+    p.pivot_all = e->pivoting == ADRT_PIVOTING_PARTIAL;
     grid = (int)std::min<long long>(grid, totals[4]);
     CUDA_TRY(cudaMemsetAsync(e->counter + 1, 0, sizeof(unsigned long long), s));
     ColumnDev c0 = e->h_cols[first[4]];
@@ -822,7 +862,8 @@ int adrt_engine_create(const adrt_engine_opts* opts, adrt_engine** out) {
     return rc;
   }
   cudaDeviceGetAttribute(&e->num_sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaMalloc(&e->counter, 64) != cudaSuccess || cudaMalloc(&e->status, 64) != cudaSuccess) {
+  if (cudaMalloc(&e->counter, 64) != cudaSuccess || cudaMalloc(&e->status, 64) != cudaSuccess ||
+      cudaMalloc(&e->redo, sizeof(unsigned long long) * (2 + kRedoCap)) != cudaSuccess) {
     delete e;
     return fail(ADRT_ERR_OUT_OF_MEMORY, "engine allocation failed");
   }
@@ -838,6 +879,7 @@ int adrt_engine_destroy(adrt_engine* e) {
   cudaFree(e->scratch);
   cudaFree(e->counter);
   cudaFree(e->status);
+  cudaFree(e->redo);
   cudaFree(e->d_cols);
   if (e->h_cols) cudaFreeHost(e->h_cols);
   if (e->cols_copied) cudaEventDestroy(e->cols_copied);
@@ -1108,6 +1150,38 @@ int adrt_engine_set_adjoint_mode(adrt_engine* e, int mode) {
   return ADRT_OK;
 }
 
+int adrt_engine_set_pivoting(adrt_engine* e, int mode) {
+  if (!e) return fail(ADRT_ERR_INVALID_ARGUMENT, "null engine");
+  if (mode != ADRT_PIVOTING_TENSOR_CORE && mode != ADRT_PIVOTING_PARTIAL)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "unknown pivoting mode %d", mode);
+  std::lock_guard<std::mutex> lk(e->mu);
+  e->pivoting = mode;
+  return ADRT_OK;
+}
+
+// Hidden helper (not in the public header): the re-solve pass alone over the
+// wavenumbers `tasks` of a batch, as if the solve had listed them (the list
+// mechanism is otherwise reached only by a weak pivot).  Synchronous.
+extern "C" int adrt_internal_resolve_listed(adrt_engine* e, const adrt_batch_desc* d,
+                                            const adrt_inputs* in, const adrt_outputs* out,
+                                            const long long* tasks, int ntasks) {
+  if (!e || !d || !in || !out || !tasks || ntasks < 1 || ntasks > kRedoCap)
+    return fail(ADRT_ERR_INVALID_ARGUMENT, "bad re-solve list");
+  int rc;
+  if ((rc = adrt_internal_check_batch(d, in))) return rc;
+  std::vector<unsigned long long> list(2 + ntasks, 0ull);
+  list[0] = (unsigned long long)ntasks;
+  for (int i = 0; i < ntasks; ++i) {
+    if (tasks[i] < 0 || tasks[i] >= d->num_wavenumbers)
+      return fail(ADRT_ERR_INVALID_ARGUMENT, "task %lld outside the batch", tasks[i]);
+    list[2 + i] = (unsigned long long)tasks[i];
+  }
+  std::lock_guard<std::mutex> lk(e->mu);
+  if ((rc = solve_locked(e, d, in, out, nullptr, nullptr, &list))) return rc;
+  CUDA_TRY(cudaStreamSynchronize(nullptr));
+  return ADRT_OK;
+}
+
 int adrt_band_integrate(adrt_engine* e, const double* spectrum, const double* weight,
                         long long num_wavenumbers, const long long* offsets, int nchannels,
                         double* out, void* stream_ptr) {
@@ -1258,6 +1332,7 @@ int adrt_adjoint(adrt_engine* e, const adrt_batch_desc* d, const adrt_inputs* in
   p.ncols = 1;
   p.counter = e->counter;
   p.status = e->status;
+  p.pivot_all = e->pivoting == ADRT_PIVOTING_PARTIAL;  // the taping forward's solves
   p.scratch = e->adj_scratch;
   p.slot_bytes = k.scr;
   p.max_layers = L;

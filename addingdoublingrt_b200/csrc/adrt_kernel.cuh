@@ -471,8 +471,10 @@ __device__ __noinline__ int doubling(unsigned goff, unsigned tb, int t_, int bar
   // An unstable first-order start (tau0 beyond half the smallest quadrature
   // cosine: T = I - tau0 Gpp with large negative diagonal entries) leaves
   // I - R^2 outside the diagonally dominant class the pivot-free solve is
-  // argued for; its solves use the reference's partial pivoting.
-  const int pivot = ADRT_UNSTABLE_PIVOT && tau0 > 0.5 * mu[0];
+  // argued for; its solves use the reference's partial pivoting, as every
+  // solve does in the re-solve of a wavenumber that met a weak pivot (the
+  // group's S_PIVALL flag: the re-solve pass, or wav_body_checked).
+  const int pivot = X.sc[S_PIVALL] != 0.0 || (ADRT_UNSTABLE_PIVOT && tau0 > 0.5 * mu[0]);
   using GC = Geo<NP, Real>;  // record order
   using Tp = TapeLayout<Gm>;
   Real* Rrm = sp<Real>(oR);
@@ -1238,6 +1240,10 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
         om = om * (1.0 - f) / (1.0 - of);
       }
     }
+    // the reference's rule would take more doublings than the device's bound
+    // (tau of order 1e15 and beyond): the layer is solved at the bound, flagged
+    if (tau > 0.0 && om > 0.0 && tau >= ldexp(1.0, kMaxDoublings + 1 - ipow0(om > 1.0 ? 1.0 : om)))
+      bad = 1;
     lv.tau[l] = tau;
     lv.om[l] = om;
     double fl = 0.0;
@@ -1278,6 +1284,7 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
     }
     X.sc[S_BS] = Bs;
     X.sc[S_BTOP] = Btop;
+    X.sc[S_PIVALL] = 0.0;
   }
   X.sync();
   return any != 0u;
@@ -1289,10 +1296,10 @@ __device__ __noinline__ int wav_prologue(unsigned goff, int t_, int bar, int w, 
 // MODE picks the doubling form per layer (see the top of this file); tbF is
 // the FP32 region of a class-D group.
 template <class Gm, int MODE>
-__device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, int t_, int bar,
-                                      int w, char* slot, int lmax, unsigned* status,
-                                      double* ivec = nullptr, double* tape_all = nullptr,
-                                      long long tape_cap = 0, long long* toff = nullptr) {
+__device__ __noinline__ int wav_body(unsigned goff, unsigned tb, unsigned tbF, int t_, int bar,
+                                     int w, char* slot, int lmax, unsigned* status,
+                                     double* ivec = nullptr, double* tape_all = nullptr,
+                                     long long tape_cap = 0, long long* toff = nullptr) {
   using Real = typename Gm::Real;
   const Ctx<Gm> X(goff, tb, t_, bar);
   using SLay = SlotLayout<Gm>;
@@ -1549,7 +1556,8 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
       }
       op_gemm<Gm, true>(oRb, X.mo(0), kNoMat, 1, oSp, kNoMat, t);  // A1 = I - R_b R
       X.sync();
-      singular |= op_gj<Gm>(oSp, oTl, kNoMat, oD1, X.gjo(), X.redo(), t, X.bar);  // D1 (cm)
+      singular |= op_gj<Gm>(oSp, oTl, kNoMat, oD1, X.gjo(), X.redo(), t, X.bar, kNoMat, nullptr,
+                            X.sc[S_PIVALL] != 0.0);  // D1 (cm)
       X.sync();
       if (X.warp == 0) {
         const Real* vv[1] = {X.V(V_TMP)};
@@ -1623,7 +1631,8 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
       // (I - R R_base) x = rhs, as x^T = rhs^T (I - R R_base)^{-T}
       op_gemm<Gm>(X.mo(2), X.mo(1), kNoMat, 1, X.mo(3), kNoMat, t);  // (I - R R_base)^T
       X.sync();
-      singular |= op_gj<Gm>(X.mo(3), kNoMat, X.vo(V_RHS), X.mo(4), X.gjo(), X.redo(), t, X.bar);
+      singular |= op_gj<Gm>(X.mo(3), kNoMat, X.vo(V_RHS), X.mo(4), X.gjo(), X.redo(), t, X.bar,
+                            kNoMat, nullptr, X.sc[S_PIVALL] != 0.0);
       X.sync();
       xsol = X.m(4);
       xstride = Gm::LD;
@@ -1650,9 +1659,72 @@ __device__ __noinline__ void wav_body(unsigned goff, unsigned tb, unsigned tbF, 
   }
   if (singular && t == 0) atomicOr(status, status_bits(singular));
   X.sync();
+  return singular;
+}
+
+// The wavenumber with the tensor-core solves, and once more at once with
+// partial pivoting in every solve (the group's S_PIVALL flag) when one of
+// them met a weak pivot; its status then carries the pivoted re-solve bit.
+// The body only reads what the prologue left, so the second pass starts from
+// the same state.  For the adjoint's taping forward; the forward kernels list
+// such wavenumbers for a second launch instead, which keeps a second call of
+// the body (and its registers) out of them.
+template <class Gm, int MODE>
+__device__ __forceinline__ void wav_body_checked(unsigned goff, unsigned tb, unsigned tbF, int t,
+                                                 int bar, int w, char* slot, int lmax,
+                                                 unsigned* status, double* ivec = nullptr,
+                                                 double* tape_all = nullptr,
+                                                 long long tape_cap = 0,
+                                                 long long* toff = nullptr) {
+  const int fl = wav_body<Gm, MODE>(goff, tb, tbF, t, bar, w, slot, lmax, status, ivec, tape_all,
+                                    tape_cap, toff);
+  if (ADRT_GJ_FALLBACK && (fl & kGjWeakPivot)) {
+    const Ctx<Gm> X(goff, tb, t, bar);
+    if (t == 0) X.sc[S_PIVALL] = 1.0;  // the next prologue clears it
+    X.sync();
+    wav_body<Gm, MODE>(goff, tb, tbF, t, bar, w, slot, lmax, status, ivec, tape_all, tape_cap,
+                       toff);
+  }
 }
 
 // ------------------------------------------------------------- persistent kernel
+// ------------------------------------------------------------- re-solve pass
+// A launch's tasks: its own, or in the re-solve pass the ones the first pass
+// listed (at most redo_cap), each taken from that pass's work counter.
+__device__ __forceinline__ long long pass_tasks(const SolveParams& P) {
+  if (!P.redo_pass) return P.ntasks;
+  const long long n = (long long)P.redo[0];
+  return n < P.redo_cap ? n : P.redo_cap;
+}
+__device__ __forceinline__ unsigned long long* pass_counter(const SolveParams& P) {
+  return P.redo_pass ? P.redo + 1 : P.counter;
+}
+__device__ __forceinline__ long long pass_task(const SolveParams& P, long long i) {
+  return P.redo_pass ? (long long)P.redo[2 + i] : i;
+}
+// In the re-solve pass (or with ADRT_PIVOTING_PARTIAL), after the prologue:
+// every solve of the wavenumber with partial pivoting (the group's S_PIVALL
+// flag; the next prologue clears it).
+template <int G>
+__device__ __forceinline__ void pass_pivot_all(const SolveParams& P, unsigned goff, int t,
+                                               int bar, int np_common_misc) {
+  if (!P.redo_pass && !P.pivot_all) return;
+  if (t == 0) sp<double>(goff + (unsigned)np_common_misc + 48)[S_PIVALL] = 1.0;
+  gsync<G>(bar);
+}
+// In the first pass, after the body: a wavenumber whose pivot-free solve met
+// a weak pivot goes on the re-solve list (ADRT_FLAG_PIVOT_UNRESOLVED when
+// the list is full: that wavenumber keeps the pivot-free result).
+__device__ __forceinline__ void pass_list_weak(const SolveParams& P, int flags, long long task,
+                                               int t) {
+  if (!ADRT_GJ_FALLBACK || P.redo_pass || !(flags & kGjWeakPivot) || t != 0) return;
+  const unsigned long long k = P.redo ? atomicAdd(P.redo, 1ull) : ~0ull;
+  if (P.redo && k < (unsigned long long)P.redo_cap)
+    P.redo[2 + k] = (unsigned long long)task;
+  else
+    atomicOr(P.status, 16u);
+}
+
 template <int NP, int KIND>
 __global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev col0) {
   using GD = Geo<NP, double>;
@@ -1673,19 +1745,22 @@ __global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev 
   if (P.ncols <= 1 && t == 0) *colp = col0;
   long long* task_s = sp<long long>(goff + CommonLayout<NP>::misc + 32);
   int cur_col = -1;
+  const long long ntasks = pass_tasks(P);
+  unsigned long long* const counter = pass_counter(P);
   for (;;) {
     long long task;
     if constexpr (G == 32) {
       unsigned long long v = 0;
-      if (t == 0) v = atomicAdd(P.counter, 1ull);
+      if (t == 0) v = atomicAdd(counter, 1ull);
       task = (long long)__shfl_sync(0xffffffffu, v, 0);
     } else {
       gsync<G>(bar);
-      if (t == 0) *task_s = (long long)atomicAdd(P.counter, 1ull);
+      if (t == 0) *task_s = (long long)atomicAdd(counter, 1ull);
       gsync<G>(bar);
       task = *task_s;
     }
-    if (task >= P.ntasks) break;
+    if (task >= ntasks) break;
+    task = pass_task(P, task);
     int w = (int)task;
     if (P.ncols > 1) {
       int lo = 0, hi = P.ncols - 1;
@@ -1703,16 +1778,19 @@ __global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev 
     gsync<G>(bar);
     const int any =
         wav_prologue<NP>(goff, t, bar, w, sl, P.max_layers, P.status, KIND == KIND_MIXED);
+    pass_pivot_all<G>(P, goff, t, bar, (int)CommonLayout<NP>::misc);
+    int fl = 0;
     if constexpr (KIND == KIND_FP64) {
-      wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+      fl = wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else if (colp->precision == 0) {  // an FP64 column of an uneven batch
-      wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+      fl = wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else if (!any && !ADRT_MIX_FORCE_D) {
-      wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
+      fl = wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, P.max_layers, P.status);
     } else {
-      wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,
-                               P.max_layers, P.status);
+      fl = wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl,
+                                    P.max_layers, P.status);
     }
+    pass_list_weak(P, fl, task, t);
   }
 }
 
@@ -1722,21 +1800,22 @@ __global__ void __launch_bounds__(128, 3) solve_kernel(SolveParams P, ColumnDev 
 // is dispatched on its column's padded order and precision.  The group's
 // shared memory and slot are sized for the largest order.
 template <int NP>
-__device__ __noinline__ void multi_task(unsigned goff, int t, int bar, int w, char* sl, int lmax,
-                                        unsigned* status, int precision) {
+__device__ __noinline__ int multi_task(unsigned goff, int t, int bar, int w, char* sl, int lmax,
+                                       unsigned* status, int precision, int pivot_all) {
   using GD = Geo<NP, double>;
   using GF = Geo<NP, float>;
   using GL = GroupLayout<NP, KIND_MIXED>;
   const unsigned tb = goff + (unsigned)CommonLayout<NP>::bytes;
   const int any = wav_prologue<NP>(goff, t, bar, w, sl, lmax, status, precision != 0);
-  if (precision == 0) {
-    wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, lmax, status);
-  } else if (!any && !ADRT_MIX_FORCE_D) {
-    wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, lmax, status);
-  } else {
-    wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl, lmax,
-                             status);
+  if (pivot_all) {  // the re-solve pass
+    if (t == 0) sp<double>(goff + (unsigned)CommonLayout<NP>::misc + 48)[S_PIVALL] = 1.0;
+    __syncwarp();
   }
+  if (precision == 0) return wav_body<GD, MODE_FP64>(goff, tb, 0u, t, bar, w, sl, lmax, status);
+  if (!any && !ADRT_MIX_FORCE_D)
+    return wav_body<GF, MODE_MIX_S>(goff, tb, 0u, t, bar, w, sl, lmax, status);
+  return wav_body<GD, MODE_MIX_D>(goff, tb, tb + (unsigned)GL::lamF_in_D, t, bar, w, sl, lmax,
+                                  status);
 }
 
 constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
@@ -1758,11 +1837,14 @@ __global__ void __launch_bounds__(128) solve_kernel_multi(SolveParams P) {
   __syncwarp();
   ColumnDev* colp = sp<ColumnDev>(goff);
   int cur_col = -1;
+  const long long ntasks = pass_tasks(P);
+  unsigned long long* const counter = pass_counter(P);
   for (;;) {
     unsigned long long v = 0;
-    if (t == 0) v = atomicAdd(P.counter, 1ull);
-    const long long task = (long long)__shfl_sync(0xffffffffu, v, 0);
-    if (task >= P.ntasks) break;
+    if (t == 0) v = atomicAdd(counter, 1ull);
+    long long task = (long long)__shfl_sync(0xffffffffu, v, 0);
+    if (task >= ntasks) break;
+    task = pass_task(P, task);
     int lo = 0, hi = P.ncols - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -1776,13 +1858,18 @@ __global__ void __launch_bounds__(128) solve_kernel_multi(SolveParams P) {
     __syncwarp();
     const int w = (int)(task - colp->task_begin);
     const int np = colp->NP, prec = colp->precision;
+    int fl;
     if (np <= 4) {
-      multi_task<4>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
+      fl = multi_task<4>(goff, t, bar, w, sl, P.max_layers, P.status, prec,
+                         P.redo_pass | P.pivot_all);
     } else if (np <= 8) {
-      multi_task<8>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
+      fl = multi_task<8>(goff, t, bar, w, sl, P.max_layers, P.status, prec,
+                         P.redo_pass | P.pivot_all);
     } else {
-      multi_task<16>(goff, t, bar, w, sl, P.max_layers, P.status, prec);
+      fl = multi_task<16>(goff, t, bar, w, sl, P.max_layers, P.status, prec,
+                         P.redo_pass | P.pivot_all);
     }
+    pass_list_weak(P, fl, task, t);
   }
 }
 

@@ -57,7 +57,12 @@ constexpr size_t quad_offset(int n) {
   for (int m = 2; m < n; ++m) off += (quad_doubles(m) * sizeof(double) + 255) & ~size_t(255);
   return off;
 }
-constexpr size_t kSlotsOffset = quad_offset(kMaxN + 1);
+// The re-solve list (SolveParams::redo): two counters and kRedoCap task
+// indices after the quadrature tables, then the wavenumber slots.
+constexpr long long kRedoCap = 4096;
+constexpr size_t kRedoOffset = quad_offset(kMaxN + 1);
+constexpr size_t kSlotsOffset =
+    kRedoOffset + (((2 + kRedoCap) * sizeof(unsigned long long) + 255) & ~size_t(255));
 static_assert(kSlotsOffset < kNoAllocScratchBytes / 8, "quadrature tables fit well inside");
 
 int na_fail(int code, const char* fmt, ...) {
@@ -268,7 +273,9 @@ extern "C" int adrt_solve_batch_noalloc(const adrt_batch_desc* d, const adrt_inp
   blocks = std::min<long long>(blocks, (d->num_wavenumbers + k.groups - 1) / k.groups);
 
   char* base = nd->addr;
-  const cudaError_t e0 = cudaMemsetAsync(base, 0, sizeof(unsigned long long), s);
+  cudaError_t e0 = cudaMemsetAsync(base, 0, sizeof(unsigned long long), s);
+  if (e0 == cudaSuccess)
+    e0 = cudaMemsetAsync(base + kRedoOffset, 0, 2 * sizeof(unsigned long long), s);
   if (e0 != cudaSuccess)
     return na_fail(ADRT_ERR_CUDA, "work counter reset: %s", cudaGetErrorString(e0));
 
@@ -332,8 +339,16 @@ extern "C" int adrt_solve_batch_noalloc(const adrt_batch_desc* d, const adrt_inp
   p.slot_bytes = slot;
   p.nslots = (int)(blocks * k.groups);
   p.max_layers = d->num_layers;
+  p.redo = reinterpret_cast<unsigned long long*>(base + kRedoOffset);
+  p.redo_cap = kRedoCap;
   k.launch(p, c, (int)blocks, k.smem, s);
-  const cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) {  // the re-solve pass over the listed wavenumbers
+    SolveParams q = p;
+    q.redo_pass = 1;
+    k.launch(q, c, (int)blocks, k.smem, s);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess)
     return na_fail(ADRT_ERR_CUDA, "solve kernel launch: %s", cudaGetErrorString(e));
   return ADRT_OK;

@@ -132,7 +132,9 @@ enum VecSlot {
 // the direct-transmission diagonal of the Lambda-split doubling (ping-pong).
 enum DVecSlot { D_MU = 0, D_WT, D_CW, D_HW, D_PP, D_PM, D_LAM0, D_LAM1 };
 // FP64 per-wavenumber scalars inside CommonLayout::misc (+48).
-enum MiscSlot { S_BS = 0, S_BTOP };
+// S_PIVALL: nonzero while a wavenumber is solved again with partial pivoting
+// in every solve (after a weak pivot of the tensor-core solve).
+enum MiscSlot { S_BS = 0, S_BTOP, S_PIVALL };
 
 // ============================================================== sync / reductions
 template <int G>
@@ -595,13 +597,16 @@ struct UseGjMMA {
 
 // The pivot-free solve's safety net: a pivot below kGjMinPivot in magnitude
 // (or not finite) means the matrix is not the diagonally dominant one the
-// argument above covers; gj_mma then returns kGjWeakPivot and op_gj solves
-// again with partial pivoting.  Every such matrix here is I minus a product
+// argument above covers; gj_mma then returns kGjWeakPivot and the caller
+// solves again with partial pivoting.  Every such matrix here is I minus a product
 // of reflection matrices with O(1) entries, so the bound is absolute.
 #ifndef ADRT_GJ_FALLBACK
 #define ADRT_GJ_FALLBACK 1  // tuning: 0 leaves out the pivoted re-solve
 #endif
-constexpr double kGjMinPivot = 1e-10;
+#ifndef ADRT_GJ_MIN_PIVOT
+#define ADRT_GJ_MIN_PIVOT 1e-10  // tuning
+#endif
+constexpr double kGjMinPivot = ADRT_GJ_MIN_PIVOT;
 constexpr int kGjWeakPivot = 2;  // op_gj result bit: solved again with pivoting
 
 // Device status bits of op_gj results (adrt_device_flag): an exactly zero
@@ -1103,10 +1108,11 @@ __device__ __noinline__ int op_gj_rows(unsigned a_off, unsigned b_off, unsigned 
 // The right-solve X = B A^{-1} (arguments as gj_pivoted): FP64 orders >= 8
 // on the tensor cores without pivoting (gj_mma), and the pivoted
 // elimination (a function of its own, so that the tensor-core path keeps its
-// registers) when `pivot` asks for it, when gj_mma met a weak pivot, or for
-// the other orders and FP32.  Returns bit 0 if a pivot was exactly 0, and
-// kGjWeakPivot when the tensor-core solve met a weak pivot and the pivoted
-// elimination was used instead.
+// registers) when `pivot` asks for it, or for the other orders and FP32.
+// Returns bit 0 if a pivot was exactly 0, and kGjWeakPivot when the
+// tensor-core solve met a weak pivot: its result is then not to be used, and
+// the caller solves again with pivoting (op_gj_safe below for one solve; the
+// forward solves the whole wavenumber again in a second pass).
 template <class Gm, class GO = Gm, bool OUTG = false>
 __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_off,
                                   unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
@@ -1116,7 +1122,7 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
   if constexpr (UseGjMMA<Gm>::value) {
     constexpr int NP = Gm::NP, LD = Gm::LD, DIM = Gm::DIM;
     static_assert(4 * (NP + 4) <= 6 * DIM + 4 && 8 * NP <= NP * LD, "gj_mma scratch");
-    if (!pivot || !ADRT_GJ_FALLBACK) {
+    if (!pivot) {
       const Real* A_rm = sp<Real>(a_off);
       const Real* B_rm = (b_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(b_off);
       const Real* bvec = (bvec_off == kNoMat || b_off == kIdentity) ? nullptr : sp<Real>(bvec_off);
@@ -1126,17 +1132,27 @@ __device__ __noinline__ int op_gj(unsigned a_off, unsigned b_off, unsigned bvec_
       Real* lbuf = o_cm ? o_cm : out_rm;
       const int r = gj_mma<Gm, GO, OUTG>(A_rm, B_rm, bvec, o_cm, out_rm, lbuf, sp<Real>(gj_off),
                                          t, bar, out_g);
-      if (!ADRT_GJ_FALLBACK) return r & 1;
-      if (!(r & kGjWeakPivot)) return r;
-      // A and B are intact: solve again with partial pivoting, once every
-      // thread is done with the scratch
-      gsync<Gm::G>(bar);
-      return gj_pivoted<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar,
-                                      orm_off, out_g) | kGjWeakPivot;
+      return ADRT_GJ_FALLBACK ? r : (r & 1);
     }
   }
   return gj_pivoted<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar,
                                   orm_off, out_g);
+}
+
+// op_gj with its own safety net, for solves outside the forward's wavenumber
+// pass (whose re-solve covers the whole wavenumber): on a weak pivot the same
+// solve again with partial pivoting (A and B are intact), kGjWeakPivot set.
+template <class Gm, class GO = Gm, bool OUTG = false>
+__device__ __noinline__ int op_gj_safe(unsigned a_off, unsigned b_off, unsigned bvec_off,
+                                       unsigned ocm_off, unsigned gj_off, unsigned red_off, int t,
+                                       int bar, unsigned orm_off = 0xffffffffu,
+                                       typename Gm::Real* out_g = nullptr) {
+  const int r = op_gj<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar,
+                                    orm_off, out_g);
+  if (!ADRT_GJ_FALLBACK || !(r & kGjWeakPivot)) return r & ~kGjWeakPivot;
+  gsync<Gm::G>(bar);
+  return op_gj<Gm, GO, OUTG>(a_off, b_off, bvec_off, ocm_off, gj_off, red_off, t, bar, orm_off,
+                             out_g, 1) | kGjWeakPivot;
 }
 
 // Tile copies between the HBM scratch and smem.  The HBM side is in the tile

@@ -375,6 +375,8 @@ __device__ void solve_wavenumber(const ColumnDev* C, int w, const Slot& S, int l
         om = om * (1.0 - f) / (1.0 - of);
       }
     }
+    if (tau > 0.0 && om > 0.0 && tau >= ldexp(1.0, kMaxDoublings + 1 - ipow0(om > 1.0 ? 1.0 : om)))
+      bad = 1;  // beyond the doubling bound (as the warp kernels)
     S[oTAU + l] = tau;
     S[oOM + l] = om;
     tc += tau;

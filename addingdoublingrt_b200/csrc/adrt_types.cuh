@@ -55,6 +55,14 @@ struct SolveParams {
   size_t slot_bytes;
   int nslots;
   int max_layers;               // L of the largest column (sizes the slot)
+  // Wavenumbers whose pivot-free solve met a weak pivot, solved again by a
+  // second launch of the same kernel (redo_pass = 1) with partial pivoting
+  // in every solve: redo[0] entries, redo[1] that pass's work counter,
+  // redo[2 ..] their task indices (room for redo_cap).  Null: no list.
+  unsigned long long* redo;
+  long long redo_cap;
+  int redo_pass;
+  int pivot_all;  // every solve with partial pivoting (ADRT_PIVOTING_PARTIAL)
 };
 
 }  // namespace adrt_dev

@@ -68,6 +68,12 @@ class Engine:
         _abi.ADJOINT_RECOMPUTE (every doubling chain recomputed in the backward pass)."""
         _lib.check(self.lib.adrt_engine_set_adjoint_mode(self.handle, int(mode)))
 
+    def set_pivoting(self, mode: int) -> None:
+        """adrt_engine_set_pivoting: _abi.PIVOTING_TENSOR_CORE (default: pivot-free
+        tensor-core solves with a pivoted re-solve on weak pivots) or
+        _abi.PIVOTING_PARTIAL (every solve with the reference's partial pivoting)."""
+        _lib.check(self.lib.adrt_engine_set_pivoting(self.handle, int(mode)))
+
     def read_status(self) -> int:
         v = C.c_int()
         _lib.check(self.lib.adrt_engine_read_status(self.handle, C.byref(v)))

@@ -771,7 +771,9 @@ def main():
             "e2e": ({"value": job_rate(args.wavenumbers, world, e2e_s),
                      "unit": "wavenumber-solves/s",
                      "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h} if e2e_s else None),
-            "gpu_launches": args.steps,
+            # per step: the solve kernel and its re-solve pass (empty unless a
+            # wavenumber met a weak pivot)
+            "gpu_launches": 2 * args.steps,
             **adj,
             "config4": c4,
             "clocks": results[pname]["clocks"],

@@ -61,8 +61,12 @@ enum adrt_device_flag {
   ADRT_FLAG_NONFINITE = 2,      /* a non-finite flux was produced */
   ADRT_FLAG_BAD_INPUT = 4,      /* tau < 0, omega outside [0,1], T < 0 seen on the device, or
                                    a channel range outside the spectrum (band integration) */
-  ADRT_FLAG_PIVOT_FALLBACK = 8  /* a pivot-free tensor-core right-solve met a pivot below 1e-10
-                                   and was solved again with partial pivoting (results valid) */
+  ADRT_FLAG_PIVOT_FALLBACK = 8, /* a pivot-free tensor-core right-solve met a pivot below 1e-10;
+                                   its wavenumber was solved again with partial pivoting in
+                                   every solve (results valid) */
+  ADRT_FLAG_PIVOT_UNRESOLVED = 16 /* more such wavenumbers in one launch than the re-solve list
+                                     holds (65536; 4096 for adrt_solve_batch_noalloc): the
+                                     excess keep their pivot-free results */
 };
 
 /* ---------------------------------------------------------------- config */
@@ -316,6 +320,17 @@ enum adrt_adjoint_mode {
 /* Select the engine's adjoint mode (enum adrt_adjoint_mode); both give the
  * same gradients to round-off. */
 int adrt_engine_set_adjoint_mode(adrt_engine* engine, int mode);
+
+/* Pivoting of the FP64 right-solves (I - R R')^{-1} (no counterpart in the
+ * reference, whose solves always pivot: src/matrix.hpp:120-124). */
+enum adrt_pivoting {
+  ADRT_PIVOTING_TENSOR_CORE = 0, /* default: pivot-free tensor-core elimination (the
+                                    matrices are diagonally dominant), partial pivoting
+                                    for unstable first-order starts, and a pivoted
+                                    re-solve of any wavenumber that meets a weak pivot */
+  ADRT_PIVOTING_PARTIAL = 1      /* every solve with the reference's partial pivoting */
+};
+int adrt_engine_set_pivoting(adrt_engine* engine, int mode);
 
 /* Reverse-mode adjoint of the batched solve: given the loss cotangents,
  * the gradients with respect to delta_tau, single_scat_albedo, the phase

@@ -263,6 +263,16 @@ def test_fp64_extremes_of_the_pivot_free_solve(eng, N):
     the layers) the engine's elimination and the oracle's pivoted LU agree to
     1.6e-6 at N = 8 (the two CPU builds, which share the LU, to 1e-10); those
     columns are held to 5e-6 plus the builds' spread."""
+    b = _extremes_batch(N)
+    ref = oracle.solve_oracle(b, 4)
+    sens = oracle.solve_oracle(b, 4, fma=True)
+    other = oracle.solve_reference(b, 4) if oracle.ref_available() else None
+    res = run_device(eng, b)
+    assert_fp64_parity(b, res, ref, sens, f"extremes N={N}", other_ref=other, nc_floor=5e-6)
+    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_SINGULAR_PIVOT) == 0
+
+
+def _extremes_batch(N):
     rng = np.random.default_rng(900 + N)
     W, L, M = 24, 12, 2 * N
     d = _abi.make_desc(num_wavenumbers=W, num_layers=L, num_quadrature=N, num_moments=M,
@@ -282,12 +292,74 @@ def test_fp64_extremes_of_the_pivot_free_solve(eng, N):
     lo = rng.uniform(500.0, 2000.0, size=W)
     b.set("wavenumber_low", lo)
     b.set("wavenumber_high", lo + 0.025)
-    ref = oracle.solve_oracle(b, 4)
-    sens = oracle.solve_oracle(b, 4, fma=True)
-    other = oracle.solve_reference(b, 4) if oracle.ref_available() else None
-    res = run_device(eng, b)
-    assert_fp64_parity(b, res, ref, sens, f"extremes N={N}", other_ref=other, nc_floor=5e-6)
-    assert eng.read_status() & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_SINGULAR_PIVOT) == 0
+    return b
+
+
+@pytest.mark.parametrize("N", [8, 16, 32])
+def test_partial_pivoting_mode_matches_the_oracle(eng, N):
+    """ADRT_PIVOTING_PARTIAL: every right-solve with the reference's partial
+    pivoting (the path a wavenumber that meets a weak pivot is solved again
+    on), on the extremes batch and a config-2 sample, against the oracle."""
+    try:
+        eng.set_pivoting(_abi.PIVOTING_PARTIAL)
+        eng.read_status()
+        for tag, b in ((f"extremes N={N}", _extremes_batch(N)),
+                       ("config2 sample", workloads.config2(W=64, L=30))):
+            ref = oracle.solve_oracle(b, 4)
+            sens = oracle.solve_oracle(b, 4, fma=True)
+            other = oracle.solve_reference(b, 4) if oracle.ref_available() else None
+            res = run_device(eng, b)
+            assert_fp64_parity(b, res, ref, sens, "partial pivoting " + tag, other_ref=other,
+                               nc_floor=5e-6)
+        st = eng.read_status()
+        assert st & (_abi.ADRT_FLAG_NONFINITE | _abi.ADRT_FLAG_SINGULAR_PIVOT
+                     | _abi.ADRT_FLAG_PIVOT_FALLBACK | _abi.ADRT_FLAG_PIVOT_UNRESOLVED) == 0
+    finally:
+        eng.set_pivoting(_abi.PIVOTING_TENSOR_CORE)
+    with pytest.raises(RuntimeError):
+        eng.set_pivoting(7)
+
+
+def test_resolve_list_pass_solves_only_the_listed_wavenumbers(eng):
+    """The second pass of a solve (the pivoted re-solve of wavenumbers whose
+    pivot-free solve met a weak pivot -- none of the physical inputs tested
+    here do) run alone over a given list: the listed wavenumbers match the
+    oracle, every other output is left as it was."""
+    import ctypes as C
+    import torch
+    from addingdoublingrt_b200 import _lib
+    from addingdoublingrt_b200.engine import _ptr, alloc_device_outputs, to_device
+    b = workloads.config2(W=96, L=25)
+    di = to_device(b)
+    do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+    for v in do.values():
+        v.fill_(float("nan"))
+    listed = [5, 17, 18, 60, 95]
+    ins = _abi.Inputs()
+    for f in _abi.INPUT_FIELDS:
+        setattr(ins, f, _ptr(di.get(f)))
+    outs = _abi.Outputs()
+    for f in _abi.OUTPUT_FIELDS:
+        setattr(outs, f, _ptr(do.get(f)))
+    lib = _lib.load()
+    fn = lib.adrt_internal_resolve_listed
+    fn.argtypes = [C.c_void_p, C.POINTER(_abi.BatchDesc), C.POINTER(_abi.Inputs),
+                   C.POINTER(_abi.Outputs), C.POINTER(C.c_longlong), C.c_int]
+    arr = (C.c_longlong * len(listed))(*listed)
+    assert fn(eng.handle, C.byref(b.desc), C.byref(ins), C.byref(outs), arr, len(listed)) == 0, \
+        lib.adrt_last_status_detail().decode()
+    torch.cuda.synchronize()
+    sub = b.subset(listed)
+    ref = oracle.solve_oracle(sub, 4, which=_abi.INTERFACE_OUTPUTS)
+    sens = oracle.solve_oracle(sub, 4, which=_abi.INTERFACE_OUTPUTS, fma=True)
+    res = {k: v.view(b.W, b.L + 1)[listed].cpu().numpy().ravel() for k, v in do.items()}
+    assert_fp64_parity(sub, res, ref, sens, "re-solve list")
+    others = [w for w in range(b.W) if w not in listed]
+    for k, v in do.items():
+        assert torch.isnan(v.view(b.W, b.L + 1)[others]).all(), k
+    bad = (C.c_longlong * 1)(b.W)
+    assert fn(eng.handle, C.byref(b.desc), C.byref(ins), C.byref(outs), bad, 1) == \
+        _abi.ADRT_ERR_INVALID_ARGUMENT
 
 
 MIXED_CASES = [
