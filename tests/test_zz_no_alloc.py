@@ -182,3 +182,28 @@ def test_noalloc_rejects_a_batch_beyond_its_work_memory():
     rc = _call_noalloc(lib, b.desc, di, do)
     assert rc == _abi.ADRT_ERR_WORKSPACE, lib.adrt_last_status_detail().decode()
     assert "work memory" in lib.adrt_last_status_detail().decode()
+
+
+@pytest.mark.gpu
+def test_noalloc_calls_take_no_device_memory():
+    """After a first call (which loads the module and uploads the order's
+    quadrature table), further calls leave the device's free memory exactly
+    as it was: nothing is allocated, not even by the driver."""
+    if not cuda_available():
+        pytest.skip("no CUDA device")
+    import torch
+    from addingdoublingrt_b200.engine import alloc_device_outputs, to_device
+    lib = _lib.load()
+    b = workloads.config2(W=4096, L=30)
+    di = to_device(b)
+    do = alloc_device_outputs(b, _abi.INTERFACE_OUTPUTS)
+    assert _call_noalloc(lib, b.desc, di, do) == 0, lib.adrt_last_status_detail().decode()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    torch_bytes = torch.cuda.memory_allocated()
+    for _ in range(3):
+        assert _call_noalloc(lib, b.desc, di, do) == 0, lib.adrt_last_status_detail().decode()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_allocated() == torch_bytes
+    assert _read_status(lib) & ~_abi.ADRT_FLAG_PIVOT_FALLBACK == 0
