@@ -1484,10 +1484,19 @@ int adrt_engine_autotune_uneven(adrt_engine* e, const adrt_column_desc* cols, in
     (void)taken;
     adrt_uneven_plan p = plan;
     double ns[2] = {0.0, 0.0};
-    for (int m = 0; m < 2 && !rc; ++m) {
-      p.mapping[oi] = m;
-      rc = time_plan(cv, p, &ns[m]);
-    }
+    p.mapping[oi] = ADRT_MAPPING_WARP;
+    rc = time_plan(cv, p, &ns[0]);
+    if (rc) break;
+    // the thread mapping first on an eighth of the sample; one more than four
+    // times slower there per wavenumber is not timed on the whole sample (at
+    // N = 16 that takes seconds).  The pilot fills at most 3/8 of the thread
+    // slots, which inflates its time per wavenumber by less than 4x, so a
+    // mapping it drops is slower than the warp mapping on the whole sample.
+    std::vector<UnevenColumn> pilot = cv;
+    for (auto& c : pilot) c.W = std::max(1, c.W / 8);
+    p.mapping[oi] = ADRT_MAPPING_THREAD;
+    rc = time_plan(pilot, p, &ns[1]);
+    if (!rc && !(ns[1] > 4.0 * ns[0])) rc = time_plan(cv, p, &ns[1]);
     if (rc) break;
     plan.ns_per_wavenumber[oi][0] = ns[0];
     plan.ns_per_wavenumber[oi][1] = ns[1];

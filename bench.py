@@ -779,8 +779,20 @@ def main():
             "clocks": results[pname]["clocks"],
             "device_status": {p: results[p]["status"] for p in precisions},
         }
+        if "mixed" in results and pname != "mixed":
+            # the mixed form's own roofline: its algorithmic flops against the
+            # FP32 FMA peak (its FP32 products run as TF32 x3 tensor-core
+            # tiles, the rest in FP64)
+            am = fl / (results["mixed"]["ms"] * 1e-3) / 1e12
+            line["roofline_mixed"] = {"bound": "fp32", "achieved": am,
+                                      "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                                      "frac": am / peaks["fp32_tflops"]
+                                      if peaks["fp32_tflops"] else None}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(b)
+            one = cpu_baseline(b, seconds=4.0, threads=1)
+            line["cpu_baseline"]["value_1_thread"] = one["value"]
+            line["cpu_baseline"]["sample_1_thread"] = one["sample"]
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

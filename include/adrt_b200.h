@@ -390,7 +390,9 @@ int adrt_solve_batch_uneven(adrt_engine* engine, const adrt_column_desc* cols, i
  * caps the warp launch's grid (0 = the occupancy limit); cost_order sorts the
  * columns longest first (L N^3 per wavenumber) so that the dynamic task
  * queue ends with short tasks.  ns_per_wavenumber holds what the autotuner
- * measured for [order 4, 8, 16][warp, thread] (0 = not measured). */
+ * measured for [order 4, 8, 16][warp, thread] (0 = not measured; a thread
+ * mapping more than 4x slower on an eighth of the sample keeps that
+ * pilot's figure). */
 enum adrt_mapping { ADRT_MAPPING_WARP = 0, ADRT_MAPPING_THREAD = 1 };
 typedef struct adrt_uneven_plan {
   int mapping[3];
