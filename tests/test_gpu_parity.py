@@ -420,6 +420,25 @@ def test_bad_values_set_the_device_status_flag(eng):
     assert eng.read_status() == 0  # read clears
 
 
+@pytest.mark.parametrize("om,tau,flagged", [(0.5, 2.0 ** 48, False), (0.5, 2.0 ** 49, True),
+                                            (0.05, 2.0 ** 55, True), (0.005, 2.0 ** 60, False),
+                                            (0.005, 2.0 ** 61, True)])
+def test_layers_beyond_the_doubling_bound_are_flagged(eng, om, tau, flagged):
+    """The reference's rule nn = trunc(log2 tau) + ipow0(omega) above the
+    device's bound of 64 doublings (tau >= 2^(65 - ipow0)): the layer is
+    solved at the bound and the wavenumber flagged as bad input; one below
+    the bound is not flagged (and its fluxes are finite)."""
+    b = workloads.config1(W=3)
+    b.arrays["delta_tau"].reshape(3, -1)[1, 4] = tau
+    b.arrays["single_scat_albedo"] = np.full(b.W * b.L, 0.9)
+    b.arrays["single_scat_albedo"].reshape(3, -1)[1, 4] = om
+    eng.read_status()
+    res = run_device(eng, b)
+    st = eng.read_status()
+    assert bool(st & _abi.ADRT_FLAG_BAD_INPUT) == flagged, st
+    assert np.all(np.isfinite(res["flux_up"]))
+
+
 def _uneven_cols(seed=4, ncols=12, per=200):
     cols = [c.subset(np.arange(min(c.W, per)))
             for c in workloads.config4_columns(ncols=ncols, seed=seed)]
