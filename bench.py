@@ -740,6 +740,15 @@ def main():
                 "4000-wavenumber capture (profiles/solve_kernel_traffic.json)",
                 "peak_source": peaks["source"] + " (of measured)",
                 "flops_per_launch": fl}
+        if pname == "fp64" and tpk and tpk.get("fp64_dmma_tflops"):
+            # the FP64 products run on the FP64 tensor cores: their measured
+            # DMMA rate (above the FMA rate) is the roof; the FMA fraction stays
+            dm = tpk["fp64_dmma_tflops"]
+            roof.update({"bound": "tensor", "peak": dm, "frac": achieved / dm,
+                         "peak_source": "measured live: FP64 DMMA (mma.sync m8n8k4.f64) "
+                                        "throughput probe on this GPU (of measured)",
+                         "frac_of_fp64_fma_peak": achieved / pk if pk else None,
+                         "fp64_fma_peak": pk})
         line = {
             "metric": METRIC,
             "value": job_rate(args.wavenumbers, world, ms * 1e-3),
