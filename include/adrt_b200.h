@@ -59,8 +59,10 @@ enum adrt_status {
 enum adrt_device_flag {
   ADRT_FLAG_SINGULAR_PIVOT = 1, /* an LU pivot was exactly zero (reference: silent inv=0) */
   ADRT_FLAG_NONFINITE = 2,      /* a non-finite flux was produced */
-  ADRT_FLAG_BAD_INPUT = 4,      /* tau < 0, omega outside [0,1], T < 0 seen on the device, or
-                                   a channel range outside the spectrum (band integration) */
+  ADRT_FLAG_BAD_INPUT = 4,      /* tau < 0, omega outside [0,1], T < 0 seen on the device, a
+                                   layer so thick that the doubling rule asks for more than 64
+                                   doublings (solved at 64), or a channel range outside the
+                                   spectrum (band integration) */
   ADRT_FLAG_PIVOT_FALLBACK = 8, /* a pivot-free tensor-core right-solve met a pivot below 1e-10;
                                    its wavenumber was solved again with partial pivoting in
                                    every solve (results valid) */
