@@ -797,6 +797,8 @@ def main():
                                       "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
                                       "frac": am / peaks["fp32_tflops"]
                                       if peaks["fp32_tflops"] else None}
+            if tpk and tpk.get("tf32_mma_tflops"):
+                line["roofline_mixed"]["frac_of_tf32_mma_peak"] = am / tpk["tf32_mma_tflops"]
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(b)
             one = cpu_baseline(b, seconds=4.0, threads=1)
