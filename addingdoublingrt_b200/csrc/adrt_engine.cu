@@ -1437,14 +1437,28 @@ int adrt_engine_autotune_uneven(adrt_engine* e, const adrt_column_desc* cols, in
   cudaEvent_t ev0, ev1;
   CUDA_TRY(cudaEventCreate(&ev0));
   CUDA_TRY(cudaEventCreate(&ev1));
-  // ns per wavenumber of `cv` under `p` (one untimed run, then one timed)
-  auto time_plan = [&](std::vector<UnevenColumn>& cv, const adrt_uneven_plan& p,
-                       double* ns) -> int {
+  // ns per wavenumber of `cv` under `p` (one warm-up run, then one timed).
+  // With give_up > 0 the warm-up run is timed too (allocation included), and
+  // a mapping already slower than give_up ns per wavenumber there keeps that
+  // figure without the second run.
+  auto time_plan = [&](std::vector<UnevenColumn>& cv, const adrt_uneven_plan& p, double* ns,
+                       double give_up = 0.0) -> int {
     long long n = 0;
     for (auto& c : cv) n += c.W;
     if (n == 0) return ADRT_OK;
+    if (give_up > 0.0) CUDA_TRY(cudaEventRecord(ev0, s));
     int r = uneven_locked(e, cv, s, p);
     if (r) return r;
+    if (give_up > 0.0) {
+      CUDA_TRY(cudaEventRecord(ev1, s));
+      CUDA_TRY(cudaEventSynchronize(ev1));
+      float ms0 = 0.f;
+      CUDA_TRY(cudaEventElapsedTime(&ms0, ev0, ev1));
+      if (ms0 * 1e6 / (double)n > give_up) {
+        *ns = ms0 * 1e6 / (double)n;
+        return ADRT_OK;
+      }
+    }
     CUDA_TRY(cudaEventRecord(ev0, s));
     if ((r = uneven_locked(e, cv, s, p))) return r;
     CUDA_TRY(cudaEventRecord(ev1, s));
@@ -1495,7 +1509,10 @@ int adrt_engine_autotune_uneven(adrt_engine* e, const adrt_column_desc* cols, in
     std::vector<UnevenColumn> pilot = cv;
     for (auto& c : pilot) c.W = std::max(1, c.W / 8);
     p.mapping[oi] = ADRT_MAPPING_THREAD;
-    rc = time_plan(pilot, p, &ns[1]);
+    // (a warm-up pilot fifty times slower than the warp mapping -- the thread
+    // mapping at N = 16, whose every launch lasts one whole wavenumber's
+    // solve, seconds -- is not run a second time)
+    rc = time_plan(pilot, p, &ns[1], 50.0 * ns[0]);
     if (!rc && !(ns[1] > 4.0 * ns[0])) rc = time_plan(cv, p, &ns[1]);
     if (rc) break;
     plan.ns_per_wavenumber[oi][0] = ns[0];
